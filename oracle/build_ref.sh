@@ -1,0 +1,33 @@
+#!/usr/bin/env bash
+# Test infrastructure only (oracle). Compiles the reference's own CPU sources
+# for the ISDF path, unmodified, where they lie under the reference checkout,
+# together with the single-rank MPI / FFTW shims and BLAS forwarders in
+# oracle/shims, into oracle/_ref/libisdf_ref.so. The reference's flags are
+# kept (-O2 -std=c++14, no -march, so no FMA contraction: Makefile:102,159).
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+set -euo pipefail
+HERE="$(cd "$(dirname "$0")" && pwd)"
+REF="${1:-/root/reference}"
+OUT="$HERE/_ref"
+if [ ! -d "$REF/src" ]; then
+  echo "reference sources not found under $REF; skipping oracle/_ref build" >&2
+  exit 0
+fi
+OPENBLAS_DIR="$(python3 -c 'import scipy, os; print(os.path.join(os.path.dirname(os.path.dirname(scipy.__file__)), "scipy.libs"))')"
+OPENBLAS="$(ls "$OPENBLAS_DIR"/libscipy_openblas*.so | head -1)"
+mkdir -p "$OUT/obj"
+CXXFLAGS="-O2 -std=c++14 -fPIC -w -I$HERE/shims -I$REF/include -I$REF/include/common"
+SRCS="src/common/utility.cpp src/common/global.cpp src/common/fourier.cpp src/common/checkcode.cpp
+      src/cpu/getpoints_Kmeans_MPI.cpp src/cpu/getbasis_MPI.cpp src/cpu/blas.cpp src/cpu/lapack.cpp"
+OBJS=""
+for s in $SRCS; do
+  o="$OUT/obj/$(echo "$s" | tr '/' '_' ).o"
+  g++ $CXXFLAGS -c "$REF/$s" -o "$o"
+  OBJS="$OBJS $o"
+done
+g++ $CXXFLAGS -c "$HERE/ref_driver.cpp" -o "$OUT/obj/ref_driver.o"
+g++ -O2 -std=c++14 -fPIC -c "$HERE/shims/minifft.cpp" -o "$OUT/obj/minifft.o"
+gcc -O2 -fPIC -c "$HERE/shims/blas_alias.c" -o "$OUT/obj/blas_alias.o"
+g++ -shared -o "$OUT/libisdf_ref.so" $OBJS "$OUT/obj/ref_driver.o" "$OUT/obj/minifft.o" \
+    "$OUT/obj/blas_alias.o" "$OPENBLAS" -Wl,-rpath,"$OPENBLAS_DIR"
+echo "built $OUT/libisdf_ref.so"

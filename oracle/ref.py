@@ -1,0 +1,114 @@
+"""Test infrastructure only (oracle): ctypes bindings of oracle/_ref/libisdf_ref.so.
+
+That library is the reference's own CPU code for the ISDF path (K-means
+selection in src/common/utility.cpp:631-988, the FP64 fit in
+src/cpu/getbasis_MPI.cpp, the check in src/common/checkcode.cpp) compiled by
+oracle/build_ref.sh with single-rank shims. Only tests, the smoke check and
+bench.py's CPU-baseline leg import this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "libisdf_ref.so")
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        I = ctypes.c_int
+        _lib.ref_kmeans_piv.argtypes = [P, P, P, I, I, I, I, I, I, I, I, ctypes.c_uint, I, P, P, P,
+                                        P, P, I]
+        _lib.ref_getbasis.argtypes = [P, P, P, I, I, I, I, I, I, I, P, P, P, I]
+        _lib.ref_checkcode.argtypes = [P, P, P, I, I, I, I, I, I, I, P, P, P, P, P, I]
+        _lib.ref_weight.argtypes = [P, I, I, I, I, I, I, P]
+        _lib.ref_iround.argtypes = [ctypes.c_double]
+        _lib.ref_iround.restype = I
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _geom(ng, length):
+    ng = np.ascontiguousarray(ng, dtype=np.int32)
+    ln = np.ascontiguousarray(length, dtype=np.float64)
+    return ng, ln
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def weight(psi, nocc, nv1, nc1, nv2, nc2):
+    psi = np.asfortranarray(psi, dtype=np.float64)
+    w = np.empty(psi.shape[0])
+    lib().ref_weight(_ptr(psi), psi.shape[0], nocc, nv1, nc1, nv2, nc2, _ptr(w))
+    return w
+
+
+def kmeans_piv(psi, ng, length, nocc, nv1, nc1, nv2, nc2, mu, iters, rand_seed=1,
+               cross_check=False):
+    """Returns (piv int32[Ng], rk_eff, iterations run, weight)."""
+    psi = np.asfortranarray(psi, dtype=np.float64)
+    g, ln = _geom(ng, length)
+    n = int(np.prod(g))
+    assert psi.shape[0] == n
+    piv = np.zeros(n, dtype=np.int32)
+    rk = np.zeros(1, dtype=np.int32)
+    it = np.zeros(1, dtype=np.int32)
+    w = np.empty(n)
+    log = ctypes.create_string_buffer(1 << 16)
+    rc = lib().ref_kmeans_piv(_ptr(psi), _ptr(g), _ptr(ln), nocc, psi.shape[1], nv1, nc1, nv2,
+                              nc2, mu, iters, rand_seed, int(cross_check), _ptr(piv), _ptr(rk),
+                              _ptr(it), _ptr(w), log, len(log))
+    if rc != 0:
+        raise OracleError(f"ref_kmeans_piv rc={rc}: {log.value.decode(errors='replace')[-400:]}")
+    return piv, int(rk[0]), int(it[0]), w
+
+
+def getbasis(psi, ng, length, nocc, nv1, nc1, nv2, nc2, rk, piv):
+    """theta (Ng x rk, F-order) from the reference's getbasis_MPI at one rank."""
+    psi = np.asfortranarray(psi, dtype=np.float64)
+    g, ln = _geom(ng, length)
+    n = int(np.prod(g))
+    piv = np.ascontiguousarray(piv, dtype=np.int32)
+    theta = np.zeros((n, rk), dtype=np.float64, order="F")
+    log = ctypes.create_string_buffer(1 << 14)
+    rc = lib().ref_getbasis(_ptr(psi), _ptr(g), _ptr(ln), nocc, psi.shape[1], nv1, nc1, nv2, nc2,
+                            rk, _ptr(piv), _ptr(theta), log, len(log))
+    if rc != 0:
+        raise OracleError(f"ref_getbasis rc={rc}: {log.value.decode(errors='replace')[-400:]}")
+    return theta
+
+
+def checkcode(psi, ng, length, nocc, nv1, nc1, nv2, nc2, rk, piv, theta):
+    """(fit error, Coulomb error) as printed by the reference's checkcode."""
+    psi = np.asfortranarray(psi, dtype=np.float64)
+    theta = np.asfortranarray(theta, dtype=np.float64)
+    g, ln = _geom(ng, length)
+    piv = np.ascontiguousarray(piv, dtype=np.int32)
+    fe = np.zeros(1)
+    ce = np.zeros(1)
+    log = ctypes.create_string_buffer(1 << 14)
+    rc = lib().ref_checkcode(_ptr(psi), _ptr(g), _ptr(ln), nocc, psi.shape[1], nv1, nc1, nv2, nc2,
+                             rk, _ptr(piv), _ptr(theta), _ptr(fe), _ptr(ce), log, len(log))
+    if rc != 0:
+        raise OracleError(f"ref_checkcode rc={rc}: {log.value.decode(errors='replace')[-400:]}")
+    return float(fe[0]), float(ce[0])
+
+
+def iround(a: float) -> int:
+    return int(lib().ref_iround(float(a)))

@@ -1,0 +1,184 @@
+// Test infrastructure only (oracle). Thin extern "C" entry points into the
+// reference's own CPU sources for the ISDF path, compiled unmodified from
+// src/common/utility.cpp (KMEAN), src/cpu/getpoints_Kmeans_MPI.cpp (weight +
+// KMEAN), src/cpu/getbasis_MPI.cpp (the FP64 fit) and src/common/checkcode.cpp
+// + src/common/fourier.cpp (the Coulomb check), with the single-rank MPI and
+// FFTW shims in oracle/shims. Built by oracle/build_ref.sh into oracle/_ref/.
+//
+// Only the tests, the smoke check and the CPU-baseline leg of bench.py load
+// the library this file builds; the product never does.
+#include "isdf.hpp"
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <sstream>
+#include <string>
+
+using namespace isdf;
+
+namespace {
+
+Domain make_domain(const int* ng, const double* len) {
+  Domain d;
+  d.length = Point3(len[0], len[1], len[2]);
+  d.posStart = Point3(0.0, 0.0, 0.0);
+  d.numGrid = Index3(ng[0], ng[1], ng[2]);
+  d.numGridFine = Index3(ng[0], ng[1], ng[2]);
+  return d;
+}
+
+// Routes the reference's log stream (isdfOFS) into a string for one call.
+struct LogCapture {
+  std::stringbuf buf;
+  std::streambuf* old;
+  LogCapture() {
+    std::ostream& os = isdfOFS;
+    old = os.rdbuf(&buf);
+    os.clear();
+    os.precision(17);
+  }
+  ~LogCapture() {
+    std::ostream& os = isdfOFS;
+    os.rdbuf(old);
+  }
+  std::string str() const { return buf.str(); }
+};
+
+int parse_after(const std::string& log, const std::string& key, double* out) {
+  size_t p = log.rfind(key);
+  if (p == std::string::npos) return -1;
+  *out = std::strtod(log.c_str() + p + key.size(), nullptr);
+  return 0;
+}
+
+void copy_log(const std::string& s, char* log, int loglen) {
+  if (!log || loglen <= 0) return;
+  std::snprintf(log, (size_t)loglen, "%s", s.c_str());
+}
+
+}  // namespace
+
+extern "C" {
+
+// Weight w(r) = sum_{S2} psi^2 * sum_{S1} psi^2, the loop of
+// src/cpu/getpoints_Kmeans_MPI.cpp:33-45 restated for one rank (the reference
+// keeps it inside getpoints_Kmeans_MPI, which also runs KMEAN).
+void ref_weight(const double* psi, int ng_total, int nocc, int nv1, int nc1, int nv2, int nc2,
+                double* w) {
+  std::vector<double> sumI(ng_total, 0.0), sumJ(ng_total, 0.0);
+  for (int i = nocc - nv2; i < nocc + nc2; i++)
+    for (int kk = 0; kk < ng_total; kk++)
+      sumI[kk] += psi[(size_t)i * ng_total + kk] * psi[(size_t)i * ng_total + kk];
+  for (int j = nocc - nv1; j < nocc + nc1; j++)
+    for (int kk = 0; kk < ng_total; kk++)
+      sumJ[kk] += psi[(size_t)j * ng_total + kk] * psi[(size_t)j * ng_total + kk];
+  for (int kk = 0; kk < ng_total; kk++) w[kk] = 0.0 + sumI[kk] * sumJ[kk];
+}
+
+// The K-means point selection of the GPU ISDF() path: weight, then KMEAN
+// (src/common/utility.cpp:631-988) with the tolerances of
+// src/cuda/isdf-gpu.cpp:31-32, piv zeroed first as src/common/isdf.cpp:174-175
+// does. rk_eff receives the (possibly shrunk) number of selected points.
+// When cross_check is set the reference's getpoints_Kmeans_MPI is also run on
+// the same input and its piv must equal this one (returns -100 otherwise).
+int ref_kmeans_piv(const double* psi, const int* ng, const double* len, int nocc, int nstate,
+                   int nv1, int nc1, int nv2, int nc2, int mu, int iters, unsigned rand_seed,
+                   int cross_check, int* piv, int* rk_eff, int* n_iter, double* weight_out,
+                   char* log, int loglen) {
+  try {
+    LogCapture cap;
+    Domain dom = make_domain(ng, len);
+    const int n = dom.NumGridTotal();
+    DblNumVec weight(n);
+    ref_weight(psi, n, nocc, nv1, nc1, nv2, nc2, weight.Data());
+    if (weight_out) std::memcpy(weight_out, weight.Data(), sizeof(double) * n);
+    std::memset(piv, 0, sizeof(int) * n);
+    Int rk = mu;
+    std::srand(rand_seed);
+    KMEAN(n, weight, rk, 1e-5, iters, 1e-8, dom, piv);
+    *rk_eff = rk;
+    std::string s = cap.str();
+    double it = -1;
+    *n_iter = parse_after(s, "Converged in ", &it) == 0 ? (int)it : -1;
+    if (cross_check) {
+      std::vector<int> piv2(n, 0);
+      DblNumMat psiRow(n, nstate, false, const_cast<double*>(psi));
+      IntNumVec pv(n, false, piv2.data());
+      Int ntot = n, mu_ = mu, it_ = iters;
+      Real tmpi = 0.0;
+      std::srand(rand_seed);
+      isdffunc::getpoints_Kmeans_MPI(psiRow, dom, nocc, nv1, nc1, nv2, nc2, ntot, mu_, pv, tmpi,
+                                     it_);
+      if (std::memcmp(piv2.data(), piv, sizeof(int) * n) != 0) return -100;
+    }
+    copy_log(s, log, loglen);
+    return 0;
+  } catch (const std::exception& e) {
+    copy_log(e.what(), log, loglen);
+    return -1;
+  }
+}
+
+// The FP64 fit of src/cpu/getbasis_MPI.cpp:9-250 at one rank: gather psi(mu),
+// GEMM (+ second GEMM when S1 != S2), Hadamard product, C C^T gather, +eps*I,
+// dpotrf, two dtrsm. theta is Ng x rk column-major. Pass the rk that the
+// selector produced (the GPU path fits with the shrunk rk, isdf-gpu.cpp:99).
+int ref_getbasis(const double* psi, const int* ng, const double* len, int nocc, int nstate,
+                 int nv1, int nc1, int nv2, int nc2, int rk, const int* piv, double* theta,
+                 char* log, int loglen) {
+  try {
+    LogCapture cap;
+    Domain dom = make_domain(ng, len);
+    const int n = dom.NumGridTotal();
+    DblNumMat psiRow(n, nstate, false, const_cast<double*>(psi));
+    DblNumMat psiCol(n, nstate);
+    std::memcpy(psiCol.Data(), psi, sizeof(double) * (size_t)n * nstate);
+    IntNumVec pv(n, false, const_cast<int*>(piv));
+    DblNumMat out(n, rk, false, theta);
+    Int ntot = n;
+    Real tmpi = 0.0;
+    isdffunc::getbasis_MPI(psiRow, psiCol, dom, nocc, nv1, nc1, nv2, nc2, ntot, rk, out, pv, tmpi);
+    copy_log(cap.str(), log, loglen);
+    return 0;
+  } catch (const std::exception& e) {
+    copy_log(e.what(), log, loglen);
+    return -1;
+  }
+}
+
+// The check of src/common/checkcode.cpp:54-313 (pair-density fit error and
+// truncated-Coulomb 4-index error), read back from the lines it prints.
+int ref_checkcode(const double* psi, const int* ng, const double* len, int nocc, int nstate,
+                  int nv1, int nc1, int nv2, int nc2, int rk, const int* piv, const double* theta,
+                  double* fit_err, double* coul_err, char* log, int loglen) {
+  try {
+    LogCapture cap;
+    Domain dom = make_domain(ng, len);
+    const int n = dom.NumGridTotal();
+    DblNumMat psiRow(n, nstate, false, const_cast<double*>(psi));
+    DblNumMat psiCol(n, nstate);
+    std::memcpy(psiCol.Data(), psi, sizeof(double) * (size_t)n * nstate);
+    IntNumVec pv(n, false, const_cast<int*>(piv));
+    DblNumMat th(n, rk);
+    std::memcpy(th.Data(), theta, sizeof(double) * (size_t)n * rk);
+    Int ntot = n;
+    Fourier fft;
+    fft.Initialize(dom);
+    isdffunc::checkcode(psiRow, psiCol, dom, nocc, nv1, nc1, nv2, nc2, ntot, rk, th, pv, fft);
+    std::string s = cap.str();
+    copy_log(s, log, loglen);
+    if (parse_after(s, "sqrt((rhoij-rho^hat)^2)/sqrt(rhoij^2)=", fit_err)) return -2;
+    if (parse_after(s, "sqrt((ijkl-ijkl^hat)^2)/sqrt(ijkl^2) =", coul_err)) return -3;
+    return 0;
+  } catch (const std::exception& e) {
+    copy_log(e.what(), log, loglen);
+    return -1;
+  }
+}
+
+// The reference's integer rounding IRound (include/common/utility.hpp:18-23),
+// used for the default mu and the QRCP sketch width.
+int ref_iround(double a) { return IRound(a); }
+
+}  // extern "C"
