@@ -1,0 +1,135 @@
+/*
+ * isdf_c.h - C ABI of the B200 ISDF engine (libisdf_b200.so).
+ *
+ * Drop-in boundary for the GPU ISDF() entry point of LibISDF:
+ *   void isdf::isdffunc::ISDF(double* d_psirow, Domain domain, int nocc,
+ *        int nstate, int nv1, int nc1, int nv2, int nc2, int mu_points,
+ *        double* d_thetaCol, int* piv, int KmeansMaxIter_ISDF, bool check)
+ *   (reference include/isdf.hpp:37, src/common/isdf.cpp:132-209).
+ * The C++ overloads with that exact signature live in include/isdf.hpp and
+ * wrap isdf_solve() below.
+ *
+ * Conventions (same as the reference, README.md:246-260):
+ *  - one rank, one GPU; the caller allocates and frees every buffer;
+ *  - psi: device, Ng x nstate, column-major, ld = Ng, read only;
+ *  - theta: device, Ng x mu, column-major, ld = Ng, fully written (columns
+ *    past the effective mu are zero-filled);
+ *  - piv: HOST int[Ng], fully written;
+ *  - grid index g = ix + nx*(iy + ny*iz).
+ * Every function returns ISDF_OK (0) or a negative ISDF_ERR_* code and never
+ * throws or exits; isdf_last_error() gives a message for the calling thread.
+ * All plain pointers; no CUDA or torch types appear in the signatures
+ * (streams are passed as void*, a cudaStream_t, NULL = the library's own).
+ */
+#ifndef ISDF_C_H
+#define ISDF_C_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ISDF_OK 0
+#define ISDF_ERR_ARG (-1)         /* invalid argument */
+#define ISDF_ERR_CUDA (-2)        /* CUDA runtime / launch failure */
+#define ISDF_ERR_NOMEM (-3)       /* device allocation failed */
+#define ISDF_ERR_NOT_SPD (-4)     /* C C^T + eps I not positive definite */
+#define ISDF_ERR_TIMEOUT (-5)     /* a bounded device wait ran out */
+#define ISDF_ERR_UNSUPPORTED (-6) /* shape or option outside what is built */
+#define ISDF_ERR_CANCELLED (-7)   /* serving: request cancelled */
+#define ISDF_ERR_BUSY (-8)        /* serving: queue full */
+
+#define ISDF_SELECT_KMEANS 0
+#define ISDF_SELECT_QRCP 1
+
+#define ISDF_PRECISION_FP64 0  /* the reference's FP64 method */
+#define ISDF_PRECISION_MIXED 1 /* split-BF16 tensor-core GEMMs + FP64 refinement */
+
+/* Layout-compatible with the numeric fields of the reference's Domain
+ * (include/common/domain.hpp:8-36); the MPI communicators are not needed
+ * at world size 1. */
+typedef struct isdf_domain_t {
+  double length[3];
+  double pos_start[3];
+  int num_grid[3];
+  int num_grid_fine[3];
+} isdf_domain_t;
+
+typedef struct isdf_options_t {
+  int precision;          /* ISDF_PRECISION_* (default FP64) */
+  int refine_steps;       /* mixed precision: FP64 refinement steps (default 2) */
+  double qrcp_oversample; /* QRCP sketch width = IRound(sqrt(f * mu)); reference 1.5 */
+  long long qrcp_seed;    /* srand48 seed of the QRCP sketch; reference 41 */
+  long long rand_seed;    /* >= 0: srand() before K-means (only its npt < mu branch
+                             draws from rand()); < 0: keep the process state */
+  void* stream;           /* cudaStream_t to run on; NULL = library stream */
+  int reserved[8];
+} isdf_options_t;
+
+typedef struct isdf_report_t {
+  int rk_requested;  /* mu used (mu_points or the default formula) */
+  int rk_eff;        /* selected points after de-duplication */
+  int kmeans_iters;  /* Lloyd iterations run (-1: early-return branch) */
+  int npt;           /* grid points kept by the weight filter */
+  double fit_err;    /* check: ||rho - theta C||_F / ||rho||_F */
+  double coul_err;   /* check: relative truncated-Coulomb 4-index error */
+  double t_select_ms, t_fit_ms, t_chol_ms, t_solve_ms, t_check_ms, t_total_ms;
+  int chol_info;     /* > 0: leading minor that failed */
+  int reserved[7];
+} isdf_report_t;
+
+/* Fills *opt with the reference's defaults. */
+void isdf_default_options(isdf_options_t* opt);
+
+/* Full ISDF solve (reference src/common/isdf.cpp:132-209 ->
+ * src/cuda/isdf-gpu.cpp:9-403, with the Kmeans/QRCP selector of the CPU entry
+ * point src/common/isdf.cpp:60-74). mu_points = 0 selects
+ * IRound(sqrt((nc1+nv1)(nc2+nv2)) * 8) (isdf.cpp:160-164). opt and rep may
+ * be NULL. Synchronous: returns after theta and piv are written. */
+int isdf_solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, int nv1,
+               int nc1, int nv2, int nc2, int mu_points, double* d_theta, int* piv,
+               int kmeans_max_iter, int selector, int check, const isdf_options_t* opt,
+               isdf_report_t* rep);
+
+/* K-means weight w(r) = sum_{S2} psi^2 * sum_{S1} psi^2, bit-exact with the
+ * reference CPU loop src/cpu/getpoints_Kmeans_MPI.cpp:33-45 (the GPU kernel
+ * it replaces is calculateKmeansWeight, src/cuda/cuda_utils.cu:124-166,553-564).
+ * d_w: device double[ng]. */
+int isdf_kmeans_weight(const double* d_psi, long long ng, int nstate, int nocc, int nv1, int nc1,
+                       int nv2, int nc2, double* d_w, void* stream);
+
+/* K-means interpolation-point selection from a device weight vector
+ * (reference KMEAN, src/common/utility.cpp:631-988). piv: host int[Ng]
+ * (fully written); *rk_eff: distinct points selected; *iters: Lloyd
+ * iterations run (-1 on the npt < mu early return). */
+int isdf_kmeans_select(const isdf_domain_t* dom, const double* d_w, int mu, int max_iter,
+                       long long rand_seed, int* piv, int* rk_eff, int* iters, int* npt,
+                       void* stream);
+
+/* FP64 fit for given pivots (reference src/cuda/isdf-gpu.cpp:112-402 /
+ * src/cpu/getbasis_MPI.cpp:9-250): theta = (Z C^T)(C C^T + eps I)^{-1} with
+ * eps = 1e-10 tr(C C^T)/rk, Z C^T = (psi_S1 psi_S1(mu)^T) o (psi_S2 psi_S2(mu)^T).
+ * piv: host int[>= rk], the first rk entries are the interpolation points.
+ * d_theta: device Ng x rk, ld = Ng. *chol_info > 0 on a non-SPD matrix. */
+int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, int nc1, int nv2,
+             int nc2, int rk, const int* piv, double* d_theta, int precision, int refine_steps,
+             int* chol_info, void* stream);
+
+/* Message for the last error on this thread ("" if none). */
+const char* isdf_last_error(void);
+const char* isdf_status_string(int code);
+
+/* Device memory the solve needs beyond psi and theta, in bytes (the serving
+ * loop admits requests by it). */
+size_t isdf_workspace_bytes(long long ng, int nstate, int mu, int selector, int precision,
+                            int check);
+
+/* Releases the per-device workspace cached by isdf_solve(). */
+void isdf_release_workspace(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ISDF_C_H */

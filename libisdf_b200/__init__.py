@@ -1,0 +1,244 @@
+"""libisdf_b200: a B200-native ISDF engine behind LibISDF's GPU ISDF() interface.
+
+The compute path is libisdf_b200.so (hand-written sm_100a CUDA kernels behind
+the C ABI in include/isdf_c.h). This module binds that ABI with ctypes and
+mirrors the reference's entry point
+
+    isdf::isdffunc::ISDF(d_psirow, domain, nocc, nstate, nv1, nc1, nv2, nc2,
+                         mu_points, d_thetaCol, piv, KmeansMaxIter_ISDF, check)
+
+(reference include/isdf.hpp:37, src/common/isdf.cpp:132-209) with the
+Kmeans/QRCP selector of its CPU overload (isdf.hpp:39). Device buffers are
+torch CUDA tensors (float64, column-major data: a tensor of shape
+(nstate, Ng) row-major is the same bytes as Ng x nstate column-major) or raw
+device pointers; piv is a host int32 numpy array of length Ng.
+
+There is no CPU fallback: if the shared library is missing, importing the
+binding raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libisdf_b200.so")
+
+ISDF_OK = 0
+ISDF_ERR_ARG = -1
+ISDF_ERR_CUDA = -2
+ISDF_ERR_NOMEM = -3
+ISDF_ERR_NOT_SPD = -4
+ISDF_ERR_TIMEOUT = -5
+ISDF_ERR_UNSUPPORTED = -6
+ISDF_ERR_CANCELLED = -7
+ISDF_ERR_BUSY = -8
+
+SELECT_KMEANS = 0
+SELECT_QRCP = 1
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+
+class IsdfError(RuntimeError):
+    """Raised for a non-zero status (the reference throws std::runtime_error)."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+class _Domain(ctypes.Structure):
+    _fields_ = [("length", ctypes.c_double * 3), ("pos_start", ctypes.c_double * 3),
+                ("num_grid", ctypes.c_int * 3), ("num_grid_fine", ctypes.c_int * 3)]
+
+
+class _Options(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("refine_steps", ctypes.c_int),
+                ("qrcp_oversample", ctypes.c_double), ("qrcp_seed", ctypes.c_longlong),
+                ("rand_seed", ctypes.c_longlong), ("stream", ctypes.c_void_p),
+                ("reserved", ctypes.c_int * 8)]
+
+
+class _Report(ctypes.Structure):
+    _fields_ = [("rk_requested", ctypes.c_int), ("rk_eff", ctypes.c_int),
+                ("kmeans_iters", ctypes.c_int), ("npt", ctypes.c_int),
+                ("fit_err", ctypes.c_double), ("coul_err", ctypes.c_double),
+                ("t_select_ms", ctypes.c_double), ("t_fit_ms", ctypes.c_double),
+                ("t_chol_ms", ctypes.c_double), ("t_solve_ms", ctypes.c_double),
+                ("t_check_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double),
+                ("chol_info", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
+
+
+@dataclass
+class Domain:
+    """Numeric fields of the reference's Domain (include/common/domain.hpp:8-36)."""
+
+    length: tuple
+    num_grid: tuple
+    pos_start: tuple = (0.0, 0.0, 0.0)
+    num_grid_fine: tuple | None = None
+
+    def NumGridTotal(self) -> int:
+        return int(self.num_grid[0] * self.num_grid[1] * self.num_grid[2])
+
+    def _c(self) -> _Domain:
+        d = _Domain()
+        for i in range(3):
+            d.length[i] = float(self.length[i])
+            d.pos_start[i] = float(self.pos_start[i])
+            d.num_grid[i] = int(self.num_grid[i])
+            d.num_grid_fine[i] = int((self.num_grid_fine or self.num_grid)[i])
+        return d
+
+
+@dataclass
+class Options:
+    precision: int = PRECISION_FP64
+    refine_steps: int = 2
+    qrcp_oversample: float = 1.5
+    qrcp_seed: int = 41
+    rand_seed: int = -1
+    stream: int = 0
+
+    def _c(self) -> _Options:
+        o = _Options()
+        o.precision = self.precision
+        o.refine_steps = self.refine_steps
+        o.qrcp_oversample = self.qrcp_oversample
+        o.qrcp_seed = self.qrcp_seed
+        o.rand_seed = self.rand_seed
+        o.stream = self.stream or None
+        return o
+
+
+@dataclass
+class Report:
+    rk_requested: int
+    rk_eff: int
+    kmeans_iters: int
+    npt: int
+    fit_err: float
+    coul_err: float
+    t_select_ms: float
+    t_fit_ms: float
+    t_total_ms: float
+    chol_info: int
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded libisdf_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m libisdf_b200.build` "
+                              "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I, LL = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong
+        L.isdf_solve.argtypes = [ctypes.POINTER(_Domain), P, I, I, I, I, I, I, I, P, P, I, I, I,
+                                 ctypes.POINTER(_Options), ctypes.POINTER(_Report)]
+        L.isdf_solve.restype = I
+        L.isdf_kmeans_weight.argtypes = [P, LL, I, I, I, I, I, I, P, P]
+        L.isdf_kmeans_weight.restype = I
+        L.isdf_kmeans_select.argtypes = [ctypes.POINTER(_Domain), P, I, I, LL, P, P, P, P, P]
+        L.isdf_kmeans_select.restype = I
+        L.isdf_fit.argtypes = [P, LL, I, I, I, I, I, I, I, P, P, I, I, P, P]
+        L.isdf_fit.restype = I
+        L.isdf_last_error.restype = ctypes.c_char_p
+        L.isdf_status_string.argtypes = [I]
+        L.isdf_status_string.restype = ctypes.c_char_p
+        L.isdf_workspace_bytes.argtypes = [LL, I, I, I, I, I]
+        L.isdf_workspace_bytes.restype = ctypes.c_size_t
+        L.isdf_default_options.argtypes = [ctypes.POINTER(_Options)]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != ISDF_OK:
+        msg = lib().isdf_last_error().decode(errors="replace")
+        raise IsdfError(rc, msg or lib().isdf_status_string(rc).decode())
+
+
+def _dptr(x) -> int:
+    """Device address of a torch CUDA tensor (or an int address)."""
+    if isinstance(x, int):
+        return x
+    if not getattr(x, "is_cuda", False):
+        raise TypeError("expected a CUDA tensor or a device address")
+    return int(x.data_ptr())
+
+
+def _host_int32(piv, n: int) -> np.ndarray:
+    if not isinstance(piv, np.ndarray) or piv.dtype != np.int32 or not piv.flags.c_contiguous:
+        raise TypeError("piv must be a C-contiguous numpy int32 array (host memory)")
+    if piv.size < n:
+        raise ValueError(f"piv holds {piv.size} entries, needs {n}")
+    return piv
+
+
+def ISDF(d_psirow, domain: Domain, nocc: int, nstate: int, nv1: int, nc1: int, nv2: int,
+         nc2: int, mu_points: int, d_thetaCol, piv: np.ndarray, KmeansMaxIter_ISDF: int,
+         s1: str = "Kmeans", check: bool = False, options: Options | None = None) -> Report:
+    """The reference's GPU ISDF() (src/common/isdf.cpp:132-209) on one B200.
+
+    Writes theta (Ng x mu, column-major) into d_thetaCol and the pivots into
+    the host array piv; raises IsdfError where the reference would throw."""
+    sel = {"Kmeans": SELECT_KMEANS, "QRCP": SELECT_QRCP}.get(s1)
+    if sel is None:
+        raise IsdfError(ISDF_ERR_ARG, "Wrong select points method")
+    n = domain.NumGridTotal()
+    piv = _host_int32(piv, n)
+    d = domain._c()
+    o = (options or Options())._c()
+    r = _Report()
+    rc = lib().isdf_solve(ctypes.byref(d), _dptr(d_psirow), nocc, nstate, nv1, nc1, nv2, nc2,
+                          mu_points, _dptr(d_thetaCol), piv.ctypes.data, KmeansMaxIter_ISDF, sel,
+                          int(bool(check)), ctypes.byref(o), ctypes.byref(r))
+    _check(rc)
+    return Report(r.rk_requested, r.rk_eff, r.kmeans_iters, r.npt, r.fit_err, r.coul_err,
+                  r.t_select_ms, r.t_fit_ms, r.t_total_ms, r.chol_info)
+
+
+def kmeans_weight(d_psi, ng: int, nstate: int, nocc: int, nv1: int, nc1: int, nv2: int, nc2: int,
+                  d_w, stream: int = 0):
+    _check(lib().isdf_kmeans_weight(_dptr(d_psi), ng, nstate, nocc, nv1, nc1, nv2, nc2,
+                                    _dptr(d_w), stream or None))
+
+
+def kmeans_select(domain: Domain, d_w, mu: int, max_iter: int, rand_seed: int = -1,
+                  stream: int = 0):
+    """Returns (piv int32[Ng], rk_eff, iterations, npt)."""
+    n = domain.NumGridTotal()
+    piv = np.zeros(n, dtype=np.int32)
+    out = (ctypes.c_int * 3)()
+    d = domain._c()
+    _check(lib().isdf_kmeans_select(ctypes.byref(d), _dptr(d_w), mu, max_iter, rand_seed,
+                                    piv.ctypes.data, ctypes.addressof(out),
+                                    ctypes.addressof(out) + 4, ctypes.addressof(out) + 8,
+                                    stream or None))
+    return piv, out[0], out[1], out[2]
+
+
+def fit(d_psi, ng: int, nstate: int, nocc: int, nv1: int, nc1: int, nv2: int, nc2: int, rk: int,
+        piv: np.ndarray, d_theta, precision: int = PRECISION_FP64, refine_steps: int = 2,
+        stream: int = 0) -> int:
+    """theta for given pivots; returns the Cholesky info (0 = ok)."""
+    piv = np.ascontiguousarray(piv, dtype=np.int32)
+    info = ctypes.c_int(0)
+    rc = lib().isdf_fit(_dptr(d_psi), ng, nstate, nocc, nv1, nc1, nv2, nc2, rk, piv.ctypes.data,
+                        _dptr(d_theta), precision, refine_steps, ctypes.addressof(info),
+                        stream or None)
+    _check(rc)
+    return info.value
+
+
+def workspace_bytes(ng: int, nstate: int, mu: int, selector: int = SELECT_KMEANS,
+                    precision: int = PRECISION_FP64, check: bool = False) -> int:
+    return int(lib().isdf_workspace_bytes(ng, nstate, mu, selector, precision, int(check)))

@@ -1,0 +1,80 @@
+"""Builds libisdf_b200.so in-tree with nvcc for sm_100a.
+
+    python -m libisdf_b200.build        (or call build())
+
+Every .cu / .cpp file under libisdf_b200/csrc is compiled with
+-gencode arch=compute_100a,code=sm_100a -lineinfo -O3 and linked into
+libisdf_b200/libisdf_b200.so (static CUDA runtime, cuFFT). A rebuild happens
+only when a source or header is newer than the library.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libisdf_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+         "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
+
+
+def _sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
+
+
+def _inputs():
+    return _sources() + sorted(glob.glob(os.path.join(CSRC, "*.h")) +
+                               glob.glob(os.path.join(CSRC, "*.cuh")) +
+                               glob.glob(os.path.join(ROOT, "include", "*.h")) +
+                               glob.glob(os.path.join(ROOT, "include", "*.hpp")))
+
+
+def needs_build() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(f) > t for f in _inputs())
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not needs_build():
+        return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = []
+    procs = []
+    for src in _sources():
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
+        if src.endswith(".cpp"):
+            cmd = [NVCC] + FLAGS + ["-x", "c++", "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+        objs.append(obj)
+    failed = []
+    for src, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            failed.append((src, out.decode(errors="replace")))
+        elif verbose and out:
+            print(out.decode(errors="replace"))
+    if failed:
+        msg = "\n".join(f"{s}:\n{o}" for s, o in failed)
+        raise RuntimeError(f"nvcc failed:\n{msg}")
+    tmp = LIB + ".tmp"
+    cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcufft", "-lcublas"]
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)
+    print(LIB)

@@ -1,0 +1,366 @@
+// C ABI of libisdf_b200 (include/isdf_c.h): argument checks, the per-device
+// workspace, the stream, and the stage order of one ISDF solve.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "arena.h"
+#include "common.cuh"
+#include "fit.h"
+#include "kmeans.h"
+#include "solve.h"
+
+namespace isdf_b200 {
+
+static thread_local std::string g_last_error;
+
+int record_error(int code, const char* msg) {
+  g_last_error = msg ? msg : "";
+  return code;
+}
+
+int record_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+  char buf[512];
+  std::snprintf(buf, sizeof(buf), "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file,
+                line);
+  g_last_error = buf;
+  return e == cudaErrorMemoryAllocation ? ISDF_ERR_NOMEM : ISDF_ERR_CUDA;
+}
+
+const char* last_error_message() { return g_last_error.c_str(); }
+
+// ---------------------------------------------------------------- workspace
+namespace {
+
+constexpr int kMaxDevices = 64;
+struct DeviceCache {
+  std::mutex mu;
+  char* buf = nullptr;
+  size_t cap = 0;
+  cudaStream_t stream = nullptr;
+};
+DeviceCache g_cache[kMaxDevices];
+
+}  // namespace
+
+int device_cache(int* dev_out, DeviceCache** out) {
+  int dev = 0;
+  ISDF_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return record_error(ISDF_ERR_UNSUPPORTED, "device index");
+  *dev_out = dev;
+  *out = &g_cache[dev];
+  return ISDF_OK;
+}
+
+// Grows the cached device buffer of the current device to >= bytes.
+int acquire_workspace(size_t bytes, Arena* arena, cudaStream_t* lib_stream) {
+  int dev;
+  DeviceCache* c = nullptr;
+  ISDF_TRY(device_cache(&dev, &c));
+  if (!c->stream) ISDF_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  if (c->cap < bytes) {
+    if (c->buf) {
+      ISDF_CUDA(cudaDeviceSynchronize());
+      ISDF_CUDA(cudaFree(c->buf));
+      c->buf = nullptr;
+      c->cap = 0;
+    }
+    cudaError_t e = cudaMalloc((void**)&c->buf, bytes);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      return record_error(ISDF_ERR_NOMEM, "workspace allocation failed");
+    }
+    c->cap = bytes;
+  }
+  arena->base = c->buf;
+  arena->cap = c->cap;
+  arena->off = 0;
+  arena->counting = false;
+  if (lib_stream) *lib_stream = c->stream;
+  return ISDF_OK;
+}
+
+std::mutex& workspace_mutex() {
+  int dev = 0;
+  (void)cudaGetDevice(&dev);
+  if (dev < 0 || dev >= kMaxDevices) dev = 0;
+  return g_cache[dev].mu;
+}
+
+static double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// IRound of include/common/utility.hpp:18-23.
+int iround(double a) {
+  int b = 0;
+  if (a > 0) b = (a - (int)a < 0.5) ? (int)a : ((int)a + 1);
+  else b = ((int)a - a < 0.5) ? (int)a : ((int)a - 1);
+  return b;
+}
+
+int default_mu(int nv1, int nc1, int nv2, int nc2) {
+  return iround(std::sqrt((double)((nc1 + nv1) * (nc2 + nv2))) * 8.0);
+}
+
+int check_state_ranges(int nocc, int nstate, int nv1, int nc1, int nv2, int nc2) {
+  if (nstate <= 0 || nv1 < 0 || nc1 < 0 || nv2 < 0 || nc2 < 0)
+    return record_error(ISDF_ERR_ARG, "negative state counts");
+  if (nv1 + nc1 <= 0 || nv2 + nc2 <= 0) return record_error(ISDF_ERR_ARG, "empty state sets");
+  if (nocc - nv1 < 0 || nocc + nc1 > nstate || nocc - nv2 < 0 || nocc + nc2 > nstate)
+    return record_error(ISDF_ERR_ARG, "state window outside [0, nstate)");
+  return ISDF_OK;
+}
+
+size_t solve_workspace_bytes(long long ng, int nstate, int mu, int selector, int precision,
+                             int check) {
+  (void)selector;
+  (void)precision;
+  (void)check;
+  Arena a;
+  a.counting = true;
+  a.take<double>((size_t)ng);  // weight
+  size_t sel = kmeans_workspace_bytes(ng, mu);
+  size_t fit = fit_workspace_bytes(ng, nstate, mu);
+  return a.off + (sel > fit ? sel : fit) + 4096;
+}
+
+int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, int nv1, int nc1,
+          int nv2, int nc2, int mu_points, double* d_theta, int* piv, int kmeans_max_iter,
+          int selector, int check, const isdf_options_t* opt_in, isdf_report_t* rep_out) {
+  auto t0 = std::chrono::steady_clock::now();
+  isdf_options_t opt;
+  isdf_default_options(&opt);
+  if (opt_in) opt = *opt_in;
+  isdf_report_t rep;
+  std::memset(&rep, 0, sizeof(rep));
+  if (!dom || !d_psi || !d_theta || !piv) return record_error(ISDF_ERR_ARG, "null pointer");
+  const long long ng = (long long)dom->num_grid[0] * dom->num_grid[1] * dom->num_grid[2];
+  if (dom->num_grid[0] <= 0 || dom->num_grid[1] <= 0 || dom->num_grid[2] <= 0)
+    return record_error(ISDF_ERR_ARG, "empty grid");
+  ISDF_TRY(check_state_ranges(nocc, nstate, nv1, nc1, nv2, nc2));
+  if (kmeans_max_iter < 0) return record_error(ISDF_ERR_ARG, "negative K-means iteration cap");
+  const int rk = mu_points == 0 ? default_mu(nv1, nc1, nv2, nc2) : mu_points;
+  if (rk <= 0 || rk > ng) return record_error(ISDF_ERR_ARG, "mu outside [1, Ng]");
+  if (selector != ISDF_SELECT_KMEANS && selector != ISDF_SELECT_QRCP)
+    return record_error(ISDF_ERR_ARG, "unknown selector");
+  if (selector == ISDF_SELECT_QRCP)
+    return record_error(ISDF_ERR_UNSUPPORTED, "QRCP selector not built yet");
+  if (opt.precision != ISDF_PRECISION_FP64)
+    return record_error(ISDF_ERR_UNSUPPORTED, "mixed precision not built yet");
+  if (check) return record_error(ISDF_ERR_UNSUPPORTED, "check not built yet");
+  if (rk > kKmeansMaxMu) return record_error(ISDF_ERR_UNSUPPORTED, "mu above the K-means limit");
+  rep.rk_requested = rk;
+
+  std::lock_guard<std::mutex> lock(workspace_mutex());
+  Arena arena;
+  cudaStream_t lib_stream;
+  ISDF_TRY(acquire_workspace(solve_workspace_bytes(ng, nstate, rk, selector, opt.precision, check),
+                             &arena, &lib_stream));
+  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : lib_stream;
+  double* d_w = arena.take<double>((size_t)ng);
+  const size_t mark = arena.off;
+
+  // (a) K-means selection
+  KmeansArgs ka;
+  ka.d_w = d_w;
+  ka.ng = ng;
+  for (int i = 0; i < 3; ++i) {
+    ka.num_grid[i] = dom->num_grid[i];
+    ka.length[i] = dom->length[i];
+  }
+  ka.mu = rk;
+  ka.max_iter = kmeans_max_iter;
+  ka.rand_seed = opt.rand_seed;
+  ka.piv = piv;
+  ISDF_TRY(kmeans_weight(d_psi, ng, nocc, nv1, nc1, nv2, nc2, d_w, s));
+  KmeansResult kr;
+  ISDF_TRY(kmeans_select(ka, arena, s, &kr));
+  rep.rk_eff = kr.rk_eff;
+  rep.kmeans_iters = kr.iters;
+  rep.npt = kr.npt;
+  rep.t_select_ms = ms_since(t0);
+
+  // (c, d) fit with the selected points (the GPU path fits with the shrunk
+  // rk, isdf-gpu.cpp:12,99); columns past rk_eff are zero-filled.
+  auto t1 = std::chrono::steady_clock::now();
+  arena.off = mark;
+  FitArgs fa;
+  fa.d_psi = d_psi;
+  fa.ng = ng;
+  fa.nstate = nstate;
+  fa.nocc = nocc;
+  fa.nv1 = nv1;
+  fa.nc1 = nc1;
+  fa.nv2 = nv2;
+  fa.nc2 = nc2;
+  fa.rk = kr.rk_eff;
+  fa.piv = piv;
+  fa.d_theta = d_theta;
+  FitResult fr;
+  int rc = fit_fp64(fa, arena, s, &fr);
+  rep.chol_info = fr.chol_info;
+  if (rc != ISDF_OK) {
+    if (rep_out) *rep_out = rep;
+    return rc;
+  }
+  if (kr.rk_eff < rk)
+    ISDF_CUDA(cudaMemsetAsync(d_theta + (size_t)kr.rk_eff * ng, 0,
+                              sizeof(double) * (size_t)(rk - kr.rk_eff) * ng, s));
+  ISDF_CUDA(cudaStreamSynchronize(s));
+  rep.t_fit_ms = ms_since(t1);
+  rep.t_total_ms = ms_since(t0);
+  if (rep_out) *rep_out = rep;
+  return ISDF_OK;
+}
+
+}  // namespace isdf_b200
+
+using namespace isdf_b200;
+
+extern "C" {
+
+void isdf_default_options(isdf_options_t* opt) {
+  if (!opt) return;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->precision = ISDF_PRECISION_FP64;
+  opt->refine_steps = 2;
+  opt->qrcp_oversample = 1.5;
+  opt->qrcp_seed = 41;
+  opt->rand_seed = -1;
+  opt->stream = nullptr;
+}
+
+int isdf_solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, int nv1,
+               int nc1, int nv2, int nc2, int mu_points, double* d_theta, int* piv,
+               int kmeans_max_iter, int selector, int check, const isdf_options_t* opt,
+               isdf_report_t* rep) {
+  try {
+    return solve(dom, d_psi, nocc, nstate, nv1, nc1, nv2, nc2, mu_points, d_theta, piv,
+                 kmeans_max_iter, selector, check, opt, rep);
+  } catch (const std::exception& e) {
+    return record_error(ISDF_ERR_NOMEM, e.what());
+  } catch (...) {
+    return record_error(ISDF_ERR_CUDA, "unknown exception");
+  }
+}
+
+int isdf_kmeans_weight(const double* d_psi, long long ng, int nstate, int nocc, int nv1, int nc1,
+                       int nv2, int nc2, double* d_w, void* stream) {
+  if (!d_psi || !d_w || ng <= 0) return record_error(ISDF_ERR_ARG, "bad weight arguments");
+  ISDF_TRY(check_state_ranges(nocc, nstate, nv1, nc1, nv2, nc2));
+  return kmeans_weight(d_psi, ng, nocc, nv1, nc1, nv2, nc2, d_w, (cudaStream_t)stream);
+}
+
+int isdf_kmeans_select(const isdf_domain_t* dom, const double* d_w, int mu, int max_iter,
+                       long long rand_seed, int* piv, int* rk_eff, int* iters, int* npt,
+                       void* stream) {
+  try {
+    if (!dom || !d_w || !piv) return record_error(ISDF_ERR_ARG, "null pointer");
+    const long long ng = (long long)dom->num_grid[0] * dom->num_grid[1] * dom->num_grid[2];
+    if (ng <= 0 || mu <= 0 || mu > ng || max_iter < 0) return record_error(ISDF_ERR_ARG, "sizes");
+    if (mu > kKmeansMaxMu) return record_error(ISDF_ERR_UNSUPPORTED, "mu above the K-means limit");
+    std::lock_guard<std::mutex> lock(workspace_mutex());
+    Arena arena;
+    cudaStream_t ls;
+    ISDF_TRY(acquire_workspace(kmeans_workspace_bytes(ng, mu) + 4096, &arena, &ls));
+    KmeansArgs ka;
+    ka.d_w = d_w;
+    ka.ng = ng;
+    for (int i = 0; i < 3; ++i) {
+      ka.num_grid[i] = dom->num_grid[i];
+      ka.length[i] = dom->length[i];
+    }
+    ka.mu = mu;
+    ka.max_iter = max_iter;
+    ka.rand_seed = rand_seed;
+    ka.piv = piv;
+    KmeansResult kr;
+    ISDF_TRY(kmeans_select(ka, arena, stream ? (cudaStream_t)stream : ls, &kr));
+    if (rk_eff) *rk_eff = kr.rk_eff;
+    if (iters) *iters = kr.iters;
+    if (npt) *npt = kr.npt;
+    return ISDF_OK;
+  } catch (const std::exception& e) {
+    return record_error(ISDF_ERR_NOMEM, e.what());
+  }
+}
+
+int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, int nc1, int nv2,
+             int nc2, int rk, const int* piv, double* d_theta, int precision, int refine_steps,
+             int* chol_info, void* stream) {
+  (void)refine_steps;
+  try {
+    if (!d_psi || !d_theta || !piv || ng <= 0 || rk <= 0 || rk > ng)
+      return record_error(ISDF_ERR_ARG, "bad fit arguments");
+    ISDF_TRY(check_state_ranges(nocc, nstate, nv1, nc1, nv2, nc2));
+    for (int j = 0; j < rk; ++j)
+      if (piv[j] < 0 || piv[j] >= ng) return record_error(ISDF_ERR_ARG, "pivot outside the grid");
+    if (precision != ISDF_PRECISION_FP64)
+      return record_error(ISDF_ERR_UNSUPPORTED, "mixed precision not built yet");
+    std::lock_guard<std::mutex> lock(workspace_mutex());
+    Arena arena;
+    cudaStream_t ls;
+    ISDF_TRY(acquire_workspace(fit_workspace_bytes(ng, nstate, rk) + 4096, &arena, &ls));
+    FitArgs fa;
+    fa.d_psi = d_psi;
+    fa.ng = ng;
+    fa.nstate = nstate;
+    fa.nocc = nocc;
+    fa.nv1 = nv1;
+    fa.nc1 = nc1;
+    fa.nv2 = nv2;
+    fa.nc2 = nc2;
+    fa.rk = rk;
+    fa.piv = piv;
+    fa.d_theta = d_theta;
+    FitResult fr;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ls;
+    int rc = fit_fp64(fa, arena, s, &fr);
+    if (chol_info) *chol_info = fr.chol_info;
+    if (rc == ISDF_OK) ISDF_CUDA(cudaStreamSynchronize(s));
+    return rc;
+  } catch (const std::exception& e) {
+    return record_error(ISDF_ERR_NOMEM, e.what());
+  }
+}
+
+const char* isdf_last_error(void) { return last_error_message(); }
+
+const char* isdf_status_string(int code) {
+  switch (code) {
+    case ISDF_OK: return "ok";
+    case ISDF_ERR_ARG: return "invalid argument";
+    case ISDF_ERR_CUDA: return "CUDA error";
+    case ISDF_ERR_NOMEM: return "out of device memory";
+    case ISDF_ERR_NOT_SPD: return "C C^T + eps I is not positive definite";
+    case ISDF_ERR_TIMEOUT: return "device wait timed out";
+    case ISDF_ERR_UNSUPPORTED: return "unsupported shape or option";
+    case ISDF_ERR_CANCELLED: return "cancelled";
+    case ISDF_ERR_BUSY: return "queue full";
+    default: return "unknown status";
+  }
+}
+
+size_t isdf_workspace_bytes(long long ng, int nstate, int mu, int selector, int precision,
+                            int check) {
+  return solve_workspace_bytes(ng, nstate, mu, selector, precision, check);
+}
+
+void isdf_release_workspace(void) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return;
+  std::lock_guard<std::mutex> lock(g_cache[dev].mu);
+  if (g_cache[dev].buf) {
+    cudaDeviceSynchronize();
+    cudaFree(g_cache[dev].buf);
+  }
+  g_cache[dev].buf = nullptr;
+  g_cache[dev].cap = 0;
+}
+
+}  // extern "C"

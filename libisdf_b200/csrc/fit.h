@@ -1,0 +1,27 @@
+// Host-side entry points of the fit (fit.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "arena.h"
+
+namespace isdf_b200 {
+
+struct FitArgs {
+  const double* d_psi;  // Ng x nstate, ld = Ng
+  long long ng;
+  int nstate, nocc, nv1, nc1, nv2, nc2;
+  int rk;
+  const int* piv;   // host, first rk entries used
+  double* d_theta;  // Ng x rk, ld = Ng
+};
+
+struct FitResult {
+  int chol_info = 0;
+};
+
+size_t fit_workspace_bytes(long long ng, int nstate, int rk);
+int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t stream, FitResult* res);
+
+}  // namespace isdf_b200

@@ -1,0 +1,691 @@
+// Density-weighted K-means interpolation-point selection on sm_100a.
+//
+// Reproduces the reference's CPU KMEAN (src/common/utility.cpp:631-988) bit
+// for bit at one rank: every FP64 operation is an explicitly rounded add /
+// sub / mul / div (no FMA contraction, like the reference's SSE2 x86-64
+// build), the centroid sums are folded in point-index order per cluster, and
+// every argmin keeps the first minimum. The reference's own GPU kernels
+// (src/cuda/cuda_utils.cu:124-234,368-428) materialise an Npt x mu distance
+// matrix and FMA-contract the distance; here the distance matrix is never
+// stored and the arithmetic follows the CPU path.
+//
+// Device data layout (SoA, one entry per K-means point p in [0, Ng)):
+//   pidx[p]   grid index of point p: the kept points ascending, then the
+//             zero tail that aliases grid point 0 (utility.cpp:648,659,707);
+//   px,py,pz  coordinates by the formula of utility.cpp:711-713;
+//   pw        weight w[pidx[p]];
+//   label[p]  nearest centroid.
+// Centroids: double4 (x, y, z, 0) in cen[], rk on the device in st->rk.
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "arena.h"
+#include "common.cuh"
+#include "kmeans.h"
+
+namespace isdf_b200 {
+
+namespace {
+
+constexpr int kTile = 4096;      // points per counting-sort tile
+constexpr int kFinalChunk = 4096;  // points per partial argmin chunk
+constexpr int kIterChunk = 8;    // Lloyd iterations launched between host checks
+
+struct KmState {
+  int s;        // Lloyd iterations completed
+  int flag;     // labels changed in the last assignment
+  int changed;  // accumulator for the running assignment
+  int done;
+  int rk;       // current number of centroids
+  int npt;      // kept points
+  int any_empty;
+  int pad;
+  unsigned long long maxw_bits;
+};
+
+// ---------------------------------------------------------------- weight
+// w(r) = 0 + (sum_{S2} psi^2) * (sum_{S1} psi^2), each sum a sequential fold
+// over the states in increasing order (getpoints_Kmeans_MPI.cpp:37-45).
+// One thread per grid point; a warp reads 32 consecutive doubles of a column.
+__global__ void __launch_bounds__(256) k_weight(const double* __restrict__ psi, long long ng,
+                                                int s2lo, int s2hi, int s1lo, int s1hi, int same,
+                                                double* __restrict__ w) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < ng; r += stride) {
+    const double* p = psi + r;
+    double si = 0.0;
+#pragma unroll 8
+    for (int i = s2lo; i < s2hi; ++i) {
+      double v = __ldg(p + (long long)i * ng);
+      si = radd(si, rmul(v, v));
+    }
+    double sj = si;
+    if (!same) {
+      sj = 0.0;
+#pragma unroll 8
+      for (int j = s1lo; j < s1hi; ++j) {
+        double v = __ldg(p + (long long)j * ng);
+        sj = radd(sj, rmul(v, v));
+      }
+    }
+    w[r] = radd(0.0, rmul(si, sj));
+  }
+}
+
+// ---------------------------------------------------------------- filter
+// maxW = max(0, max_r w(r)) (findMax starts at 0.0). Non-negative doubles
+// order like their bit patterns, so an integer atomicMax is exact.
+__global__ void k_maxw(const double* __restrict__ w, long long n, KmState* st) {
+  double m = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    m = fmax(m, w[i]);
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.0)
+    atomicMax(&st->maxw_bits, (unsigned long long)__double_as_longlong(m));
+}
+
+__device__ __forceinline__ bool kept(double wv, double thr) { return wv > thr; }
+
+// Per-tile count of kept points (tile = blockDim.x * 4 points).
+__global__ void __launch_bounds__(256) k_filter_count(const double* __restrict__ w, long long n,
+                                                      const KmState* st, int* tile_cnt) {
+  const double thr = rmul(1e-8, __longlong_as_double((long long)st->maxw_bits));
+  __shared__ int warp_cnt[8];
+  long long base = (long long)blockIdx.x * 1024;
+  int c = 0;
+  for (int k = 0; k < 4; ++k) {
+    long long i = base + k * 256 + threadIdx.x;
+    if (i < n && kept(w[i], thr)) ++c;
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) warp_cnt[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int k = 0; k < 8; ++k) t += warp_cnt[k];
+    tile_cnt[blockIdx.x] = t;
+  }
+}
+
+// Exclusive scan of ntiles counts in one block; writes npt.
+__global__ void __launch_bounds__(1024) k_scan_small(int* cnt, int ntiles, int* total) {
+  __shared__ int part[1024];
+  const int per = (ntiles + 1023) / 1024;
+  const int lo = threadIdx.x * per, hi = min(lo + per, ntiles);
+  int s = 0;
+  for (int i = lo; i < hi; ++i) s += cnt[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+  for (int i = lo; i < hi; ++i) {
+    int v = cnt[i];
+    cnt[i] = run;
+    run += v;
+  }
+  if (threadIdx.x == 1023) *total = part[1023];
+}
+
+// Order-preserving compaction of the kept grid indices into pidx[0..npt);
+// pidx[npt..n) was zeroed before (the reference's zero-initialised tail).
+__global__ void __launch_bounds__(256) k_filter_scatter(const double* __restrict__ w, long long n,
+                                                        const KmState* st, const int* tile_off,
+                                                        int* __restrict__ pidx) {
+  const double thr = rmul(1e-8, __longlong_as_double((long long)st->maxw_bits));
+  __shared__ int warp_cnt[8][4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  long long base = (long long)blockIdx.x * 1024;
+  unsigned ballots[4];
+  for (int k = 0; k < 4; ++k) {
+    long long i = base + k * 256 + threadIdx.x;
+    bool f = i < n && kept(w[i], thr);
+    ballots[k] = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) warp_cnt[wid][k] = __popc(ballots[k]);
+  }
+  __syncthreads();
+  // order of elements: k-major, then warp, then lane
+  int off = tile_off[blockIdx.x];
+  for (int k = 0; k < 4; ++k) {
+    int before = 0;
+    for (int kk = 0; kk < k; ++kk)
+      for (int ww = 0; ww < 8; ++ww) before += warp_cnt[ww][kk];
+    for (int ww = 0; ww < wid; ++ww) before += warp_cnt[ww][k];
+    long long i = base + k * 256 + threadIdx.x;
+    if (ballots[k] & (1u << lane)) {
+      int r = __popc(ballots[k] & ((1u << lane) - 1u));
+      pidx[off + before + r] = (int)i;
+    }
+  }
+}
+
+// Point coordinates and weights (utility.cpp:707-713); the centroids start
+// at the first rk kept points (utility.cpp:750-762), i.e. points 0..rk-1.
+__global__ void k_points(const int* __restrict__ pidx, const double* __restrict__ w, int n,
+                         int nx, int ny, double dx0, double dx1, double dx2,
+                         double* __restrict__ px, double* __restrict__ py,
+                         double* __restrict__ pz, double* __restrict__ pw, int rk,
+                         double4* __restrict__ cen) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    int t = pidx[p];
+    double gx = rmul((double)(t % nx), dx0);
+    double gy = rmul(rdiv(rsub((double)(t % (nx * ny)), rdiv(gx, dx0)), (double)nx), dx1);
+    double gz = rmul(rdiv(rsub(rsub((double)t, rdiv(gx, dx0)), rmul(rdiv(gy, dx1), (double)nx)),
+                          (double)(nx * ny)),
+                     dx2);
+    px[p] = gx;
+    py[p] = gy;
+    pz[p] = gz;
+    pw[p] = w[t];
+    if (p < rk) cen[p] = make_double4(gx, gy, gz, 0.0);
+  }
+}
+
+// ---------------------------------------------------------------- assign
+// d = ((dx*dx + dy*dy) + dz*dz) with dx = point - centroid (pdist2,
+// utility.cpp:598-615); label = first centroid reaching the minimum
+// (findMin Dim=1, utility.cpp:579-595). Centroids are staged in shared memory
+// in chunks; each thread owns kPPT points.
+constexpr int kAssignThreads = 256;
+constexpr int kPPT = 2;
+constexpr int kCenChunk = 1024;
+
+__global__ void __launch_bounds__(kAssignThreads) k_assign(
+    const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
+    int n, const double4* __restrict__ cen, KmState* st, int* __restrict__ label, int count) {
+  if (st->done) return;
+  const int rk = st->rk;
+  __shared__ double4 sc[kCenChunk];
+  double x[kPPT], y[kPPT], z[kPPT], best[kPPT];
+  int bj[kPPT];
+  const int p0 = blockIdx.x * kAssignThreads * kPPT + threadIdx.x;
+#pragma unroll
+  for (int k = 0; k < kPPT; ++k) {
+    int p = p0 + k * kAssignThreads;
+    bool ok = p < n;
+    x[k] = ok ? px[p] : 0.0;
+    y[k] = ok ? py[p] : 0.0;
+    z[k] = ok ? pz[p] : 0.0;
+    best[k] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+    bj[k] = 0;
+  }
+  for (int c0 = 0; c0 < rk; c0 += kCenChunk) {
+    const int m = min(kCenChunk, rk - c0);
+    __syncthreads();
+    for (int j = threadIdx.x; j < m; j += kAssignThreads) sc[j] = cen[c0 + j];
+    __syncthreads();
+    for (int j = 0; j < m; ++j) {
+      const double4 c = sc[j];
+#pragma unroll
+      for (int k = 0; k < kPPT; ++k) {
+        double d1 = rsub(x[k], c.x), d2 = rsub(y[k], c.y), d3 = rsub(z[k], c.z);
+        double d = radd(radd(rmul(d1, d1), rmul(d2, d2)), rmul(d3, d3));
+        if (d < best[k]) {
+          best[k] = d;
+          bj[k] = c0 + j;
+        }
+      }
+    }
+  }
+  int changed = 0;
+#pragma unroll
+  for (int k = 0; k < kPPT; ++k) {
+    int p = p0 + k * kAssignThreads;
+    if (p < n) {
+      if (count && label[p] != bj[k]) ++changed;
+      label[p] = bj[k];
+    }
+  }
+  if (count) {
+    for (int o = 16; o > 0; o >>= 1) changed += __shfl_xor_sync(0xffffffffu, changed, o);
+    if ((threadIdx.x & 31) == 0 && changed) atomicAdd(&st->changed, changed);
+  }
+}
+
+// ---------------------------------------------------------------- control
+__global__ void k_iter_begin(KmState* st, double max_f, int max_iter) {
+  if (st->done) return;
+  if (!((double)st->flag > max_f && st->s < max_iter)) {
+    st->done = 1;
+    return;
+  }
+  st->changed = 0;
+  st->any_empty = 0;
+}
+
+__global__ void k_iter_end(KmState* st) {
+  if (st->done) return;
+  st->flag = st->changed;
+  st->s += 1;
+}
+
+// ---------------------------------------------------------------- update
+// Stable counting sort of the points by label (tiles of kTile points), then
+// one warp per cluster folds w, w*x, w*y, w*z over the members in increasing
+// point index: the exact sequence of additions of utility.cpp:816-822.
+__global__ void __launch_bounds__(256) k_hist(const int* __restrict__ label, int n,
+                                              const KmState* st, int* __restrict__ hist) {
+  if (st->done) return;
+  extern __shared__ int sh[];
+  const int rk = st->rk;
+  for (int l = threadIdx.x; l < rk; l += blockDim.x) sh[l] = 0;
+  __syncthreads();
+  const int base = blockIdx.x * kTile;
+  const int end = min(base + kTile, n);
+  for (int p = base + threadIdx.x; p < end; p += blockDim.x) atomicAdd(&sh[label[p]], 1);
+  __syncthreads();
+  int* row = hist + (size_t)blockIdx.x * rk;
+  for (int l = threadIdx.x; l < rk; l += blockDim.x) row[l] = sh[l];
+}
+
+// Per label: exclusive scan over tiles (in place) and the member count.
+__global__ void __launch_bounds__(256) k_hist_scan(int* __restrict__ hist, int ntiles,
+                                                   const KmState* st, int* __restrict__ members) {
+  if (st->done) return;
+  const int rk = st->rk;
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= rk) return;
+  int run = 0;
+  for (int t = 0; t < ntiles; ++t) {
+    int v = hist[(size_t)t * rk + l];
+    hist[(size_t)t * rk + l] = run;
+    run += v;
+  }
+  members[l] = run;
+}
+
+// Exclusive scan of the member counts (one block): start[l].
+__global__ void __launch_bounds__(1024) k_label_start(const int* __restrict__ members,
+                                                      const KmState* st, int* __restrict__ start) {
+  if (st->done) return;
+  __shared__ int part[1024];
+  const int rk = st->rk;
+  const int per = (rk + 1023) / 1024;
+  const int lo = threadIdx.x * per, hi = min(lo + per, rk);
+  int s = 0;
+  for (int i = lo; i < hi; ++i) s += members[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+  for (int i = lo; i < hi; ++i) {
+    start[i] = run;
+    run += members[i];
+  }
+}
+
+// One warp per tile: scatters the tile's points to their stable positions.
+__global__ void __launch_bounds__(32) k_scatter(const int* __restrict__ label, int n,
+                                                const KmState* st, const int* __restrict__ hist,
+                                                const int* __restrict__ start,
+                                                int* __restrict__ sorted) {
+  if (st->done) return;
+  extern __shared__ int run[];
+  const int rk = st->rk;
+  const int lane = threadIdx.x;
+  const int* row = hist + (size_t)blockIdx.x * rk;
+  for (int l = lane; l < rk; l += 32) run[l] = start[l] + row[l];
+  __syncwarp();
+  const int base = blockIdx.x * kTile;
+  const int end = min(base + kTile, n);
+  for (int c = base; c < end; c += 32) {
+    const int p = c + lane;
+    const bool ok = p < end;
+    const int l = ok ? label[p] : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, l);
+    const int b = ok ? run[l] : 0;
+    __syncwarp();
+    if (ok) {
+      const int r = __popc(peers & ((1u << lane) - 1u));
+      sorted[b + r] = p;
+      if (lane == __ffs(peers) - 1) run[l] = b + __popc(peers);
+    }
+    __syncwarp();
+  }
+}
+
+// One warp per cluster: sequential fold over the members (in index order).
+__global__ void __launch_bounds__(256) k_segsum(const int* __restrict__ sorted,
+                                                const int* __restrict__ start,
+                                                const int* __restrict__ members,
+                                                const double* __restrict__ px,
+                                                const double* __restrict__ py,
+                                                const double* __restrict__ pz,
+                                                const double* __restrict__ pw, KmState* st,
+                                                double4* __restrict__ sums) {
+  if (st->done) return;
+  const int rk = st->rk;
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= rk) return;
+  const int s0 = start[c], m = members[c];
+  double aw = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
+  for (int q = 0; q < m; q += 32) {
+    double vw = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
+    if (q + lane < m) {
+      const int p = sorted[s0 + q + lane];
+      vw = pw[p];
+      vx = rmul(vw, px[p]);
+      vy = rmul(vw, py[p]);
+      vz = rmul(vw, pz[p]);
+    }
+    const int cnt = min(32, m - q);
+    for (int k = 0; k < cnt; ++k) {
+      aw = radd(aw, __shfl_sync(0xffffffffu, vw, k));
+      ax = radd(ax, __shfl_sync(0xffffffffu, vx, k));
+      ay = radd(ay, __shfl_sync(0xffffffffu, vy, k));
+      az = radd(az, __shfl_sync(0xffffffffu, vz, k));
+    }
+  }
+  if (lane == 0) {
+    sums[c] = make_double4(ax, ay, az, aw);
+    if (aw == 0.0) st->any_empty = 1;
+  }
+}
+
+// New centroids = sums / count; an empty cluster takes the last centroid's
+// sums and rk shrinks (utility.cpp:831-853).
+__global__ void __launch_bounds__(1024) k_centroids(double4* __restrict__ sums, KmState* st,
+                                                    double4* __restrict__ cen) {
+  if (st->done) return;
+  int rk = st->rk;
+  if (!st->any_empty) {
+    for (int i = threadIdx.x; i < rk; i += blockDim.x) {
+      double4 s = sums[i];
+      cen[i] = make_double4(rdiv(s.x, s.w), rdiv(s.y, s.w), rdiv(s.z, s.w), 0.0);
+    }
+    return;
+  }
+  if (threadIdx.x != 0) return;
+  for (int i = 0; i < rk; i++) {
+    double4 s = sums[i];
+    if (s.w != 0.0) {
+      sums[i] = make_double4(rdiv(s.x, s.w), rdiv(s.y, s.w), rdiv(s.z, s.w), s.w);
+    } else {
+      rk--;
+      sums[i] = sums[rk];
+      i--;
+    }
+  }
+  for (int i = 0; i < rk; i++) {
+    double4 s = sums[i];
+    cen[i] = make_double4(s.x, s.y, s.z, 0.0);
+  }
+  st->rk = rk;
+}
+
+// ---------------------------------------------------------------- final
+// Nearest point to every centroid: first minimum over points
+// (std::min_element, utility.cpp:926-945). Partial minima per point chunk,
+// then an in-order reduction over the chunks.
+__global__ void __launch_bounds__(128) k_final_partial(const double* __restrict__ px,
+                                                       const double* __restrict__ py,
+                                                       const double* __restrict__ pz, int n,
+                                                       const double4* __restrict__ cen,
+                                                       const KmState* st,
+                                                       double* __restrict__ part_d,
+                                                       int* __restrict__ part_i) {
+  const int rk = st->rk;
+  const int j = blockIdx.x * 128 + threadIdx.x;
+  const int chunk = blockIdx.y;
+  __shared__ double sx[512], sy[512], sz[512];
+  double cx = 0, cy = 0, cz = 0;
+  if (j < rk) {
+    double4 c = cen[j];
+    cx = c.x;
+    cy = c.y;
+    cz = c.z;
+  }
+  double best = __longlong_as_double(0x7ff0000000000000LL);
+  int bi = 0x7fffffff;
+  const int base = chunk * kFinalChunk;
+  const int end = min(base + kFinalChunk, n);
+  for (int p0 = base; p0 < end; p0 += 512) {
+    const int m = min(512, end - p0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < m; k += 128) {
+      sx[k] = px[p0 + k];
+      sy[k] = py[p0 + k];
+      sz[k] = pz[p0 + k];
+    }
+    __syncthreads();
+    for (int k = 0; k < m; ++k) {
+      double d1 = rsub(sx[k], cx), d2 = rsub(sy[k], cy), d3 = rsub(sz[k], cz);
+      double d = radd(radd(rmul(d1, d1), rmul(d2, d2)), rmul(d3, d3));
+      if (d < best) {
+        best = d;
+        bi = p0 + k;
+      }
+    }
+  }
+  if (j < rk) {
+    part_d[(size_t)chunk * rk + j] = best;
+    part_i[(size_t)chunk * rk + j] = bi;
+  }
+}
+
+__global__ void k_final_reduce(const double* __restrict__ part_d, const int* __restrict__ part_i,
+                               int nchunks, const KmState* st, const int* __restrict__ pidx,
+                               int* __restrict__ sel) {
+  const int rk = st->rk;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= rk) return;
+  double best = __longlong_as_double(0x7ff0000000000000LL);
+  int bi = 0;
+  for (int c = 0; c < nchunks; ++c) {
+    double d = part_d[(size_t)c * rk + j];
+    if (d < best) {
+      best = d;
+      bi = part_i[(size_t)c * rk + j];
+    }
+  }
+  sel[j] = pidx[bi];
+}
+
+struct KmBuffers {
+  int* pidx;
+  double *px, *py, *pz, *pw;
+  int* label;
+  int* sorted;
+  int* hist;
+  int* members;
+  int* start;
+  int* tile_cnt;
+  double4* cen;
+  double4* sums;
+  double* part_d;
+  int* part_i;
+  int* sel;
+  KmState* st;
+};
+
+KmBuffers carve(Arena& a, int n, int mu) {
+  KmBuffers b;
+  const int ntiles = (n + kTile - 1) / kTile;
+  const int nfilter = (n + 1023) / 1024;
+  const int nchunks = (n + kFinalChunk - 1) / kFinalChunk;
+  b.pidx = a.take<int>(n);
+  b.px = a.take<double>(n);
+  b.py = a.take<double>(n);
+  b.pz = a.take<double>(n);
+  b.pw = a.take<double>(n);
+  b.label = a.take<int>(n);
+  b.sorted = a.take<int>(n);
+  b.hist = a.take<int>((size_t)ntiles * mu);
+  b.members = a.take<int>(mu);
+  b.start = a.take<int>(mu);
+  b.tile_cnt = a.take<int>(nfilter);
+  b.cen = a.take<double4>(mu);
+  b.sums = a.take<double4>(mu);
+  b.part_d = a.take<double>((size_t)nchunks * mu);
+  b.part_i = a.take<int>((size_t)nchunks * mu);
+  b.sel = a.take<int>(mu);
+  b.st = a.take<KmState>(1);
+  return b;
+}
+
+}  // namespace
+
+size_t kmeans_workspace_bytes(long long ng, int mu) {
+  Arena a;
+  a.counting = true;
+  carve(a, (int)ng, mu);
+  return a.off;
+}
+
+int kmeans_weight(const double* d_psi, long long ng, int nocc, int nv1, int nc1, int nv2, int nc2,
+                  double* d_w, cudaStream_t stream) {
+  const int same = (nv1 == nv2 && nc1 == nc2);
+  unsigned grid = grid_for(ng, 256);
+  if (grid > (unsigned)kNumSMs * 16) grid = kNumSMs * 16;
+  k_weight<<<grid, 256, 0, stream>>>(d_psi, ng, nocc - nv2, nocc + nc2, nocc - nv1, nocc + nc1,
+                                     same, d_w);
+  ISDF_CHECK_LAUNCH();
+  return ISDF_OK;
+}
+
+// libstdc++'s std::random_shuffle(first, last) loop, driven by std::rand(),
+// which the reference calls on its npt < mu branch (utility.cpp:679).
+static void shuffle_like_libstdcxx(int* first, int* last) {
+  if (first == last) return;
+  for (int* i = first + 1; i != last; ++i) {
+    int* j = first + std::rand() % ((i - first) + 1);
+    if (i != j) std::swap(*i, *j);
+  }
+}
+
+int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, KmeansResult* res) {
+  const int n = (int)args.ng;
+  const int mu = args.mu;
+  if (n <= 0 || mu <= 0 || mu > kKmeansMaxMu) return record_error(ISDF_ERR_ARG, "kmeans: bad n/mu");
+  if (args.ng > 0x7fffffffLL) return record_error(ISDF_ERR_UNSUPPORTED, "kmeans: Ng >= 2^31");
+  KmBuffers b = carve(arena, n, mu);
+  if (arena.overflowed()) return record_error(ISDF_ERR_NOMEM, "kmeans: workspace too small");
+  const int ntiles = (n + kTile - 1) / kTile;
+  const int nfilter = (n + 1023) / 1024;
+  const int nchunks = (n + kFinalChunk - 1) / kFinalChunk;
+  if (args.rand_seed >= 0) std::srand((unsigned)args.rand_seed);
+
+  // filter: maxW, kept-point compaction, zero tail
+  ISDF_CUDA(cudaMemsetAsync(b.st, 0, sizeof(KmState), stream));
+  ISDF_CUDA(cudaMemsetAsync(b.pidx, 0, sizeof(int) * (size_t)n, stream));
+  k_maxw<<<kNumSMs * 4, 256, 0, stream>>>(args.d_w, n, b.st);
+  k_filter_count<<<nfilter, 256, 0, stream>>>(args.d_w, n, b.st, b.tile_cnt);
+  k_scan_small<<<1, 1024, 0, stream>>>(b.tile_cnt, nfilter, &b.st->npt);
+  k_filter_scatter<<<nfilter, 256, 0, stream>>>(args.d_w, n, b.st, b.tile_cnt, b.pidx);
+  ISDF_CHECK_LAUNCH();
+  KmState hst;
+  ISDF_CUDA(cudaMemcpyAsync(&hst, b.st, sizeof(KmState), cudaMemcpyDeviceToHost, stream));
+  ISDF_CUDA(cudaStreamSynchronize(stream));
+  const int npt = hst.npt;
+  res->npt = npt;
+  std::memset(args.piv, 0, sizeof(int) * (size_t)n);
+
+  if (npt < mu) {
+    // utility.cpp:667-681: piv from the kept list, then a shuffled tail.
+    std::vector<int> index(n, 0);
+    ISDF_CUDA(cudaMemcpyAsync(index.data(), b.pidx, sizeof(int) * (size_t)npt,
+                              cudaMemcpyDeviceToHost, stream));
+    ISDF_CUDA(cudaStreamSynchronize(stream));
+    int k0 = 0, k1 = 0;
+    for (int i = 0; i < npt; i++) {
+      if (i == index[k0]) {
+        args.piv[k0] = i;
+        k0 = std::min(k0 + 1, mu - 1);
+      } else {
+        args.piv[npt + k1] = i;
+        k1++;
+      }
+    }
+    shuffle_like_libstdcxx(args.piv + npt, args.piv + n);
+    res->rk_eff = mu;
+    res->iters = -1;
+    return ISDF_OK;
+  }
+
+  const double dx0 = args.length[0] / args.num_grid[0];
+  const double dx1 = args.length[1] / args.num_grid[1];
+  const double dx2 = args.length[2] / args.num_grid[2];
+  k_points<<<grid_for(n, 256), 256, 0, stream>>>(b.pidx, args.d_w, n, args.num_grid[0],
+                                                 args.num_grid[1], dx0, dx1, dx2, b.px, b.py,
+                                                 b.pz, b.pw, mu, b.cen);
+  {
+    KmState init{};
+    init.flag = n;
+    init.rk = mu;
+    init.npt = npt;
+    init.maxw_bits = hst.maxw_bits;
+    ISDF_CUDA(cudaMemcpyAsync(b.st, &init, sizeof(KmState), cudaMemcpyHostToDevice, stream));
+  }
+  const unsigned agrid = grid_for(n, kAssignThreads, kPPT);
+  k_assign<<<agrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.st, b.label, 0);
+  ISDF_CHECK_LAUNCH();
+
+  const double max_f = 1e-5 * n;  // KmeansTolerance * n (utility.cpp:812)
+  const size_t hist_smem = sizeof(int) * (size_t)mu;
+  int chunks = 0;
+  const int max_chunks = args.max_iter / kIterChunk + 2;
+  for (;;) {
+    for (int it = 0; it < kIterChunk; ++it) {
+      k_iter_begin<<<1, 1, 0, stream>>>(b.st, max_f, args.max_iter);
+      k_hist<<<ntiles, 256, hist_smem, stream>>>(b.label, n, b.st, b.hist);
+      k_hist_scan<<<grid_for(mu, 256), 256, 0, stream>>>(b.hist, ntiles, b.st, b.members);
+      k_label_start<<<1, 1024, 0, stream>>>(b.members, b.st, b.start);
+      k_scatter<<<ntiles, 32, hist_smem, stream>>>(b.label, n, b.st, b.hist, b.start, b.sorted);
+      k_segsum<<<grid_for(mu, 8), 256, 0, stream>>>(b.sorted, b.start, b.members, b.px, b.py,
+                                                    b.pz, b.pw, b.st, b.sums);
+      k_centroids<<<1, 1024, 0, stream>>>(b.sums, b.st, b.cen);
+      k_assign<<<agrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.st, b.label,
+                                                     1);
+      k_iter_end<<<1, 1, 0, stream>>>(b.st);
+    }
+    ISDF_CHECK_LAUNCH();
+    ISDF_CUDA(cudaMemcpyAsync(&hst, b.st, sizeof(KmState), cudaMemcpyDeviceToHost, stream));
+    ISDF_CUDA(cudaStreamSynchronize(stream));
+    if (hst.done) break;
+    if (++chunks > max_chunks) return record_error(ISDF_ERR_CUDA, "kmeans: loop did not stop");
+  }
+  res->iters = hst.s;
+  const int rk = hst.rk;
+
+  dim3 fgrid((unsigned)((rk + 127) / 128), (unsigned)nchunks);
+  k_final_partial<<<fgrid, 128, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.st, b.part_d,
+                                             b.part_i);
+  k_final_reduce<<<grid_for(rk, 128), 128, 0, stream>>>(b.part_d, b.part_i, nchunks, b.st,
+                                                        b.pidx, b.sel);
+  ISDF_CHECK_LAUNCH();
+  std::vector<int> sel(rk);
+  ISDF_CUDA(cudaMemcpyAsync(sel.data(), b.sel, sizeof(int) * (size_t)rk, cudaMemcpyDeviceToHost,
+                            stream));
+  ISDF_CUDA(cudaStreamSynchronize(stream));
+  // unique (utility.cpp:617-629) and piv (utility.cpp:973-983)
+  std::sort(sel.begin(), sel.end());
+  sel.erase(std::unique(sel.begin(), sel.end()), sel.end());
+  const int rk_eff = (int)sel.size();
+  int k0 = 0, k1 = 0;
+  for (int i = 0; i < n; i++) {
+    if (i == sel[k0]) {
+      args.piv[k0] = i;
+      k0 = std::min(k0 + 1, rk_eff - 1);
+    } else {
+      args.piv[rk_eff + k1] = i;
+      k1++;
+    }
+  }
+  res->rk_eff = rk_eff;
+  return ISDF_OK;
+}
+
+}  // namespace isdf_b200

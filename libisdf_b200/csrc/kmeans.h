@@ -1,0 +1,35 @@
+// Host-side entry points of the K-means selector (kmeans.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "arena.h"
+
+namespace isdf_b200 {
+
+constexpr int kKmeansMaxMu = 12288;  // per-tile label histograms live in 48 KB of shared memory
+
+struct KmeansArgs {
+  const double* d_w;  // device weight[ng]
+  long long ng;
+  int num_grid[3];
+  double length[3];
+  int mu;
+  int max_iter;
+  long long rand_seed;  // >= 0: srand() first
+  int* piv;             // host int[ng]
+};
+
+struct KmeansResult {
+  int rk_eff = 0;
+  int iters = 0;
+  int npt = 0;
+};
+
+size_t kmeans_workspace_bytes(long long ng, int mu);
+int kmeans_weight(const double* d_psi, long long ng, int nocc, int nv1, int nc1, int nv2, int nc2,
+                  double* d_w, cudaStream_t stream);
+int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, KmeansResult* res);
+
+}  // namespace isdf_b200

@@ -26,12 +26,17 @@
 //      (utility.cpp:973-983).
 //  * the npt < rk early return with std::random_shuffle (utility.cpp:667-681).
 //
-// Build: g++ -O2 -std=c++14 (no -march: no FMA contraction, like the
-// reference's build, Makefile:102,159).
+// Build: g++ -O2 -std=c++14 -fopenmp (no -march: no FMA contraction, like
+// the reference's build, Makefile:102,159). OpenMP splits only loops whose
+// iterations are independent (per-point argmin, per-centroid nearest point),
+// so the result does not depend on the thread count.
 #include <cstdlib>
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 namespace {
 
@@ -116,7 +121,10 @@ int port_kmeans(const double* w, int n, const int* nG, const double* len, int rk
     return d1 * d1 + d2 * d2 + d3 * d3;
   };
   std::vector<int> label(n), last(n);
+  // Each point's argmin is independent, so the points are split over
+  // OpenMP threads; every distance is still evaluated exactly as above.
   auto assign = [&]() {
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < n; i++) {
       double best = dist(i, 0);
       int bj = 0;
@@ -173,6 +181,7 @@ int port_kmeans(const double* w, int n, const int* nG, const double* len, int rk
   *iters_out = s;
   // Nearest point to each centroid (first minimum over points).
   std::vector<int> sel(rk);
+#pragma omp parallel for schedule(dynamic, 16)
   for (int j = 0; j < rk; j++) {
     double best = dist(0, j);
     int bi = 0;
@@ -199,6 +208,14 @@ int port_kmeans(const double* w, int n, const int* nG, const double* len, int rk
     }
   }
   return rk;
+}
+
+int port_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
 }
 
 }  // extern "C"

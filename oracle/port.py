@@ -24,6 +24,7 @@ def lib():
         _lib.port_weight.argtypes = [P, ctypes.c_longlong, I, I, I, I, I, P]
         _lib.port_kmeans.argtypes = [P, I, P, P, I, I, ctypes.c_longlong, P, P]
         _lib.port_kmeans.restype = I
+        _lib.port_num_threads.restype = I
     return _lib
 
 
@@ -56,3 +57,7 @@ def kmeans_piv(psi, ng, length, nocc, nv1, nc1, nv2, nc2, mu, iters, rand_seed=1
     w = weight(psi, nocc, nv1, nc1, nv2, nc2)
     piv, rk, it = kmeans(w, ng, length, mu, iters, rand_seed)
     return piv, rk, it, w
+
+
+def num_threads() -> int:
+    return int(lib().port_num_threads())

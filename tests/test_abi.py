@@ -1,0 +1,65 @@
+"""Host-side checks of the C ABI (no GPU needed): the library loads, exports
+every function that include/isdf_c.h declares, and rejects bad arguments
+before touching the device."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+import libisdf_b200 as isdf
+
+
+def _declared_functions(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(isdf_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = isdf.lib()
+    names = _declared_functions("isdf_c.h")
+    assert len(names) >= 8
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings():
+    lib = isdf.lib()
+    assert lib.isdf_status_string(0) == b"ok"
+    assert b"positive definite" in lib.isdf_status_string(isdf.ISDF_ERR_NOT_SPD)
+
+
+def test_null_arguments_are_rejected_without_a_device():
+    lib = isdf.lib()
+    rc = lib.isdf_solve(None, None, 0, 1, 1, 0, 1, 0, 0, None, None, 1, 0, 0, None, None)
+    assert rc == isdf.ISDF_ERR_ARG
+    assert b"null" in lib.isdf_last_error()
+
+
+def test_bad_state_window_rejected():
+    dom = isdf.Domain(length=(1.0, 1.0, 1.0), num_grid=(4, 4, 4))
+    piv = __import__("numpy").zeros(64, dtype="int32")
+    with pytest.raises(isdf.IsdfError) as e:
+        isdf.ISDF(0x1000, dom, 2, 4, 3, 0, 2, 0, 8, 0x2000, piv, 5)  # nocc - nv1 < 0
+    assert e.value.code == isdf.ISDF_ERR_ARG
+    with pytest.raises(isdf.IsdfError):
+        isdf.ISDF(0x1000, dom, 2, 4, 2, 0, 2, 0, 8, 0x2000, piv, 5, s1="Random")
+
+
+def test_default_options_match_reference_constants():
+    o = isdf._Options()
+    isdf.lib().isdf_default_options(ctypes.byref(o))
+    assert o.precision == isdf.PRECISION_FP64
+    assert o.qrcp_oversample == 1.5 and o.qrcp_seed == 41  # getpoints_QRCP.cpp:82, isdf.cpp:68
+    assert o.rand_seed == -1
+
+
+def test_cxx_header_compiles():
+    src = '#include "isdf.hpp"\nint main(){ isdf::Domain d; (void)d; return 0; }\n'
+    r = subprocess.run(["g++", "-std=c++14", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
+                        "-x", "c++", "-"], input=src.encode(), capture_output=True)
+    assert r.returncode == 0, r.stderr.decode()

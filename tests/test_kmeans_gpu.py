@@ -1,0 +1,75 @@
+"""K-means selection on the GPU against the reference (bit-exact weight, piv,
+effective mu and iteration count)."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from oracle import port
+
+import libisdf_b200 as isdf
+from libisdf_b200 import synth
+
+pytestmark = pytest.mark.gpu
+CASES = ["si8_example", "small_s1s2", "small_mu0", "small_iters0", "small_early"]
+
+
+def _dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(np.asfortranarray(a).T)).cuda()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_weight_bit_exact(torch_cuda, name):
+    torch = torch_cuda
+    g = load_golden(name)
+    psi = g["psi"]
+    d_psi = _dev(torch, psi)
+    d_w = torch.empty(psi.shape[0], dtype=torch.float64, device="cuda")
+    isdf.kmeans_weight(d_psi, psi.shape[0], psi.shape[1], int(g["nocc"]), int(g["nv1"]),
+                       int(g["nc1"]), int(g["nv2"]), int(g["nc2"]), d_w)
+    torch.cuda.synchronize()
+    assert np.array_equal(d_w.cpu().numpy(), g["weight"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_select_matches_reference(torch_cuda, name):
+    torch = torch_cuda
+    g = load_golden(name)
+    dom = isdf.Domain(length=tuple(g["length"]), num_grid=tuple(int(x) for x in g["ng"]))
+    d_w = torch.from_numpy(g["weight"]).cuda()
+    piv, rk, it, npt = isdf.kmeans_select(dom, d_w, int(g["rk_requested"]), int(g["iters"]),
+                                          rand_seed=int(g["rand_seed"]))
+    assert (rk, it) == (int(g["rk_eff"]), int(g["n_iter"]))
+    assert np.array_equal(piv, g["piv"])
+
+
+def test_select_si8_synthetic_matches_oracle(torch_cuda):
+    """BASELINE config-0 shape: 40^3 grid, 32 states, mu = 320, 100 iterations."""
+    torch = torch_cuda
+    s = synth.SI8
+    psi = synth.shape_orbitals(s, 0)
+    ng, ln = (s.n,) * 3, (s.length,) * 3
+    piv_o, rk_o, it_o, w_o = port.kmeans_piv(psi, ng, ln, s.nocc, s.nv1, s.nc1, s.nv2, s.nc2,
+                                             s.mu, s.kmeans_iters)
+    g = load_golden("si8_synth_seed0")
+    if synth.sha256(psi) == str(g["psi_sha256"]):  # same bits as when the golden was made
+        assert np.array_equal(piv_o, g["piv"]) and rk_o == int(g["rk_eff"])
+    dom = isdf.Domain(length=ln, num_grid=ng)
+    d_psi = _dev(torch, psi)
+    d_theta = torch.empty((s.mu, s.ng), dtype=torch.float64, device="cuda")
+    piv = np.zeros(s.ng, dtype=np.int32)
+    rep = isdf.ISDF(d_psi, dom, s.nocc, s.nstate, s.nv1, s.nc1, s.nv2, s.nc2, s.mu, d_theta, piv,
+                    s.kmeans_iters)
+    assert rep.rk_eff == rk_o and rep.kmeans_iters == it_o
+    assert np.array_equal(piv, piv_o)
+    # zero-filled columns past the effective mu
+    assert float(d_theta[rep.rk_eff:].abs().max().cpu()) == 0.0 if rep.rk_eff < s.mu else True
+
+
+def test_select_is_repeatable(torch_cuda):
+    torch = torch_cuda
+    g = load_golden("small_s1s2")
+    dom = isdf.Domain(length=tuple(g["length"]), num_grid=tuple(int(x) for x in g["ng"]))
+    d_w = torch.from_numpy(g["weight"]).cuda()
+    a = isdf.kmeans_select(dom, d_w, 40, 50)
+    b = isdf.kmeans_select(dom, d_w, 40, 50)
+    assert np.array_equal(a[0], b[0]) and a[1:] == b[1:]

@@ -1,0 +1,59 @@
+"""Pins the oracle: the CPU restatements (oracle/kmeans_port.cpp, oracle/fit.py)
+against the golden fixtures that the reference's own CPU code produced
+(tests/golden/make_golden.py), and against that code itself when it is built
+here (oracle/_ref)."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from oracle import fit as ofit
+from oracle import port
+
+CASES = ["si8_example", "small_s1s2", "small_mu0", "small_iters0", "small_early"]
+
+
+def _args(g):
+    return (tuple(int(x) for x in g["ng"]), tuple(float(x) for x in g["length"]), int(g["nocc"]),
+            int(g["nv1"]), int(g["nc1"]), int(g["nv2"]), int(g["nc2"]))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_port_kmeans_matches_reference_golden(name):
+    g = load_golden(name)
+    ng, length, nocc, nv1, nc1, nv2, nc2 = _args(g)
+    piv, rk, it, w = port.kmeans_piv(g["psi"], ng, length, nocc, nv1, nc1, nv2, nc2,
+                                     int(g["rk_requested"]), int(g["iters"]),
+                                     rand_seed=int(g["rand_seed"]))
+    assert np.array_equal(w, g["weight"])  # bit-exact weight
+    assert rk == int(g["rk_eff"]) and it == int(g["n_iter"])
+    assert np.array_equal(piv, g["piv"])  # bit-exact pivots
+
+
+@pytest.mark.parametrize("name", ["small_s1s2", "small_mu0", "small_iters0"])
+def test_fit_restatement_matches_reference_golden(name):
+    g = load_golden(name)
+    ng, length, nocc, nv1, nc1, nv2, nc2 = _args(g)
+    rk = int(g["rk_eff"])
+    th = ofit.getbasis(g["psi"], nocc, nv1, nc1, nv2, nc2, rk, g["piv"])
+    ref_th = g["theta"]
+    # fitted pair densities are well conditioned; theta carries cond(C C^T) * eps
+    fd = ofit.fitted_densities(th, g["psi"], nocc, nv1, nc1, nv2, nc2, rk, g["piv"])
+    fd_ref = ofit.fitted_densities(ref_th, g["psi"], nocc, nv1, nc1, nv2, nc2, rk, g["piv"])
+    assert ofit.rel(fd, fd_ref) < 1e-8
+    assert ofit.rel(th, ref_th) < 1e-5
+
+
+def test_port_and_reference_agree_live():
+    ref = pytest.importorskip("oracle.ref")
+    if not ref.available():
+        pytest.skip("oracle/_ref not built on this machine")
+    g = load_golden("small_s1s2")
+    rng = np.random.default_rng(5)
+    psi = np.asfortranarray(np.linalg.qr(rng.standard_normal((8 * 9 * 10, 7)))[0])
+    for mu, iters in [(20, 0), (20, 3), (33, 40)]:
+        a = ref.kmeans_piv(psi, (8, 9, 10), (7.0, 8.0, 9.5), 3, 3, 4, 2, 1, mu, iters,
+                           cross_check=True)
+        b = port.kmeans_piv(psi, (8, 9, 10), (7.0, 8.0, 9.5), 3, 3, 4, 2, 1, mu, iters)
+        assert a[1:3] == b[1:3]
+        assert np.array_equal(a[0], b[0])
+    assert g["piv"].dtype == np.int32
