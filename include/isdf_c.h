@@ -74,9 +74,16 @@ typedef struct isdf_report_t {
   int npt;           /* grid points kept by the weight filter */
   double fit_err;    /* check: ||rho - theta C||_F / ||rho||_F */
   double coul_err;   /* check: relative truncated-Coulomb 4-index error */
-  double t_select_ms, t_fit_ms, t_chol_ms, t_solve_ms, t_check_ms, t_total_ms;
-  int chol_info;     /* > 0: leading minor that failed */
-  int reserved[7];
+  double t_select_ms;  /* wall time of weight + selection */
+  double t_fit_ms;     /* wall time of the fit */
+  double t_zct_ms;     /* device time of the Z C^T GEMM (CUDA events) */
+  double t_chol_ms;    /* device time of C C^T + Cholesky */
+  double t_solve_ms;   /* device time of the two triangular sweeps */
+  double t_check_ms;
+  double t_total_ms;
+  int chol_info;       /* > 0: leading minor that failed */
+  int kernel_launches; /* kernels this library launched for the solve */
+  int reserved[6];
 } isdf_report_t;
 
 /* Fills *opt with the reference's defaults. */

@@ -68,9 +68,10 @@ class _Report(ctypes.Structure):
                 ("kmeans_iters", ctypes.c_int), ("npt", ctypes.c_int),
                 ("fit_err", ctypes.c_double), ("coul_err", ctypes.c_double),
                 ("t_select_ms", ctypes.c_double), ("t_fit_ms", ctypes.c_double),
-                ("t_chol_ms", ctypes.c_double), ("t_solve_ms", ctypes.c_double),
-                ("t_check_ms", ctypes.c_double), ("t_total_ms", ctypes.c_double),
-                ("chol_info", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
+                ("t_zct_ms", ctypes.c_double), ("t_chol_ms", ctypes.c_double),
+                ("t_solve_ms", ctypes.c_double), ("t_check_ms", ctypes.c_double),
+                ("t_total_ms", ctypes.c_double), ("chol_info", ctypes.c_int),
+                ("kernel_launches", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
 
 
 @dataclass
@@ -125,8 +126,13 @@ class Report:
     coul_err: float
     t_select_ms: float
     t_fit_ms: float
+    t_zct_ms: float
+    t_chol_ms: float
+    t_solve_ms: float
+    t_check_ms: float
     t_total_ms: float
     chol_info: int
+    kernel_launches: int
 
 
 _lib = None
@@ -203,7 +209,8 @@ def ISDF(d_psirow, domain: Domain, nocc: int, nstate: int, nv1: int, nc1: int, n
                           int(bool(check)), ctypes.byref(o), ctypes.byref(r))
     _check(rc)
     return Report(r.rk_requested, r.rk_eff, r.kmeans_iters, r.npt, r.fit_err, r.coul_err,
-                  r.t_select_ms, r.t_fit_ms, r.t_total_ms, r.chol_info)
+                  r.t_select_ms, r.t_fit_ms, r.t_zct_ms, r.t_chol_ms, r.t_solve_ms, r.t_check_ms,
+                  r.t_total_ms, r.chol_info, r.kernel_launches)
 
 
 def kmeans_weight(d_psi, ng: int, nstate: int, nocc: int, nv1: int, nc1: int, nv2: int, nc2: int,

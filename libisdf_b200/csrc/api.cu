@@ -183,6 +183,7 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
   rep.rk_eff = kr.rk_eff;
   rep.kmeans_iters = kr.iters;
   rep.npt = kr.npt;
+  rep.kernel_launches = 1 + kr.launches;
   rep.t_select_ms = ms_since(t0);
 
   // (c, d) fit with the selected points (the GPU path fits with the shrunk
@@ -204,6 +205,10 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
   FitResult fr;
   int rc = fit_fp64(fa, arena, s, &fr);
   rep.chol_info = fr.chol_info;
+  rep.kernel_launches += fr.launches;
+  rep.t_zct_ms = fr.t_zct_ms;
+  rep.t_chol_ms = fr.t_chol_ms;
+  rep.t_solve_ms = fr.t_solve_ms;
   if (rc != ISDF_OK) {
     if (rep_out) *rep_out = rep;
     return rc;

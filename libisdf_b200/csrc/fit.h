@@ -19,6 +19,8 @@ struct FitArgs {
 
 struct FitResult {
   int chol_info = 0;
+  int launches = 0;
+  float t_zct_ms = 0, t_chol_ms = 0, t_solve_ms = 0;  // CUDA-event stage times
 };
 
 size_t fit_workspace_bytes(long long ng, int nstate, int rk);

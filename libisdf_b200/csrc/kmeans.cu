@@ -612,6 +612,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     shuffle_like_libstdcxx(args.piv + npt, args.piv + n);
     res->rk_eff = mu;
     res->iters = -1;
+    res->launches = 4;
     return ISDF_OK;
   }
 
@@ -658,6 +659,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     if (++chunks > max_chunks) return record_error(ISDF_ERR_CUDA, "kmeans: loop did not stop");
   }
   res->iters = hst.s;
+  res->launches = 4 + 2 + (chunks + 1) * kIterChunk * 9 + 2;
   const int rk = hst.rk;
 
   dim3 fgrid((unsigned)((rk + 127) / 128), (unsigned)nchunks);

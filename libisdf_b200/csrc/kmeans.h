@@ -25,6 +25,7 @@ struct KmeansResult {
   int rk_eff = 0;
   int iters = 0;
   int npt = 0;
+  int launches = 0;
 };
 
 size_t kmeans_workspace_bytes(long long ng, int mu);

@@ -33,6 +33,8 @@ def lib():
         _lib.ref_getbasis.argtypes = [P, P, P, I, I, I, I, I, I, I, P, P, P, I]
         _lib.ref_checkcode.argtypes = [P, P, P, I, I, I, I, I, I, I, P, P, P, P, P, I]
         _lib.ref_weight.argtypes = [P, I, I, I, I, I, I, P]
+        _lib.ref_bench_kmeans_step.argtypes = [I, I, I]
+        _lib.ref_bench_kmeans_step.restype = ctypes.c_double
         _lib.ref_iround.argtypes = [ctypes.c_double]
         _lib.ref_iround.restype = I
     return _lib
@@ -112,3 +114,26 @@ def checkcode(psi, ng, length, nocc, nv1, nc1, nv2, nc2, rk, piv, theta):
 
 def iround(a: float) -> int:
     return int(lib().ref_iround(float(a)))
+
+
+def bench_kmeans_step(npt: int, rk: int, repeats: int = 1) -> float:
+    """Seconds of one reference Lloyd step (pdist2 + findMin) at full size."""
+    return float(lib().ref_bench_kmeans_step(npt, rk, repeats))
+
+
+def bench_getbasis_rows(psi, shape, fraction: int, repeats: int = 1) -> float:
+    """Seconds of the reference's getbasis_MPI on the first Ng/fraction grid
+    rows with the full mu (pivots drawn inside that row block)."""
+    import time
+
+    rows = psi.shape[0] // fraction
+    sub = np.asfortranarray(psi[:rows])
+    piv = np.random.default_rng(0).choice(rows, size=shape.mu, replace=False).astype(np.int32)
+    piv = np.concatenate([np.sort(piv), np.zeros(rows - shape.mu, dtype=np.int32)])
+    best = 1e300
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        getbasis(sub, (rows, 1, 1), (1.0, 1.0, 1.0), shape.nocc, shape.nv1, shape.nc1, shape.nv2,
+                 shape.nc2, shape.mu, piv)
+        best = min(best, time.perf_counter() - t0)
+    return best

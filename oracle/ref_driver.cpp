@@ -177,6 +177,31 @@ int ref_checkcode(const double* psi, const int* ng, const double* len, int nocc,
   }
 }
 
+// Seconds for one K-means Lloyd step of the reference at full size: its
+// pdist2 (utility.cpp:598-615) of npt grid points against rk centroids and its
+// findMin over centroids (utility.cpp:535-562), i.e. the per-iteration work of
+// KMEAN's loop (utility.cpp:878-901). Best of `repeats`.
+double ref_bench_kmeans_step(int npt, int rk, int repeats) {
+  DblNumMat grid(npt, 3), cen(rk, 3), D;
+  for (int i = 0; i < npt; i++) {
+    grid(i, 0) = (i % 97) * 0.25;
+    grid(i, 1) = ((i / 97) % 89) * 0.25;
+    grid(i, 2) = (i / (97 * 89)) * 0.25;
+  }
+  for (int j = 0; j < rk; j++)
+    for (int d = 0; d < 3; d++) cen(j, d) = grid((int)((long long)j * npt / rk), d) + 0.01;
+  IntNumVec label;
+  double best = 1e300;
+  for (int r = 0; r < repeats; r++) {
+    double t0 = MPI_Wtime();
+    pdist2(grid, cen, D);
+    findMin(D, 1, label);
+    double t = MPI_Wtime() - t0;
+    if (t < best) best = t;
+  }
+  return best;
+}
+
 // The reference's integer rounding IRound (include/common/utility.hpp:18-23),
 // used for the default mu and the QRCP sketch width.
 int ref_iround(double a) { return IRound(a); }
