@@ -123,6 +123,28 @@ int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, i
              int nc2, int rk, const int* piv, double* d_theta, int precision, int refine_steps,
              int* chol_info, void* stream);
 
+/* Size of the fixed device scratch array behind isdf_fit_noalloc(). */
+#define ISDF_NOALLOC_SCRATCH_BYTES (8u << 20)
+
+/* No counterpart in the reference. isdf_fit() with every scratch array taken
+ * from one fixed 8 MiB __device__ array inside the library instead of device
+ * allocations: it calls no cudaMalloc / cudaFree and no allocating library
+ * routine. For callers that cannot have the library allocate device memory
+ * mid-run, e.g. a DFT host code that has reserved (nearly) all of HBM for its
+ * own pool at start-up, or one that cannot afford the device-wide
+ * synchronisation of cudaFree. The caller still passes psi, piv and theta.
+ * Limit: the fit's scratch for (rk, nstate) must fit in 8 MiB (for example
+ * rk <= 512 with nstate <= 512); larger sizes return ISDF_ERR_UNSUPPORTED
+ * with a message naming the bytes needed. Every process that loads the
+ * library holds the array on each GPU it uses until exit. All calls on a
+ * device share the array, so calls that overlap on the GPU race; it keeps
+ * the last call's contents (each call clears what must start at zero). The
+ * first call on a device looks up the array's address once; make it before
+ * any stream capture. stream NULL = the legacy default stream. Synchronous. */
+int isdf_fit_noalloc(const double* d_psi, long long ng, int nstate, int nocc, int nv1, int nc1,
+                     int nv2, int nc2, int rk, const int* piv, double* d_theta, int* chol_info,
+                     void* stream);
+
 /* Message for the last error on this thread ("" if none). */
 const char* isdf_last_error(void);
 const char* isdf_status_string(int code);

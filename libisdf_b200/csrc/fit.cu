@@ -497,7 +497,7 @@ struct StageEvents {
   }
 };
 
-int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res) {
+int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, bool timed) {
   const long long ng = args.ng;
   const int rk = args.rk;
   if (ng <= 0 || rk <= 0 || args.nstate <= 0) return record_error(ISDF_ERR_ARG, "fit: bad sizes");
@@ -505,7 +505,8 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res) 
   FitBuffers b = carve(arena, args.nstate, rk);
   if (arena.overflowed()) return record_error(ISDF_ERR_NOMEM, "fit: workspace too small");
   StageEvents ev;
-  ISDF_TRY(ev.create());
+  if (timed) ISDF_TRY(ev.create());
+  auto mark = [&](int i) { return timed ? cudaEventRecord(ev.e[i], s) : cudaSuccess; };
   const int nblk_ = (rk + kNB - 1) / kNB;
   const bool same_ = (args.nv1 == args.nv2 && args.nc1 == args.nc2);
   res->launches = 1 + (same_ ? 1 : 2) + 2 + (nblk_ + 2 * (nblk_ - 1) + 1) + 2 * nblk_;
@@ -520,7 +521,7 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res) 
   const int lo2 = args.nocc - args.nv2, K2 = args.nv2 + args.nc2;
   const bool same = (args.nv1 == args.nv2 && args.nc1 == args.nc2);
   dim3 zg((unsigned)((rk + 127) / 128), (unsigned)((ng + 127) / 128));
-  ISDF_CUDA(cudaEventRecord(ev.e[0], s));
+  ISDF_CUDA(mark(0));
   if (same) {
     k_gemm_z<0><<<zg, 256, smem_bytes_88, s>>>((int)ng, rk, K1, args.d_psi + (long long)lo1 * ng,
                                                ng, b.Bm + (size_t)lo1 * rk, rk, args.d_theta, ng);
@@ -533,11 +534,11 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res) 
   ISDF_CHECK_LAUNCH();
 
   // C C^T, regularisation, Cholesky
-  ISDF_CUDA(cudaEventRecord(ev.e[1], s));
+  ISDF_CUDA(mark(1));
   k_gather_cct<<<grid_for((long long)rk * rk, 256), 256, 0, s>>>(args.d_theta, ng, b.piv, rk, b.P);
   k_regularise<<<1, 256, 0, s>>>(b.P, rk, b.eps);
   ISDF_TRY(cholesky(b, rk, s));
-  ISDF_CUDA(cudaEventRecord(ev.e[2], s));
+  ISDF_CUDA(mark(2));
   int info = 0;
   ISDF_CUDA(cudaMemcpyAsync(&info, b.info, sizeof(int), cudaMemcpyDeviceToHost, s));
   ISDF_CUDA(cudaStreamSynchronize(s));
@@ -558,7 +559,8 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res) 
                                                  b.dinv + (size_t)kb * kNB * kNB);
   }
   ISDF_CHECK_LAUNCH();
-  ISDF_CUDA(cudaEventRecord(ev.e[3], s));
+  ISDF_CUDA(mark(3));
+  if (!timed) return ISDF_OK;
   ISDF_CUDA(cudaEventSynchronize(ev.e[3]));
   ISDF_CUDA(cudaEventElapsedTime(&res->t_zct_ms, ev.e[0], ev.e[1]));
   ISDF_CUDA(cudaEventElapsedTime(&res->t_chol_ms, ev.e[1], ev.e[2]));

@@ -24,6 +24,9 @@ struct FitResult {
 };
 
 size_t fit_workspace_bytes(long long ng, int nstate, int rk);
-int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t stream, FitResult* res);
+// timed = false skips the stage timers (no CUDA events are created); the
+// launches are then only queued on `stream` after the Cholesky check.
+int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t stream, FitResult* res,
+             bool timed = true);
 
 }  // namespace isdf_b200
