@@ -407,8 +407,10 @@ constexpr size_t smem_bytes_trsm =
 constexpr size_t smem_bytes_potf2 = sizeof(double) * 2 * kNB * (kNB + 1);
 
 int set_smem_attrs() {
-  static bool done = false;
-  if (done) return ISDF_OK;
+  static bool done_dev[64] = {};
+  int dev = 0;
+  ISDF_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && done_dev[dev]) return ISDF_OK;
   ISDF_CUDA(cudaFuncSetAttribute(k_potf2, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem_bytes_potf2));
   ISDF_CUDA(cudaFuncSetAttribute(k_gemm_z<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -423,7 +425,7 @@ int set_smem_attrs() {
                                  (int)smem_bytes_84));
   ISDF_CUDA(cudaFuncSetAttribute(k_trsm_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem_bytes_trsm));
-  done = true;
+  if (dev >= 0 && dev < 64) done_dev[dev] = true;
   return ISDF_OK;
 }
 

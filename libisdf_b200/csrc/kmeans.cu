@@ -326,51 +326,110 @@ __global__ void __launch_bounds__(1024) k_label_start(const int* __restrict__ me
   }
 }
 
-// One warp per tile: scatters the tile's points to their stable positions.
-__global__ void __launch_bounds__(32) k_scatter(const int* __restrict__ label, int n,
-                                                const KmState* st, const int* __restrict__ hist,
-                                                const int* __restrict__ start,
-                                                int* __restrict__ sorted) {
+// One tile per block: 128 threads stage the tile's labels in shared memory,
+// then one warp walks them in order and scatters every point to its stable
+// position (peers with equal labels share one running offset).
+__global__ void __launch_bounds__(128) k_scatter(const int* __restrict__ label, int n,
+                                                 const KmState* st, const int* __restrict__ hist,
+                                                 const int* __restrict__ start,
+                                                 int* __restrict__ sorted) {
   if (st->done) return;
-  extern __shared__ int run[];
+  extern __shared__ int sm_scatter[];
   const int rk = st->rk;
-  const int lane = threadIdx.x;
+  int* run = sm_scatter;
+  int* lab = sm_scatter + rk;
   const int* row = hist + (size_t)blockIdx.x * rk;
-  for (int l = lane; l < rk; l += 32) run[l] = start[l] + row[l];
-  __syncwarp();
+  for (int l = threadIdx.x; l < rk; l += 128) run[l] = start[l] + row[l];
   const int base = blockIdx.x * kTile;
-  const int end = min(base + kTile, n);
-  for (int c = base; c < end; c += 32) {
-    const int p = c + lane;
-    const bool ok = p < end;
-    const int l = ok ? label[p] : -1;
+  const int cnt = min(kTile, n - base);
+  for (int k = threadIdx.x; k < cnt; k += 128) lab[k] = label[base + k];
+  __syncthreads();
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  for (int c = 0; c < cnt; c += 32) {
+    const int k = c + lane;
+    const bool ok = k < cnt;
+    const int l = ok ? lab[k] : -1;
     const unsigned peers = __match_any_sync(0xffffffffu, l);
     const int b = ok ? run[l] : 0;
     __syncwarp();
     if (ok) {
       const int r = __popc(peers & ((1u << lane) - 1u));
-      sorted[b + r] = p;
+      sorted[b + r] = base + k;
       if (lane == __ffs(peers) - 1) run[l] = b + __popc(peers);
     }
     __syncwarp();
   }
 }
 
+// m successive round-to-nearest additions acc <- fl(acc + c), acc >= 0,
+// c >= 0, with the exact result of the sequential loop. While acc stays in
+// one binade [2^e, 2^(e+1)) every addition adds the same number of ulps
+// (c rounded to the ulp grid), unless c's remainder is exactly half an ulp
+// (a tie, which depends on acc's parity): those steps, binade crossings and
+// subnormal accumulators are taken one at a time; the rest are jumped.
+__device__ double repeat_add(double acc, double c, long long m) {
+  const double two53 = 9007199254740992.0;
+  while (m > 0) {
+    if (c == 0.0) return radd(acc, 0.0);
+    if (!(acc >= 2.2250738585072014e-308) || c >= ldexp(1.0, ilogb(acc))) {
+      acc = radd(acc, c);
+      --m;
+      continue;
+    }
+    const int e = ilogb(acc);
+    const double u = ldexp(1.0, e - 52);  // ulp of acc
+    const double cu = c / u;              // exact: u is a power of two
+    const double q = floor(cu);
+    const double r = cu - q;
+    if (r == 0.5) {
+      acc = radd(acc, c);
+      --m;
+      continue;
+    }
+    const double qp = q + (r > 0.5 ? 1.0 : 0.0);  // ulps added per step
+    if (qp == 0.0) return acc;  // c rounds away now and at every larger exponent
+    const double a = acc / u;   // integer in [2^52, 2^53)
+    const double room = two53 - q - 2.0 - a;
+    if (room < 0.0) {
+      acc = radd(acc, c);
+      --m;
+      continue;
+    }
+    long long k = (long long)floor(room / qp) + 1;
+    if (k > m) k = m;
+    acc = __dmul_rn(__dadd_rn(a, __dmul_rn((double)k, qp)), u);  // all exact
+    m -= k;
+  }
+  return acc;
+}
+
 // One warp per cluster: sequential fold over the members (in index order).
+// The zero-tail points p >= npt are identical copies of grid point 0 (weight
+// w[0], coordinates (0, 0, 0)) and come last in their cluster's member list,
+// so their part of the fold is a repeated addition of one value.
 __global__ void __launch_bounds__(256) k_segsum(const int* __restrict__ sorted,
                                                 const int* __restrict__ start,
                                                 const int* __restrict__ members,
                                                 const double* __restrict__ px,
                                                 const double* __restrict__ py,
                                                 const double* __restrict__ pz,
-                                                const double* __restrict__ pw, KmState* st,
-                                                double4* __restrict__ sums) {
+                                                const double* __restrict__ pw,
+                                                const int* __restrict__ label, int n,
+                                                KmState* st, double4* __restrict__ sums) {
   if (st->done) return;
   const int rk = st->rk;
   const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (c >= rk) return;
-  const int s0 = start[c], m = members[c];
+  const int npt = st->npt;
+  const int s0 = start[c];
+  int m = members[c];
+  long long tail = 0;
+  if (npt < n && label[npt] == c) {
+    tail = n - npt;
+    m -= (int)tail;
+  }
   double aw = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
   for (int q = 0; q < m; q += 32) {
     double vw = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
@@ -390,6 +449,13 @@ __global__ void __launch_bounds__(256) k_segsum(const int* __restrict__ sorted,
     }
   }
   if (lane == 0) {
+    if (tail) {
+      const double w0 = pw[npt];
+      aw = repeat_add(aw, w0, tail);
+      ax = repeat_add(ax, rmul(w0, px[npt]), tail);
+      ay = repeat_add(ay, rmul(w0, py[npt]), tail);
+      az = repeat_add(az, rmul(w0, pz[npt]), tail);
+    }
     sums[c] = make_double4(ax, ay, az, aw);
     if (aw == 0.0) st->any_empty = 1;
   }
@@ -492,6 +558,20 @@ __global__ void k_final_reduce(const double* __restrict__ part_d, const int* __r
     }
   }
   sel[j] = pidx[bi];
+}
+
+// Dynamic shared memory above 48 KB needs an opt-in per kernel and device.
+int set_kmeans_smem_attrs() {
+  static bool done[64] = {};
+  int dev = 0;
+  ISDF_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && done[dev]) return ISDF_OK;
+  ISDF_CUDA(cudaFuncSetAttribute(k_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(int) * kKmeansMaxMu)));
+  ISDF_CUDA(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(int) * (kKmeansMaxMu + kTile))));
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return ISDF_OK;
 }
 
 struct KmBuffers {
@@ -636,6 +716,8 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
 
   const double max_f = 1e-5 * n;  // KmeansTolerance * n (utility.cpp:812)
   const size_t hist_smem = sizeof(int) * (size_t)mu;
+  const size_t scatter_smem = sizeof(int) * ((size_t)mu + kTile);
+  ISDF_TRY(set_kmeans_smem_attrs());
   int chunks = 0;
   const int max_chunks = args.max_iter / kIterChunk + 2;
   for (;;) {
@@ -644,9 +726,10 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
       k_hist<<<ntiles, 256, hist_smem, stream>>>(b.label, n, b.st, b.hist);
       k_hist_scan<<<grid_for(mu, 256), 256, 0, stream>>>(b.hist, ntiles, b.st, b.members);
       k_label_start<<<1, 1024, 0, stream>>>(b.members, b.st, b.start);
-      k_scatter<<<ntiles, 32, hist_smem, stream>>>(b.label, n, b.st, b.hist, b.start, b.sorted);
+      k_scatter<<<ntiles, 128, scatter_smem, stream>>>(b.label, n, b.st, b.hist, b.start,
+                                                       b.sorted);
       k_segsum<<<grid_for(mu, 8), 256, 0, stream>>>(b.sorted, b.start, b.members, b.px, b.py,
-                                                    b.pz, b.pw, b.st, b.sums);
+                                                    b.pz, b.pw, b.label, n, b.st, b.sums);
       k_centroids<<<1, 1024, 0, stream>>>(b.sums, b.st, b.cen);
       k_assign<<<agrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.st, b.label,
                                                      1);

@@ -73,3 +73,25 @@ def test_select_is_repeatable(torch_cuda):
     a = isdf.kmeans_select(dom, d_w, 40, 50)
     b = isdf.kmeans_select(dom, d_w, 40, 50)
     assert np.array_equal(a[0], b[0]) and a[1:] == b[1:]
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_select_heavy_zero_tail(torch_cuda, seed):
+    """Half of the grid falls below the weight filter, so half of the K-means
+    points are copies of grid point 0 (the reference's zero-initialised index
+    tail), here carrying the largest weight: their cluster's fold is dominated
+    by that repeated addition."""
+    torch = torch_cuda
+    rng = np.random.default_rng(seed)
+    ng = (20, 21, 19)
+    n = int(np.prod(ng))
+    w = rng.uniform(0.1, 1.0, size=n) ** 3
+    w[rng.random(n) < 0.5] = 1e-13
+    w[0] = 1.7
+    length = (9.5, 10.0, 9.0)
+    piv_o, rk_o, it_o = port.kmeans(w, ng, length, 50, 30)
+    piv, rk, it, npt = isdf.kmeans_select(isdf.Domain(length=length, num_grid=ng),
+                                          torch.from_numpy(w).cuda(), 50, 30)
+    assert npt < n / 2 + n / 10
+    assert (rk, it) == (rk_o, it_o)
+    assert np.array_equal(piv, piv_o)
