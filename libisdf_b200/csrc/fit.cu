@@ -11,160 +11,69 @@
 //   4. eps = 1e-10 * (trace / rk) added to the diagonal         (:346-349)
 //   5. lower Cholesky L                                          (:365)
 //   6. theta L^T = Z C^T, then theta L = (that), in place        (:372-382)
-// Kernels: one DFMA register-tiled GEMM core (128 x 128 or 128 x 64 CTA
-// tiles, 8 x 8 / 8 x 4 outputs per thread, cp.async double buffering) used by
-// the Z GEMM, the Cholesky panel / trailing updates and the triangular-solve
-// steps; a single-CTA 64 x 64 diagonal-block factor + inverse.
+// Kernels: one FP64 tensor-core GEMM core (dgemm.cuh: mma.sync m16n8k8 f64,
+// 3-stage cp.async pipeline) used by the Z GEMM, the Cholesky panel and
+// trailing updates and the triangular-solve steps; a single-CTA 64 x 64
+// diagonal-block factor + inverse.
+//
+// Triangular solve. For a 64-column block K = [c0, c0+bs) with diagonal block
+// L_KK and D = L_KK^{-1}, the forward step of theta L^T = Z is
+//   X_K = (Z_K - X_{<K} L_{K,<K}^T) D^T = [X_{<K} | Z_K] . [-L_{K,<K}^T D^T ; D^T]
+// and the backward step of theta L = X is
+//   T_K = (X_K - T_{>K} L_{>K,K}) D   = [X_K | T_{>K}] . [D ; -L_{>K,K} D].
+// Both are one GEMM over a contiguous column range of theta (whose columns
+// hold the solved and the pending parts side by side) with a small operand
+// W_K built just before the step; each CTA owns a row tile of theta and writes
+// block K in place after it has read everything it needs. Only the 64 x 64
+// diagonal blocks are inverted explicitly; every other block takes part by
+// substitution, as in a blocked dtrsm.
 // theta is column-major Ng x rk (ld = Ng), overwritten in place.
 #include <vector>
 
 #include "arena.h"
 #include "common.cuh"
+#include "dgemm.cuh"
 #include "fit.h"
 
 namespace isdf_b200 {
 
 namespace {
 
-constexpr int kBK = 16;  // k-depth of one smem stage
-constexpr int kNB = 64;  // Cholesky / TRSM block size
+constexpr int kNB = 64;  // Cholesky / triangular-solve block size
 
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool ok) {
-  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  int sz = ok ? 8 : 0;
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+using CoreZ = dmma::Core<128, 128>;  // Z GEMM, Cholesky trailing update
+using CoreN = dmma::Core<128, 64>;   // panel and triangular-solve steps
+
+// 16-byte cp.async needs 16-byte aligned rows: base aligned, even leading dimension.
+__host__ __device__ inline bool vec2_ok(const void* a, long long lda, const void* b,
+                                        long long ldb) {
+  return ((reinterpret_cast<size_t>(a) | reinterpret_cast<size_t>(b)) & 15) == 0 &&
+         (lda % 2) == 0 && (ldb % 2) == 0;
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
-// CTA tile: BM = 16*TM rows, BN = 16*TN columns, 256 threads as 16 x 16.
-// Thread (tx, ty) owns rows {i*64 + tx*4 + r} and columns {j*64 + ty*4 + c}.
-// A: column-major (row m, depth k) at A[m + k*lda], already offset to the
-// tile's first row. B: depth-major (depth k, column n) at B[k*ldb + n],
-// already offset to the tile's first column.
-template <int TM, int TN>
-struct Tile {
-  static constexpr int BM = 16 * TM;
-  static constexpr int BN = 16 * TN;
-  static constexpr int A_STAGE = kBK * BM;
-  static constexpr int B_STAGE = kBK * BN;
-  static constexpr int SMEM_DOUBLES = 2 * (A_STAGE + B_STAGE);
-
-  __device__ static void load(double* As, double* Bs, const double* A, long long lda,
-                              const double* B, long long ldb, int m_rem, int n_rem, int k0,
-                              int k_end) {
-    const int tid = threadIdx.x;
-#pragma unroll
-    for (int r = 0; r < A_STAGE / 256; ++r) {
-      int e = tid + r * 256;
-      int k = e / BM, m = e % BM;
-      bool ok = (m < m_rem) && (k0 + k < k_end);
-      const double* src = ok ? A + m + (long long)(k0 + k) * lda : A;
-      cp_async8(As + e, src, ok);
-    }
-#pragma unroll
-    for (int r = 0; r < B_STAGE / 256; ++r) {
-      int e = tid + r * 256;
-      int k = e / BN, n = e % BN;
-      bool ok = (n < n_rem) && (k0 + k < k_end);
-      const double* src = ok ? B + (long long)(k0 + k) * ldb + n : B;
-      cp_async8(Bs + e, src, ok);
-    }
-  }
-
-  // acc += A[0:BM, k_begin:k_end] * B[k_begin:k_end, 0:BN]
-  __device__ static void accumulate(double (&acc)[TM][TN], double* smem, const double* A,
-                                    long long lda, const double* B, long long ldb, int m_rem,
-                                    int n_rem, int k_begin, int k_end) {
-    if (k_end <= k_begin) return;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    double* As0 = smem;
-    double* Bs0 = smem + 2 * A_STAGE;
-    const int nk = (k_end - k_begin + kBK - 1) / kBK;
-    load(As0, Bs0, A, lda, B, ldb, m_rem, n_rem, k_begin, k_end);
-    cp_async_commit();
-    for (int t = 0; t < nk; ++t) {
-      const int cur = t & 1;
-      if (t + 1 < nk) {
-        load(As0 + (cur ^ 1) * A_STAGE, Bs0 + (cur ^ 1) * B_STAGE, A, lda, B, ldb, m_rem, n_rem,
-             k_begin + (t + 1) * kBK, k_end);
-      }
-      cp_async_commit();
-      cp_async_wait<1>();
-      __syncthreads();
-      const double* As = As0 + cur * A_STAGE;
-      const double* Bs = Bs0 + cur * B_STAGE;
-#pragma unroll
-      for (int kk = 0; kk < kBK; ++kk) {
-        double a[TM], b[TN];
-#pragma unroll
-        for (int i = 0; i < TM / 4; ++i) {
-          const double2* p = reinterpret_cast<const double2*>(As + kk * BM + i * 64 + tx * 4);
-          double2 v0 = p[0], v1 = p[1];
-          a[i * 4 + 0] = v0.x;
-          a[i * 4 + 1] = v0.y;
-          a[i * 4 + 2] = v1.x;
-          a[i * 4 + 3] = v1.y;
-        }
-#pragma unroll
-        for (int j = 0; j < TN / 4; ++j) {
-          const double2* p = reinterpret_cast<const double2*>(Bs + kk * BN + j * 64 + ty * 4);
-          double2 v0 = p[0], v1 = p[1];
-          b[j * 4 + 0] = v0.x;
-          b[j * 4 + 1] = v0.y;
-          b[j * 4 + 2] = v1.x;
-          b[j * 4 + 3] = v1.y;
-        }
-#pragma unroll
-        for (int i = 0; i < TM; ++i)
-#pragma unroll
-          for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-      }
-      __syncthreads();
-    }
-    cp_async_wait<0>();
-  }
-
-  __device__ static int row(int i) { return (i >> 2) * 64 + (threadIdx.x & 15) * 4 + (i & 3); }
-  __device__ static int col(int j) { return (j >> 2) * 64 + (threadIdx.x >> 4) * 4 + (j & 3); }
-};
 
 // ----------------------------------------------------------- Z C^T GEMM
 // mode 0: C = acc*acc (S1 = S2); mode 1: C = acc (first factor);
 // mode 2: C = C * acc (second factor, S1 != S2).
-template <int MODE>
+template <int MODE, int VEC>
 __global__ void __launch_bounds__(256) k_gemm_z(int M, int N, int K, const double* __restrict__ A,
                                                 long long lda, const double* __restrict__ B,
                                                 long long ldb, double* __restrict__ C,
                                                 long long ldc) {
-  using T = Tile<8, 8>;
   extern __shared__ double smem[];
-  const int n0 = blockIdx.x * T::BN;
-  const long long m0 = (long long)blockIdx.y * T::BM;
-  double acc[8][8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
-  T::accumulate(acc, smem, A + m0, lda, B + n0, ldb, (int)(M - m0 < T::BM ? M - m0 : T::BM), N - n0,
-                0, K);
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int n = n0 + T::col(j);
-    if (n >= N) continue;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const long long m = m0 + T::row(i);
-      if (m >= M) continue;
-      double* c = C + m + (long long)n * ldc;
-      if (MODE == 0) *c = acc[i][j] * acc[i][j];
-      else if (MODE == 1) *c = acc[i][j];
-      else *c = *c * acc[i][j];
+  const int n0 = blockIdx.x * CoreZ::BN;
+  const long long m0 = (long long)blockIdx.y * CoreZ::BM;
+  CoreZ core;
+  core.zero();
+  const int m_rem = (int)(M - m0 < CoreZ::BM ? M - m0 : CoreZ::BM);
+  core.run<VEC>(smem, A + m0, lda, B + n0, ldb, m_rem, N - n0, 0, K);
+  core.for_each([&](int r, int c, double v) {
+    if (r < m_rem && n0 + c < N) {
+      double* p = C + (m0 + r) + (long long)(n0 + c) * ldc;
+      if (MODE == 0) *p = v * v;
+      else if (MODE == 1) *p = v;
+      else *p = *p * v;
     }
-  }
+  });
 }
 
 // ----------------------------------------------------------- gathers
@@ -265,166 +174,120 @@ __global__ void __launch_bounds__(256) k_potf2(double* A, int lda, int k0, int b
 
 // Panel: L[k0+bs:, k0:k0+bs] = A[k0+bs:, k0:k0+bs] * X^T, in place (a CTA
 // reads its whole row tile before it writes it back).
+template <int VEC>
 __global__ void __launch_bounds__(256) k_chol_panel(double* A, int lda, int k0, int bs, int n,
                                                     const double* __restrict__ dinvT) {
-  using T = Tile<8, 4>;
   extern __shared__ double smem[];
-  const int m0 = k0 + bs + blockIdx.x * T::BM;
-  double acc[8][4];
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  double* Ablk = A + m0 + (long long)k0 * lda;
-  T::accumulate(acc, smem, Ablk, lda, dinvT, kNB, n - m0, bs, 0, bs);
-  __syncthreads();
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    int c = T::col(j);
-    if (c >= bs) continue;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      int m = m0 + T::row(i);
-      if (m < n) A[m + (long long)(k0 + c) * lda] = acc[i][j];
-    }
-  }
+  const int m0 = k0 + bs + blockIdx.x * CoreN::BM;
+  CoreN core;
+  core.zero();
+  core.run<VEC>(smem, A + m0 + (long long)k0 * lda, lda, dinvT, kNB, n - m0, bs, 0, bs);
+  core.for_each([&](int r, int c, double v) {
+    if (m0 + r < n && c < bs) A[(m0 + r) + (long long)(k0 + c) * lda] = v;
+  });
 }
 
 // Trailing update of the lower part: A[r, c] -= sum_k L[r, k] L[c, k] for
 // r, c >= k0+bs, k in the panel. Tiles wholly above the diagonal are skipped.
+template <int VEC>
 __global__ void __launch_bounds__(256) k_chol_update(double* A, int lda, int k0, int bs, int n) {
-  using T = Tile<8, 8>;
   extern __shared__ double smem[];
   const int base = k0 + bs;
-  const int n0 = base + blockIdx.x * T::BN;
-  const int m0 = base + blockIdx.y * T::BM;
-  if (m0 + T::BM <= n0) return;
-  double acc[8][8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
-  const double* Ap = A + m0 + (long long)k0 * lda;
-  const double* Bp = A + n0 + (long long)k0 * lda;  // B(k, c) = L[n0 + c, k0 + k]
-  T::accumulate(acc, smem, Ap, lda, Bp, lda, n - m0, n - n0, 0, bs);
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    int c = n0 + T::col(j);
-    if (c >= n) continue;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      int r = m0 + T::row(i);
-      if (r < n && r >= c) A[r + (long long)c * lda] -= acc[i][j];
-    }
-  }
+  const int n0 = base + blockIdx.x * CoreZ::BN;
+  const int m0 = base + blockIdx.y * CoreZ::BM;
+  if (m0 + CoreZ::BM <= n0) return;
+  CoreZ core;
+  core.zero();
+  // B(k, c) = L[n0 + c, k0 + k]
+  core.run<VEC>(smem, A + m0 + (long long)k0 * lda, lda, A + n0 + (long long)k0 * lda, lda,
+                n - m0, n - n0, 0, bs);
+  core.for_each([&](int r, int c, double v) {
+    const int gr = m0 + r, gc = n0 + c;
+    if (gr < n && gc < n && gr >= gc) A[gr + (long long)gc * lda] -= v;
+  });
 }
 
-// LT = L^T (column-major), and the strict upper triangle of L cleared.
-__global__ void k_transpose_lower(double* L, int n, double* __restrict__ LT) {
+// Clears the strict upper triangle left over in the factor's storage.
+__global__ void k_clear_upper(double* L, int n) {
   const long long total = (long long)n * n;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
-    int r = (int)(e % n), c = (int)(e / n);
-    double v = r >= c ? L[e] : 0.0;
+    const int r = (int)(e % n), c = (int)(e / n);
     if (r < c) L[e] = 0.0;
-    LT[(long long)c + (long long)r * n] = v;
   }
 }
 
 // ----------------------------------------------------------- triangular solve
-// One column block [c0, c0+bs) of one sweep, for a 128-row tile of theta:
-//   out = (theta[rows, c0:c0+bs] - theta[rows, kr] * B[kr, c0:c0+bs]) * D
-// forward  (theta L^T = Z): kr = [0, c0),       B(k, n) = L(c0+n, k) = L[c0+n + k*rk]
-// backward (theta L = Y):   kr = [c0+bs, rk),   B(k, n) = L(k, c0+n) = LT[c0+n + k*rk]
-// D = the padded inverse of the diagonal block (dinvT forward, dinv backward).
-// Rows are independent, so each CTA overwrites its own tile in place.
-__global__ void __launch_bounds__(256) k_trsm_step(double* theta, long long ng, int rk,
-                                                   const double* __restrict__ Bop, int c0, int bs,
-                                                   int k_begin, int k_end,
-                                                   const double* __restrict__ D) {
-  using T = Tile<8, 4>;
-  extern __shared__ double smem[];
-  const long long m0 = (long long)blockIdx.x * T::BM;
-  const int m_rem = (int)(ng - m0 < T::BM ? ng - m0 : T::BM);
-  double acc[8][4];
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  T::accumulate(acc, smem, theta + m0, ng, Bop + c0, rk, m_rem, bs, k_begin, k_end);
+// W_K (depth-major, 64 columns, W[k*64 + n]) for column block [c0, c0+bs):
+//  forward  (rows k < c0+bs): k < c0: -sum_j L(c0+j, k) D^T(j, n);  else D^T(k-c0, n)
+//  backward (rows k >= c0):   k >= c0+bs: -sum_j L(k, c0+j) D(j, n); else D(k-c0, n)
+// with dT[j*64 + n] = D(n, j) and d[j*64 + n] = D(j, n), D = L_KK^{-1} (zero-padded).
+template <bool FORWARD>
+__global__ void __launch_bounds__(256) k_build_w(const double* __restrict__ L, int rk, int c0,
+                                                 int bs, const double* __restrict__ dmat,
+                                                 double* __restrict__ W) {
+  __shared__ double ds[kNB * kNB];
+  for (int e = threadIdx.x; e < kNB * kNB; e += 256) ds[e] = dmat[e];
   __syncthreads();
-  // stage t = rhs - acc (128 x 64, column-major, ld 128) and D (64 x 64)
-  double* ts = smem;
-  double* ds = smem + T::BM * kNB;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int c = T::col(j);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int r = T::row(i);
-      double v = 0.0;
-      if (r < m_rem && c < bs) v = theta[m0 + r + (long long)(c0 + c) * ng] - acc[i][j];
-      ts[r + c * T::BM] = v;
+  const int n = threadIdx.x & 63;
+  const int klo = FORWARD ? 0 : c0, khi = FORWARD ? c0 + bs : rk;
+  for (int k = klo + blockIdx.x * 4 + (threadIdx.x >> 6); k < khi; k += gridDim.x * 4) {
+    double v;
+    if (FORWARD ? (k < c0) : (k >= c0 + bs)) {
+      double s = 0.0;
+      for (int j = 0; j < bs; ++j) {
+        const double l = FORWARD ? L[(c0 + j) + (long long)k * rk] : L[k + (long long)(c0 + j) * rk];
+        s = fma(l, ds[j * kNB + n], s);
+      }
+      v = -s;
+    } else {
+      v = ds[(k - c0) * kNB + n];
     }
-  }
-  for (int e = threadIdx.x; e < kNB * kNB; e += 256) ds[e] = D[e];
-  __syncthreads();
-  double out[8][4];
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) out[i][j] = 0.0;
-  for (int k = 0; k < kNB; ++k) {
-    double a[8], b[4];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) a[i] = ts[T::row(i) + k * T::BM];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) b[j] = ds[k * kNB + T::col(j)];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) out[i][j] = fma(a[i], b[j], out[i][j]);
-  }
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int c = T::col(j);
-    if (c >= bs) continue;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int r = T::row(i);
-      if (r < m_rem) theta[m0 + r + (long long)(c0 + c) * ng] = out[i][j];
-    }
+    W[(long long)k * kNB + n] = v;
   }
 }
 
-constexpr size_t smem_bytes_88 = sizeof(double) * Tile<8, 8>::SMEM_DOUBLES;
-constexpr size_t smem_bytes_84 = sizeof(double) * Tile<8, 4>::SMEM_DOUBLES;
-constexpr size_t smem_bytes_trsm =
-    sizeof(double) * ((Tile<8, 4>::SMEM_DOUBLES > 128 * kNB + kNB * kNB)
-                          ? Tile<8, 4>::SMEM_DOUBLES
-                          : 128 * kNB + kNB * kNB);
+// theta[rows, c0:c0+bs] = theta[rows, kb:ke] * W[kb:ke, 0:bs], in place per row tile.
+template <int VEC>
+__global__ void __launch_bounds__(256) k_trsm_gemm(double* theta, long long ng, int c0, int bs,
+                                                   int kb, int ke, const double* __restrict__ W) {
+  extern __shared__ double smem[];
+  const long long m0 = (long long)blockIdx.x * CoreN::BM;
+  const int m_rem = (int)(ng - m0 < CoreN::BM ? ng - m0 : CoreN::BM);
+  CoreN core;
+  core.zero();
+  core.run<VEC>(smem, theta + m0, ng, W, kNB, m_rem, bs, kb, ke);
+  core.for_each([&](int r, int c, double v) {
+    if (r < m_rem && c < bs) theta[(m0 + r) + (long long)(c0 + c) * ng] = v;
+  });
+}
 
 constexpr size_t smem_bytes_potf2 = sizeof(double) * 2 * kNB * (kNB + 1);
+
+template <class K>
+int set_attr(K kernel, size_t bytes) {
+  ISDF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return ISDF_OK;
+}
 
 int set_smem_attrs() {
   static bool done_dev[64] = {};
   int dev = 0;
   ISDF_CUDA(cudaGetDevice(&dev));
   if (dev >= 0 && dev < 64 && done_dev[dev]) return ISDF_OK;
-  ISDF_CUDA(cudaFuncSetAttribute(k_potf2, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_bytes_potf2));
-  ISDF_CUDA(cudaFuncSetAttribute(k_gemm_z<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_bytes_88));
-  ISDF_CUDA(cudaFuncSetAttribute(k_gemm_z<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_bytes_88));
-  ISDF_CUDA(cudaFuncSetAttribute(k_gemm_z<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_bytes_88));
-  ISDF_CUDA(cudaFuncSetAttribute(k_chol_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_bytes_88));
-  ISDF_CUDA(cudaFuncSetAttribute(k_chol_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_bytes_84));
-  ISDF_CUDA(cudaFuncSetAttribute(k_trsm_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem_bytes_trsm));
+  ISDF_TRY(set_attr(k_potf2, smem_bytes_potf2));
+  ISDF_TRY(set_attr(k_gemm_z<0, 1>, CoreZ::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_gemm_z<1, 1>, CoreZ::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_gemm_z<2, 1>, CoreZ::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_gemm_z<0, 2>, CoreZ::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_gemm_z<1, 2>, CoreZ::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_gemm_z<2, 2>, CoreZ::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_chol_update<1>, CoreZ::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_chol_update<2>, CoreZ::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_chol_panel<1>, CoreN::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_chol_panel<2>, CoreN::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_trsm_gemm<1>, CoreN::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_trsm_gemm<2>, CoreN::SMEM_BYTES));
   if (dev >= 0 && dev < 64) done_dev[dev] = true;
   return ISDF_OK;
 }
@@ -432,8 +295,8 @@ int set_smem_attrs() {
 struct FitBuffers {
   int* piv;
   double* Bm;
-  double* P;   // C C^T, then L (column-major rk x rk)
-  double* LT;  // L^T
+  double* P;  // C C^T, then L (column-major rk x rk)
+  double* W;  // one triangular-solve block operand, rk x 64
   double* dinvT;
   double* dinv;
   double* eps;
@@ -446,7 +309,7 @@ FitBuffers carve(Arena& a, int nstate, int rk) {
   b.piv = a.take<int>(rk);
   b.Bm = a.take<double>((size_t)nstate * rk);
   b.P = a.take<double>((size_t)rk * rk);
-  b.LT = a.take<double>((size_t)rk * rk);
+  b.W = a.take<double>((size_t)rk * kNB);
   b.dinvT = a.take<double>((size_t)nblk * kNB * kNB);
   b.dinv = a.take<double>((size_t)nblk * kNB * kNB);
   b.eps = a.take<double>(1);
@@ -468,20 +331,27 @@ size_t fit_workspace_bytes(long long ng, int nstate, int rk) {
 // inverses for the solve. Returns the failing column + 1 in *info (0 = ok).
 static int cholesky(const FitBuffers& b, int rk, cudaStream_t s) {
   const int nblk = (rk + kNB - 1) / kNB;
+  const bool v2 = (rk % 2) == 0;
   for (int kb = 0; kb < nblk; ++kb) {
     const int k0 = kb * kNB;
     const int bs = min(kNB, rk - k0);
     k_potf2<<<1, 256, smem_bytes_potf2, s>>>(b.P, rk, k0, bs, b.dinvT + (size_t)kb * kNB * kNB,
-                              b.dinv + (size_t)kb * kNB * kNB, b.info);
+                                             b.dinv + (size_t)kb * kNB * kNB, b.info);
     const int rem = rk - k0 - bs;
     if (rem > 0) {
-      k_chol_panel<<<(rem + 127) / 128, 256, smem_bytes_84, s>>>(
-          b.P, rk, k0, bs, rk, b.dinvT + (size_t)kb * kNB * kNB);
-      dim3 g((rem + 127) / 128, (rem + 127) / 128);
-      k_chol_update<<<g, 256, smem_bytes_88, s>>>(b.P, rk, k0, bs, rk);
+      const double* dT = b.dinvT + (size_t)kb * kNB * kNB;
+      const unsigned pg = (unsigned)((rem + CoreN::BM - 1) / CoreN::BM);
+      dim3 g((rem + CoreZ::BN - 1) / CoreZ::BN, (rem + CoreZ::BM - 1) / CoreZ::BM);
+      if (v2) {
+        k_chol_panel<2><<<pg, 256, CoreN::SMEM_BYTES, s>>>(b.P, rk, k0, bs, rk, dT);
+        k_chol_update<2><<<g, 256, CoreZ::SMEM_BYTES, s>>>(b.P, rk, k0, bs, rk);
+      } else {
+        k_chol_panel<1><<<pg, 256, CoreN::SMEM_BYTES, s>>>(b.P, rk, k0, bs, rk, dT);
+        k_chol_update<1><<<g, 256, CoreZ::SMEM_BYTES, s>>>(b.P, rk, k0, bs, rk);
+      }
     }
   }
-  k_transpose_lower<<<grid_for((long long)rk * rk, 256), 256, 0, s>>>(b.P, rk, b.LT);
+  k_clear_upper<<<grid_for((long long)rk * rk, 256), 256, 0, s>>>(b.P, rk);
   ISDF_CHECK_LAUNCH();
   return ISDF_OK;
 }
@@ -511,7 +381,7 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
   auto mark = [&](int i) { return timed ? cudaEventRecord(ev.e[i], s) : cudaSuccess; };
   const int nblk_ = (rk + kNB - 1) / kNB;
   const bool same_ = (args.nv1 == args.nv2 && args.nc1 == args.nc2);
-  res->launches = 1 + (same_ ? 1 : 2) + 2 + (nblk_ + 2 * (nblk_ - 1) + 1) + 2 * nblk_;
+  res->launches = 1 + (same_ ? 1 : 2) + 2 + (nblk_ + 2 * (nblk_ - 1) + 1) + 4 * nblk_;
 
   ISDF_CUDA(cudaMemcpyAsync(b.piv, args.piv, sizeof(int) * rk, cudaMemcpyHostToDevice, s));
   ISDF_CUDA(cudaMemsetAsync(b.info, 0, sizeof(int), s));
@@ -522,16 +392,23 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
   const int lo1 = args.nocc - args.nv1, K1 = args.nv1 + args.nc1;
   const int lo2 = args.nocc - args.nv2, K2 = args.nv2 + args.nc2;
   const bool same = (args.nv1 == args.nv2 && args.nc1 == args.nc2);
-  dim3 zg((unsigned)((rk + 127) / 128), (unsigned)((ng + 127) / 128));
+  dim3 zg((unsigned)((rk + CoreZ::BN - 1) / CoreZ::BN), (unsigned)((ng + CoreZ::BM - 1) / CoreZ::BM));
   ISDF_CUDA(mark(0));
+  const double* A1 = args.d_psi + (long long)lo1 * ng;
+  const double* A2 = args.d_psi + (long long)lo2 * ng;
+  const double* B1 = b.Bm + (size_t)lo1 * rk;
+  const double* B2 = b.Bm + (size_t)lo2 * rk;
+  const bool zv2 = vec2_ok(A1, ng, B1, rk) && vec2_ok(A2, ng, B2, rk);
+  const size_t zs = CoreZ::SMEM_BYTES;
   if (same) {
-    k_gemm_z<0><<<zg, 256, smem_bytes_88, s>>>((int)ng, rk, K1, args.d_psi + (long long)lo1 * ng,
-                                               ng, b.Bm + (size_t)lo1 * rk, rk, args.d_theta, ng);
+    if (zv2) k_gemm_z<0, 2><<<zg, 256, zs, s>>>((int)ng, rk, K1, A1, ng, B1, rk, args.d_theta, ng);
+    else k_gemm_z<0, 1><<<zg, 256, zs, s>>>((int)ng, rk, K1, A1, ng, B1, rk, args.d_theta, ng);
+  } else if (zv2) {
+    k_gemm_z<1, 2><<<zg, 256, zs, s>>>((int)ng, rk, K1, A1, ng, B1, rk, args.d_theta, ng);
+    k_gemm_z<2, 2><<<zg, 256, zs, s>>>((int)ng, rk, K2, A2, ng, B2, rk, args.d_theta, ng);
   } else {
-    k_gemm_z<1><<<zg, 256, smem_bytes_88, s>>>((int)ng, rk, K1, args.d_psi + (long long)lo1 * ng,
-                                               ng, b.Bm + (size_t)lo1 * rk, rk, args.d_theta, ng);
-    k_gemm_z<2><<<zg, 256, smem_bytes_88, s>>>((int)ng, rk, K2, args.d_psi + (long long)lo2 * ng,
-                                               ng, b.Bm + (size_t)lo2 * rk, rk, args.d_theta, ng);
+    k_gemm_z<1, 1><<<zg, 256, zs, s>>>((int)ng, rk, K1, A1, ng, B1, rk, args.d_theta, ng);
+    k_gemm_z<2, 1><<<zg, 256, zs, s>>>((int)ng, rk, K2, A2, ng, B2, rk, args.d_theta, ng);
   }
   ISDF_CHECK_LAUNCH();
 
@@ -549,16 +426,25 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
 
   // theta L^T = Z C^T (forward over column blocks), then theta L = Y (backward)
   const int nblk = (rk + kNB - 1) / kNB;
-  const unsigned tg = (unsigned)((ng + 127) / 128);
+  const unsigned tg = (unsigned)((ng + CoreN::BM - 1) / CoreN::BM);
+  const bool tv2 = vec2_ok(args.d_theta, ng, b.W, kNB);
+  auto step = [&](int c0, int bs, int kb, int ke) {
+    if (tv2)
+      k_trsm_gemm<2><<<tg, 256, CoreN::SMEM_BYTES, s>>>(args.d_theta, ng, c0, bs, kb, ke, b.W);
+    else
+      k_trsm_gemm<1><<<tg, 256, CoreN::SMEM_BYTES, s>>>(args.d_theta, ng, c0, bs, kb, ke, b.W);
+  };
   for (int kb = 0; kb < nblk; ++kb) {
     const int c0 = kb * kNB, bs = min(kNB, rk - c0);
-    k_trsm_step<<<tg, 256, smem_bytes_trsm, s>>>(args.d_theta, ng, rk, b.P, c0, bs, 0, c0,
-                                                 b.dinvT + (size_t)kb * kNB * kNB);
+    k_build_w<true><<<(c0 + bs + 3) / 4 < 1024 ? (c0 + bs + 3) / 4 : 1024, 256, 0, s>>>(
+        b.P, rk, c0, bs, b.dinvT + (size_t)kb * kNB * kNB, b.W);
+    step(c0, bs, 0, c0 + bs);
   }
   for (int kb = nblk - 1; kb >= 0; --kb) {
     const int c0 = kb * kNB, bs = min(kNB, rk - c0);
-    k_trsm_step<<<tg, 256, smem_bytes_trsm, s>>>(args.d_theta, ng, rk, b.LT, c0, bs, c0 + bs, rk,
-                                                 b.dinv + (size_t)kb * kNB * kNB);
+    k_build_w<false><<<(rk - c0 + 3) / 4 < 1024 ? (rk - c0 + 3) / 4 : 1024, 256, 0, s>>>(
+        b.P, rk, c0, bs, b.dinv + (size_t)kb * kNB * kNB, b.W);
+    step(c0, bs, c0, rk);
   }
   ISDF_CHECK_LAUNCH();
   ISDF_CUDA(mark(3));
