@@ -12,6 +12,7 @@
 #include "common.cuh"
 #include "fit.h"
 #include "kmeans.h"
+#include "qrcp.h"
 #include "solve.h"
 
 namespace isdf_b200 {
@@ -117,14 +118,14 @@ int check_state_ranges(int nocc, int nstate, int nv1, int nc1, int nv2, int nc2)
 }
 
 size_t solve_workspace_bytes(long long ng, int nstate, int mu, int selector, int precision,
-                             int check) {
-  (void)selector;
+                             int check, double qrcp_factor) {
   (void)precision;
   (void)check;
   Arena a;
   a.counting = true;
   a.take<double>((size_t)ng);  // weight
-  size_t sel = kmeans_workspace_bytes(ng, mu);
+  size_t sel = selector == ISDF_SELECT_QRCP ? qrcp_workspace_bytes(ng, nstate, mu, qrcp_factor)
+                                            : kmeans_workspace_bytes(ng, mu);
   size_t fit = fit_workspace_bytes(ng, nstate, mu);
   return a.off + (sel > fit ? sel : fit) + 4096;
 }
@@ -148,42 +149,72 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
   if (rk <= 0 || rk > ng) return record_error(ISDF_ERR_ARG, "mu outside [1, Ng]");
   if (selector != ISDF_SELECT_KMEANS && selector != ISDF_SELECT_QRCP)
     return record_error(ISDF_ERR_ARG, "unknown selector");
-  if (selector == ISDF_SELECT_QRCP)
-    return record_error(ISDF_ERR_UNSUPPORTED, "QRCP selector not built yet");
   if (opt.precision != ISDF_PRECISION_FP64)
     return record_error(ISDF_ERR_UNSUPPORTED, "mixed precision not built yet");
   if (check) return record_error(ISDF_ERR_UNSUPPORTED, "check not built yet");
-  if (rk > kKmeansMaxMu) return record_error(ISDF_ERR_UNSUPPORTED, "mu above the K-means limit");
+  if (selector == ISDF_SELECT_KMEANS && rk > kKmeansMaxMu)
+    return record_error(ISDF_ERR_UNSUPPORTED, "mu above the K-means limit");
+  if (selector == ISDF_SELECT_QRCP && !(opt.qrcp_oversample > 0.0))
+    return record_error(ISDF_ERR_ARG, "QRCP oversampling factor must be positive");
   rep.rk_requested = rk;
 
   std::lock_guard<std::mutex> lock(workspace_mutex());
   Arena arena;
   cudaStream_t lib_stream;
-  ISDF_TRY(acquire_workspace(solve_workspace_bytes(ng, nstate, rk, selector, opt.precision, check),
-                             &arena, &lib_stream));
+  ISDF_TRY(acquire_workspace(
+      solve_workspace_bytes(ng, nstate, rk, selector, opt.precision, check, opt.qrcp_oversample),
+      &arena, &lib_stream));
   cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : lib_stream;
   double* d_w = arena.take<double>((size_t)ng);
   const size_t mark = arena.off;
 
-  // (a) K-means selection
-  KmeansArgs ka;
-  ka.d_w = d_w;
-  ka.ng = ng;
-  for (int i = 0; i < 3; ++i) {
-    ka.num_grid[i] = dom->num_grid[i];
-    ka.length[i] = dom->length[i];
+  int rk_fit = rk;
+  if (selector == ISDF_SELECT_KMEANS) {
+    // (a) K-means selection
+    KmeansArgs ka;
+    ka.d_w = d_w;
+    ka.ng = ng;
+    for (int i = 0; i < 3; ++i) {
+      ka.num_grid[i] = dom->num_grid[i];
+      ka.length[i] = dom->length[i];
+    }
+    ka.mu = rk;
+    ka.max_iter = kmeans_max_iter;
+    ka.rand_seed = opt.rand_seed;
+    ka.piv = piv;
+    ISDF_TRY(kmeans_weight(d_psi, ng, nocc, nv1, nc1, nv2, nc2, d_w, s));
+    KmeansResult kr;
+    ISDF_TRY(kmeans_select(ka, arena, s, &kr));
+    rep.rk_eff = kr.rk_eff;
+    rep.kmeans_iters = kr.iters;
+    rep.npt = kr.npt;
+    rep.kernel_launches = 1 + kr.launches;
+    rk_fit = kr.rk_eff;
+  } else {
+    // (b) QRCP selection (src/common/isdf.cpp:66-70 -> getpoints_QRCP.cpp); the
+    // fit then uses mu pivots, as the reference's getbasis does.
+    QrcpArgs qa;
+    qa.d_psi = d_psi;
+    qa.ng = ng;
+    qa.nstate = nstate;
+    qa.nocc = nocc;
+    qa.nv1 = nv1;
+    qa.nc1 = nc1;
+    qa.nv2 = nv2;
+    qa.nc2 = nc2;
+    qa.mu = rk;
+    qa.factor = opt.qrcp_oversample;
+    qa.seed = opt.qrcp_seed;
+    qa.piv = piv;
+    QrcpResult qr;
+    ISDF_TRY(qrcp_select(qa, arena, s, &qr));
+    rep.rk_eff = rk;
+    rep.kmeans_iters = 0;
+    rep.npt = qr.ntot_mg;
+    rep.kernel_launches = qr.launches;
+    rep.reserved[0] = qr.steps;
+    rep.reserved[1] = qr.nflag;
   }
-  ka.mu = rk;
-  ka.max_iter = kmeans_max_iter;
-  ka.rand_seed = opt.rand_seed;
-  ka.piv = piv;
-  ISDF_TRY(kmeans_weight(d_psi, ng, nocc, nv1, nc1, nv2, nc2, d_w, s));
-  KmeansResult kr;
-  ISDF_TRY(kmeans_select(ka, arena, s, &kr));
-  rep.rk_eff = kr.rk_eff;
-  rep.kmeans_iters = kr.iters;
-  rep.npt = kr.npt;
-  rep.kernel_launches = 1 + kr.launches;
   rep.t_select_ms = ms_since(t0);
 
   // (c, d) fit with the selected points (the GPU path fits with the shrunk
@@ -199,7 +230,7 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
   fa.nc1 = nc1;
   fa.nv2 = nv2;
   fa.nc2 = nc2;
-  fa.rk = kr.rk_eff;
+  fa.rk = rk_fit;
   fa.piv = piv;
   fa.d_theta = d_theta;
   FitResult fr;
@@ -213,9 +244,9 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
     if (rep_out) *rep_out = rep;
     return rc;
   }
-  if (kr.rk_eff < rk)
-    ISDF_CUDA(cudaMemsetAsync(d_theta + (size_t)kr.rk_eff * ng, 0,
-                              sizeof(double) * (size_t)(rk - kr.rk_eff) * ng, s));
+  if (rk_fit < rk)
+    ISDF_CUDA(cudaMemsetAsync(d_theta + (size_t)rk_fit * ng, 0,
+                              sizeof(double) * (size_t)(rk - rk_fit) * ng, s));
   ISDF_CUDA(cudaStreamSynchronize(s));
   rep.t_fit_ms = ms_since(t1);
   rep.t_total_ms = ms_since(t0);
@@ -353,7 +384,7 @@ const char* isdf_status_string(int code) {
 
 size_t isdf_workspace_bytes(long long ng, int nstate, int mu, int selector, int precision,
                             int check) {
-  return solve_workspace_bytes(ng, nstate, mu, selector, precision, check);
+  return solve_workspace_bytes(ng, nstate, mu, selector, precision, check, 1.5);
 }
 
 void isdf_release_workspace(void) {

@@ -319,6 +319,18 @@ FitBuffers carve(Arena& a, int nstate, int rk) {
 
 }  // namespace
 
+int dgemm_store(int M, int N, int K, const double* A, long long lda, const double* B,
+                long long ldb, double* C, long long ldc, cudaStream_t s) {
+  ISDF_TRY(set_smem_attrs());
+  dim3 g((unsigned)((N + CoreZ::BN - 1) / CoreZ::BN), (unsigned)((M + CoreZ::BM - 1) / CoreZ::BM));
+  if (vec2_ok(A, lda, B, ldb))
+    k_gemm_z<1, 2><<<g, 256, CoreZ::SMEM_BYTES, s>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  else
+    k_gemm_z<1, 1><<<g, 256, CoreZ::SMEM_BYTES, s>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  ISDF_CHECK_LAUNCH();
+  return ISDF_OK;
+}
+
 size_t fit_workspace_bytes(long long ng, int nstate, int rk) {
   (void)ng;
   Arena a;

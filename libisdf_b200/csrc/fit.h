@@ -24,6 +24,11 @@ struct FitResult {
 };
 
 size_t fit_workspace_bytes(long long ng, int nstate, int rk);
+
+// C = A * B on the FP64 tensor cores: A column-major (lda), B depth-major
+// (B(k, n) = B[k*ldb + n]), C column-major (ldc).
+int dgemm_store(int M, int N, int K, const double* A, long long lda, const double* B,
+                long long ldb, double* C, long long ldc, cudaStream_t s);
 // timed = false skips the stage timers (no CUDA events are created); the
 // launches are then only queued on `stream` after the Cholesky check.
 int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t stream, FitResult* res,

@@ -1,0 +1,566 @@
+// QRCP interpolation-point selection on sm_100a.
+//
+// Reference: src/cpu/getpoints_QRCP.cpp:11-500 (CPU only; the reference's GPU
+// entry point has no selector). Same algorithm:
+//   numPre = IRound(sqrt(mu * f)), f = 1.5 in the reference   (:82-86)
+//   G1, G2 = srand48(seed) Gaussian draws, orthonormal columns (:143-189)
+//   A = psi_S1 G1, B = psi_S2 G2 (Ng x numPre)                (:201-207)
+//   MG(i + j*numPre, r) = B(r, i) A(r, j); column norms        (:228-235)
+//   keep columns with norm^2 > 1e-5 * max                      (:272-284)
+//   column-pivoted QR of the kept columns; piv = MGIdx[pivots] (:440-457)
+//
+// B200 form. MG (numPre^2 x Ng: 19.5 GB at Si64 with f = 2.5) is never
+// stored. Column-pivoted Householder QR picks, at every step, the column with
+// the largest residual norm; that is the same sequence as pivoted Gram-Schmidt
+// on the columns x_r = vec(B_r (x) A_r). Step k:
+//   * pick the first column (in the current pivoted order) of maximal
+//     residual norm, swap positions as the LAPACK routine does;
+//   * q_k = x_pk orthogonalised against q_0..q_{k-1} (two passes), normalised;
+//   * every residual norm is downdated with t_r = q_k . x_r, which is
+//     t_r = sum_j A(r, j) (B_r Qm)_j, Qm(i, j) = q_k[i + j*numPre]: one
+//     FP64 tensor-core tile GEMM over all columns with the row dot fused into
+//     its epilogue, and the multiplicative downdate of LAPACK's dgeqpf,
+//     nu <- nu sqrt(max(0, 1 - (t/nu)^2)).
+// Orthonormalising G by Householder QR instead of the reference's dgesvd
+// changes G1, G2 by orthogonal factors: MG changes by an orthogonal matrix on
+// its left, which leaves the column norms and the pivot sequence unchanged.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "arena.h"
+#include "common.cuh"
+#include "dgemm.cuh"
+#include "fit.h"
+#include "qrcp.h"
+#include "solve.h"
+
+namespace isdf_b200 {
+
+namespace {
+
+constexpr int kMaxPre = 128;  // numPre limit: one 128-wide tile holds every column of Qm
+
+struct QrState {
+  unsigned long long maxbits;  // max residual norm of the active columns (bit pattern)
+  int minpos;                  // first position holding that maximum
+  int done;
+  int nflag;                   // downdates that hit LAPACK's recompute criterion
+  int ntot;
+};
+
+// ------------------------------------------------------------- norms, filter
+// Squared MG column norm per grid point, summed j-outer, i-inner with
+// explicit rounding as the reference's loop (getpoints_QRCP.cpp:228-235).
+__global__ void k_mg_norm(const double* __restrict__ A, const double* __restrict__ B, long long n,
+                          int p, double* __restrict__ norm2, QrState* st) {
+  double mx = 0.0;
+  for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int j = 0; j < p; ++j) {
+      const double a = A[r + (long long)j * n];
+      for (int i = 0; i < p; ++i) {
+        const double mg = rmul(B[r + (long long)i * n], a);
+        s = radd(s, rmul(mg, mg));
+      }
+    }
+    norm2[r] = s;
+    mx = fmax(mx, s);
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0 && mx > 0.0)
+    atomicMax(&st->maxbits, (unsigned long long)__double_as_longlong(mx));
+}
+
+__global__ void __launch_bounds__(256) k_keep_count(const double* __restrict__ norm2, long long n,
+                                                    const QrState* st, int* tile_cnt) {
+  const double thr = rmul(__longlong_as_double((long long)st->maxbits), 1e-5);
+  __shared__ int wc[8];
+  const long long base = (long long)blockIdx.x * 1024;
+  int c = 0;
+  for (int k = 0; k < 4; ++k) {
+    const long long i = base + k * 256 + threadIdx.x;
+    if (i < n && norm2[i] > thr) ++c;
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) wc[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < 8; ++w) t += wc[w];
+    tile_cnt[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_scan_tiles(int* cnt, int ntiles, int* total) {
+  __shared__ int part[1024];
+  const int per = (ntiles + 1023) / 1024;
+  const int lo = threadIdx.x * per, hi = min(lo + per, ntiles);
+  int s = 0;
+  for (int i = lo; i < hi; ++i) s += cnt[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+  for (int i = lo; i < hi; ++i) {
+    const int v = cnt[i];
+    cnt[i] = run;
+    run += v;
+  }
+  if (threadIdx.x == 1023) *total = part[1023];
+}
+
+__global__ void __launch_bounds__(256) k_keep_scatter(const double* __restrict__ norm2, long long n,
+                                                      const QrState* st, const int* tile_off,
+                                                      int* __restrict__ idx) {
+  const double thr = rmul(__longlong_as_double((long long)st->maxbits), 1e-5);
+  __shared__ int wc[8][4];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long base = (long long)blockIdx.x * 1024;
+  unsigned bal[4];
+  for (int k = 0; k < 4; ++k) {
+    const long long i = base + k * 256 + threadIdx.x;
+    bal[k] = __ballot_sync(0xffffffffu, i < n && norm2[i] > thr);
+    if (lane == 0) wc[wid][k] = __popc(bal[k]);
+  }
+  __syncthreads();
+  const int off = tile_off[blockIdx.x];
+  for (int k = 0; k < 4; ++k) {
+    int before = 0;
+    for (int kk = 0; kk < k; ++kk)
+      for (int w = 0; w < 8; ++w) before += wc[w][kk];
+    for (int w = 0; w < wid; ++w) before += wc[w][k];
+    if (bal[k] & (1u << lane))
+      idx[off + before + __popc(bal[k] & ((1u << lane) - 1u))] = (int)(base + k * 256 + threadIdx.x);
+  }
+}
+
+// Compacted operands Ac, Bc (ntot x p, column-major), residual norms, order.
+__global__ void k_compact(const double* __restrict__ A, const double* __restrict__ B, long long n,
+                          int p, const int* __restrict__ idx, const double* __restrict__ norm2,
+                          QrState* st, double* __restrict__ Ac, double* __restrict__ Bc,
+                          double* __restrict__ nu, double* __restrict__ nu0, int* __restrict__ pos,
+                          int* __restrict__ perm, unsigned char* __restrict__ active) {
+  const int ntot = st->ntot;
+  double mx = 0.0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ntot; c += gridDim.x * blockDim.x) {
+    const long long r = idx[c];
+    for (int j = 0; j < p; ++j) {
+      Ac[c + (long long)j * ntot] = A[r + (long long)j * n];
+      Bc[c + (long long)j * ntot] = B[r + (long long)j * n];
+    }
+    const double v = sqrt(norm2[r]);
+    nu[c] = v;
+    nu0[c] = v;
+    pos[c] = c;
+    perm[c] = c;
+    active[c] = 1;
+    mx = fmax(mx, v);
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0 && mx > 0.0)
+    atomicMax(&st->maxbits, (unsigned long long)__double_as_longlong(mx));
+}
+
+__global__ void k_reset_max(QrState* st) {
+  st->maxbits = 0ull;
+  st->minpos = INT_MAX;
+}
+
+// ------------------------------------------------------------- one pivot step
+// First position (in the pivoted order) holding the maximal residual norm, as
+// LAPACK's idamax over the remaining columns picks it.
+__global__ void k_argpos(const double* __restrict__ nu, const int* __restrict__ pos,
+                         const unsigned char* __restrict__ active, int ntot, QrState* st) {
+  if (st->done) return;
+  const double mx = __longlong_as_double((long long)st->maxbits);
+  int best = INT_MAX;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ntot; c += gridDim.x * blockDim.x)
+    if (active[c] && nu[c] == mx) best = min(best, pos[c]);
+  for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0 && best != INT_MAX) atomicMin(&st->minpos, best);
+}
+
+// Pivot bookkeeping (one thread) and the pivot's feature vector
+// x[i + j*p] = B(c, i) * A(c, j).
+__global__ void k_pick(int k, int p, int ntot, const double* __restrict__ Ac,
+                       const double* __restrict__ Bc, int* __restrict__ pos,
+                       int* __restrict__ perm, unsigned char* __restrict__ active,
+                       int* __restrict__ sel, QrState* st, double* __restrict__ x) {
+  __shared__ int col;
+  if (threadIdx.x == 0) {
+    col = -1;
+    const double mx = __longlong_as_double((long long)st->maxbits);
+    if (!st->done && mx > 0.0 && st->minpos != INT_MAX) {
+      const int q = st->minpos;
+      const int c = perm[q];
+      const int ck = perm[k];
+      perm[k] = c;
+      perm[q] = ck;
+      pos[ck] = q;
+      pos[c] = k;
+      active[c] = 0;
+      sel[k] = c;
+      col = c;
+    } else {
+      st->done = 1;
+    }
+    st->maxbits = 0ull;
+    st->minpos = INT_MAX;
+  }
+  __syncthreads();
+  if (col < 0) return;
+  const int m = p * p;
+  for (int e = threadIdx.x; e < m; e += blockDim.x) {
+    const int i = e % p, j = e / p;
+    x[e] = Bc[col + (long long)i * ntot] * Ac[col + (long long)j * ntot];
+  }
+}
+
+// cdot[l] = Q[:, l] . x for l < k (one warp per l).
+__global__ void k_qt_x(const double* __restrict__ Q, int m, int k, const double* __restrict__ x,
+                       const QrState* st, double* __restrict__ cdot) {
+  if (st->done) return;
+  const int l = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (l >= k) return;
+  const double* q = Q + (long long)l * m;
+  double s = 0.0;
+  for (int i = lane; i < m; i += 32) s = fma(q[i], x[i], s);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) cdot[l] = s;
+}
+
+// x -= Q[:, 0:k] cdot
+__global__ void k_x_minus_qc(const double* __restrict__ Q, int m, int k,
+                             const double* __restrict__ cdot, const QrState* st,
+                             double* __restrict__ x) {
+  if (st->done) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double s = 0.0;
+  for (int l = 0; l < k; ++l) s = fma(Q[i + (long long)l * m], cdot[l], s);
+  x[i] -= s;
+}
+
+// q_k = x / |x| into Q[:, k] and into Qm (depth-major: Qm[i*p + j] = q[i + j*p]).
+__global__ void __launch_bounds__(1024) k_normalise(int k, int p, const double* __restrict__ x,
+                                                    QrState* st, double* __restrict__ Q,
+                                                    double* __restrict__ Qm) {
+  if (st->done) return;
+  const int m = p * p;
+  __shared__ double red[32];
+  double s = 0.0;
+  for (int e = threadIdx.x; e < m; e += blockDim.x) s = fma(x[e], x[e], s);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) red[0] = v;
+  }
+  __syncthreads();
+  const double nrm = sqrt(red[0]);
+  if (!(nrm > 0.0)) {
+    if (threadIdx.x == 0) st->done = 1;
+    return;
+  }
+  const double inv = 1.0 / nrm;
+  for (int e = threadIdx.x; e < m; e += blockDim.x) {
+    const double q = x[e] * inv;
+    Q[(long long)k * m + e] = q;
+    const int i = e % p, j = e / p;
+    Qm[i * p + j] = q;
+  }
+}
+
+// Residual-norm downdate of every active column with t_c = q_k . x_c, and the
+// maximum of the new norms for the next step.
+using CoreU = dmma::Core<128, 128>;
+template <int VEC>
+__global__ void __launch_bounds__(256) k_update(const double* __restrict__ Ac,
+                                                const double* __restrict__ Bc, int ntot, int p,
+                                                const double* __restrict__ Qm,
+                                                const unsigned char* __restrict__ active,
+                                                double* __restrict__ nu,
+                                                double* __restrict__ nu0, QrState* st) {
+  if (st->done) return;
+  extern __shared__ double smem[];
+  const int m0 = blockIdx.x * CoreU::BM;
+  const int m_rem = min(CoreU::BM, ntot - m0);
+  CoreU core;
+  core.zero();
+  core.run<VEC>(smem, Bc + m0, ntot, Qm, p, m_rem, p, 0, p);
+  // row dot with A, reduced over the 4 lanes of a quad and the 4 column warps
+  double* red = smem;  // [4][128], the pipeline buffers are free again
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm0 = (warp >> 2) * CoreU::WM, wn0 = (warp & 3) * CoreU::WN;
+#pragma unroll
+  for (int i = 0; i < CoreU::MT; ++i) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = wm0 + i * 16 + g + 8 * h;
+      double s = 0.0;
+      if (r < m_rem) {
+#pragma unroll
+        for (int j = 0; j < CoreU::NT; ++j) {
+          const int c = wn0 + j * 8 + 2 * t;
+          if (c < p) s = fma(Ac[(m0 + r) + (long long)c * ntot], core.acc[i][j][2 * h], s);
+          if (c + 1 < p) s = fma(Ac[(m0 + r) + (long long)(c + 1) * ntot], core.acc[i][j][2 * h + 1], s);
+        }
+      }
+      s += __shfl_xor_sync(0xffffffffu, s, 1);
+      s += __shfl_xor_sync(0xffffffffu, s, 2);
+      if (t == 0) red[(warp & 3) * CoreU::BM + r] = s;
+    }
+  }
+  __syncthreads();
+  double mx = 0.0;
+  if (threadIdx.x < CoreU::BM && (int)threadIdx.x < m_rem) {
+    const int c = m0 + threadIdx.x;
+    if (active[c]) {
+      const double tdot = red[threadIdx.x] + red[CoreU::BM + threadIdx.x] +
+                          red[2 * CoreU::BM + threadIdx.x] + red[3 * CoreU::BM + threadIdx.x];
+      double v = nu[c];
+      if (v != 0.0) {
+        const double ratio = fabs(tdot) / v;
+        const double temp = fmax(1.0 - ratio * ratio, 0.0);
+        const double rel = v / nu0[c];
+        const double temp2 = 1.0 + 0.05 * temp * rel * rel;
+        if (temp2 == 1.0) atomicAdd(&st->nflag, 1);
+        v = v * sqrt(temp);
+        nu[c] = v;
+      }
+      mx = v;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0 && mx > 0.0)
+    atomicMax(&st->maxbits, (unsigned long long)__double_as_longlong(mx));
+}
+
+// Householder QR of the K x p draws (host, FP64): returns p orthonormal columns
+// spanning the same space, row-major (K x p) for the depth-major GEMM operand.
+std::vector<double> orthonormal_rows(const std::vector<double>& g_colmajor, int K, int p) {
+  std::vector<double> a = g_colmajor;  // column-major K x p
+  std::vector<double> tau(p, 0.0);
+  for (int j = 0; j < p; ++j) {
+    double nrm = 0.0;
+    for (int i = j; i < K; ++i) nrm += a[i + (size_t)j * K] * a[i + (size_t)j * K];
+    nrm = std::sqrt(nrm);
+    const double a0 = a[j + (size_t)j * K];
+    const double beta = a0 >= 0 ? -nrm : nrm;
+    if (nrm == 0.0) continue;
+    const double v0 = a0 - beta;
+    for (int i = j + 1; i < K; ++i) a[i + (size_t)j * K] /= v0;
+    tau[j] = (beta - a0) / beta;
+    a[j + (size_t)j * K] = beta;
+    for (int c = j + 1; c < p; ++c) {
+      double s = a[j + (size_t)c * K];
+      for (int i = j + 1; i < K; ++i) s += a[i + (size_t)j * K] * a[i + (size_t)c * K];
+      s *= tau[j];
+      a[j + (size_t)c * K] -= s;
+      for (int i = j + 1; i < K; ++i) a[i + (size_t)c * K] -= s * a[i + (size_t)j * K];
+    }
+  }
+  // Q = H_0 ... H_{p-1} I[:, 0:p]
+  std::vector<double> q((size_t)K * p, 0.0);
+  for (int j = 0; j < p; ++j) q[j + (size_t)j * K] = 1.0;
+  for (int j = p - 1; j >= 0; --j) {
+    for (int c = 0; c < p; ++c) {
+      double s = q[j + (size_t)c * K];
+      for (int i = j + 1; i < K; ++i) s += a[i + (size_t)j * K] * q[i + (size_t)c * K];
+      s *= tau[j];
+      q[j + (size_t)c * K] -= s;
+      for (int i = j + 1; i < K; ++i) q[i + (size_t)c * K] -= s * a[i + (size_t)j * K];
+    }
+  }
+  std::vector<double> rows((size_t)K * p);
+  for (int i = 0; i < K; ++i)
+    for (int j = 0; j < p; ++j) rows[(size_t)i * p + j] = q[i + (size_t)j * K];
+  return rows;
+}
+
+// srand48 Gaussian draws as include/common/utility.hpp:455-471: column-major.
+std::vector<double> gaussian_draws(int m, int n) {
+  std::vector<double> g((size_t)m * n);
+  const double pi = 3.14159265358979323846;
+  for (auto& v : g) {
+    const double a = drand48(), b = drand48();
+    v = std::sqrt(-2.0 * std::log(a)) * std::cos(2.0 * pi * b);
+  }
+  return g;
+}
+
+struct QrBuffers {
+  double *A, *B, *norm2, *Ac, *Bc, *nu, *nu0, *Q, *Qm, *x, *cdot, *G1, *G2;
+  int *idx, *pos, *perm, *sel, *tile_cnt;
+  unsigned char* active;
+  QrState* st;
+};
+
+QrBuffers carve(Arena& a, long long n, int p, int k1, int k2, int kmax) {
+  QrBuffers b;
+  const int m = p * p;
+  const int ntiles = (int)((n + 1023) / 1024);
+  b.A = a.take<double>((size_t)n * p);
+  b.B = a.take<double>((size_t)n * p);
+  b.norm2 = a.take<double>((size_t)n);
+  b.Ac = a.take<double>((size_t)n * p);
+  b.Bc = a.take<double>((size_t)n * p);
+  b.nu = a.take<double>((size_t)n);
+  b.nu0 = a.take<double>((size_t)n);
+  b.Q = a.take<double>((size_t)m * kmax);
+  b.Qm = a.take<double>((size_t)m);
+  b.x = a.take<double>((size_t)m);
+  b.cdot = a.take<double>((size_t)kmax);
+  b.G1 = a.take<double>((size_t)k1 * p);
+  b.G2 = a.take<double>((size_t)k2 * p);
+  b.idx = a.take<int>((size_t)n);
+  b.pos = a.take<int>((size_t)n);
+  b.perm = a.take<int>((size_t)n);
+  b.sel = a.take<int>((size_t)kmax);
+  b.tile_cnt = a.take<int>((size_t)ntiles);
+  b.active = a.take<unsigned char>((size_t)n);
+  b.st = a.take<QrState>(1);
+  return b;
+}
+
+int set_update_attrs() {
+  static bool done[64] = {};
+  int dev = 0;
+  ISDF_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && done[dev]) return ISDF_OK;
+  ISDF_CUDA(cudaFuncSetAttribute(k_update<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)CoreU::SMEM_BYTES));
+  ISDF_CUDA(cudaFuncSetAttribute(k_update<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)CoreU::SMEM_BYTES));
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return ISDF_OK;
+}
+
+}  // namespace
+
+int qrcp_num_pre(int mu, double factor) { return iround(std::sqrt(mu * factor)); }
+
+size_t qrcp_workspace_bytes(long long ng, int nstate, int mu, double factor) {
+  const int p = qrcp_num_pre(mu, factor);
+  Arena a;
+  a.counting = true;
+  carve(a, ng, p, nstate, nstate, std::min(mu, p * p));
+  return a.off;
+}
+
+int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* res) {
+  const long long n = args.ng;
+  const int p = qrcp_num_pre(args.mu, args.factor);
+  const int k1 = args.nv1 + args.nc1, k2 = args.nv2 + args.nc2;
+  if (p > args.nstate)
+    return record_error(ISDF_ERR_ARG,
+                        "numMu is too large for interpolative separable density fitting!");
+  if ((long long)p * p > n)
+    return record_error(ISDF_ERR_ARG, "numPre*numPre > ntot. The number of grid points is perhaps too small!");
+  if (p > k1 || p > k2)
+    return record_error(ISDF_ERR_UNSUPPORTED, "QRCP: numPre exceeds a state window");
+  if (p > kMaxPre) return record_error(ISDF_ERR_UNSUPPORTED, "QRCP: numPre above 128");
+  if (n > 0x7fffffffLL) return record_error(ISDF_ERR_UNSUPPORTED, "QRCP: Ng >= 2^31");
+  const int m = p * p;
+  const int kmax_cap = std::min(args.mu, m);
+  QrBuffers b = carve(arena, n, p, k1, k2, kmax_cap);
+  if (arena.overflowed()) return record_error(ISDF_ERR_NOMEM, "QRCP: workspace too small");
+  ISDF_TRY(set_update_attrs());
+  int launches = 0;
+
+  // sketch (host): srand48(seed), G1 then G2, orthonormal columns
+  srand48((long)args.seed);
+  std::vector<double> g1 = gaussian_draws(k1, p);
+  std::vector<double> g2 = gaussian_draws(k2, p);
+  std::vector<double> q1 = orthonormal_rows(g1, k1, p);
+  std::vector<double> q2 = orthonormal_rows(g2, k2, p);
+  ISDF_CUDA(cudaMemcpyAsync(b.G1, q1.data(), sizeof(double) * q1.size(), cudaMemcpyHostToDevice, s));
+  ISDF_CUDA(cudaMemcpyAsync(b.G2, q2.data(), sizeof(double) * q2.size(), cudaMemcpyHostToDevice, s));
+  ISDF_CUDA(cudaMemsetAsync(b.st, 0, sizeof(QrState), s));
+
+  // A = psi_S1 G1, B = psi_S2 G2
+  ISDF_TRY(dgemm_store((int)n, p, k1, args.d_psi + (long long)(args.nocc - args.nv1) * n, n, b.G1,
+                       p, b.A, n, s));
+  ISDF_TRY(dgemm_store((int)n, p, k2, args.d_psi + (long long)(args.nocc - args.nv2) * n, n, b.G2,
+                       p, b.B, n, s));
+  launches += 2;
+
+  // norms, filter, compaction
+  const int ntiles = (int)((n + 1023) / 1024);
+  k_mg_norm<<<kNumSMs * 8, 256, 0, s>>>(b.A, b.B, n, p, b.norm2, b.st);
+  k_keep_count<<<ntiles, 256, 0, s>>>(b.norm2, n, b.st, b.tile_cnt);
+  k_scan_tiles<<<1, 1024, 0, s>>>(b.tile_cnt, ntiles, &b.st->ntot);
+  k_keep_scatter<<<ntiles, 256, 0, s>>>(b.norm2, n, b.st, b.tile_cnt, b.idx);
+  k_reset_max<<<1, 1, 0, s>>>(b.st);
+  k_compact<<<kNumSMs * 4, 256, 0, s>>>(b.A, b.B, n, p, b.idx, b.norm2, b.st, b.Ac, b.Bc, b.nu,
+                                        b.nu0, b.pos, b.perm, b.active);
+  launches += 6;
+  ISDF_CHECK_LAUNCH();
+  QrState hst;
+  ISDF_CUDA(cudaMemcpyAsync(&hst, b.st, sizeof(QrState), cudaMemcpyDeviceToHost, s));
+  ISDF_CUDA(cudaStreamSynchronize(s));
+  const int ntot = hst.ntot;
+  const int kmax = std::min(kmax_cap, ntot);
+  res->ntot_mg = ntot;
+
+  // pivoted Gram-Schmidt over the kept columns
+  const unsigned ugrid = (unsigned)((ntot + CoreU::BM - 1) / CoreU::BM);
+  const bool uv2 = ((reinterpret_cast<size_t>(b.Bc) | reinterpret_cast<size_t>(b.Qm)) & 15) == 0 &&
+                   ntot % 2 == 0 && p % 2 == 0;
+  const unsigned agrid = (unsigned)std::min(kNumSMs * 8, (ntot + 255) / 256);
+  for (int k = 0; k < kmax; ++k) {
+    k_argpos<<<agrid, 256, 0, s>>>(b.nu, b.pos, b.active, ntot, b.st);
+    k_pick<<<1, 1024, 0, s>>>(k, p, ntot, b.Ac, b.Bc, b.pos, b.perm, b.active, b.sel, b.st, b.x);
+    launches += 2;
+    if (k > 0) {
+      for (int pass = 0; pass < 2; ++pass) {
+        k_qt_x<<<(k + 7) / 8, 256, 0, s>>>(b.Q, m, k, b.x, b.st, b.cdot);
+        k_x_minus_qc<<<(m + 255) / 256, 256, 0, s>>>(b.Q, m, k, b.cdot, b.st, b.x);
+        launches += 2;
+      }
+    }
+    k_normalise<<<1, 1024, 0, s>>>(k, p, b.x, b.st, b.Q, b.Qm);
+    if (uv2)
+      k_update<2><<<ugrid, 256, CoreU::SMEM_BYTES, s>>>(b.Ac, b.Bc, ntot, p, b.Qm, b.active, b.nu,
+                                                        b.nu0, b.st);
+    else
+      k_update<1><<<ugrid, 256, CoreU::SMEM_BYTES, s>>>(b.Ac, b.Bc, ntot, p, b.Qm, b.active, b.nu,
+                                                        b.nu0, b.st);
+    launches += 2;
+    if ((k & 255) == 255) ISDF_CHECK_LAUNCH();
+  }
+  ISDF_CHECK_LAUNCH();
+
+  // piv = MGIdx[pivots], then the remaining kept columns in pivoted order, then 0
+  std::vector<int> idx(ntot), perm(ntot), sel(kmax);
+  ISDF_CUDA(cudaMemcpyAsync(&hst, b.st, sizeof(QrState), cudaMemcpyDeviceToHost, s));
+  ISDF_CUDA(cudaMemcpyAsync(idx.data(), b.idx, sizeof(int) * ntot, cudaMemcpyDeviceToHost, s));
+  ISDF_CUDA(cudaMemcpyAsync(perm.data(), b.perm, sizeof(int) * ntot, cudaMemcpyDeviceToHost, s));
+  if (kmax > 0)
+    ISDF_CUDA(cudaMemcpyAsync(sel.data(), b.sel, sizeof(int) * kmax, cudaMemcpyDeviceToHost, s));
+  ISDF_CUDA(cudaStreamSynchronize(s));
+  std::memset(args.piv, 0, sizeof(int) * (size_t)n);
+  for (int j = 0; j < ntot; ++j) args.piv[j] = idx[perm[j]];
+  res->steps = kmax;
+  res->num_pre = p;
+  res->nflag = hst.nflag;
+  res->done_early = hst.done;
+  res->launches = launches;
+  return ISDF_OK;
+}
+
+}  // namespace isdf_b200

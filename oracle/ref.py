@@ -35,6 +35,8 @@ def lib():
         _lib.ref_weight.argtypes = [P, I, I, I, I, I, I, P]
         _lib.ref_bench_kmeans_step.argtypes = [I, I, I]
         _lib.ref_bench_kmeans_step.restype = ctypes.c_double
+        _lib.ref_qrcp_sketch.argtypes = [I, I, I, ctypes.c_long, P, P]
+        _lib.ref_qrcp_gaussians.argtypes = [I, I, I, ctypes.c_long, P, P]
         _lib.ref_iround.argtypes = [ctypes.c_double]
         _lib.ref_iround.restype = I
     return _lib
@@ -137,3 +139,12 @@ def bench_getbasis_rows(psi, shape, fraction: int, repeats: int = 1) -> float:
                  shape.nc2, shape.mu, piv)
         best = min(best, time.perf_counter() - t0)
     return best
+
+
+def qrcp_sketch(k1: int, k2: int, num_pre: int, seed: int, orth: bool = True):
+    """G1, G2 of the reference's QRCP (srand48 + GaussianRandom [+ lapack::Orth])."""
+    g1 = np.zeros((k1, num_pre), order="F")
+    g2 = np.zeros((k2, num_pre), order="F")
+    f = lib().ref_qrcp_sketch if orth else lib().ref_qrcp_gaussians
+    f(k1, k2, num_pre, seed, _ptr(g1), _ptr(g2))
+    return g1, g2

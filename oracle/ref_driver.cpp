@@ -202,6 +202,33 @@ double ref_bench_kmeans_step(int npt, int rk, int repeats) {
   return best;
 }
 
+// The QRCP sketch of src/cpu/getpoints_QRCP.cpp:143-189 at rank 0:
+// srand48(seed) (the caller's seed; isdf.cpp:68 uses 41), G1 then G2 filled
+// column by column with GaussianRandom (include/common/utility.hpp:455-471),
+// each orthonormalised by lapack::Orth (dgesvd jobu='O', src/cpu/lapack.cpp:115-147).
+void ref_qrcp_sketch(int k1, int k2, int num_pre, long seed, double* g1, double* g2) {
+  srand48(seed);
+  DblNumMat G1(k1, num_pre), G2(k2, num_pre);
+  SetValue(G1, 0.0);
+  SetValue(G2, 0.0);
+  GaussianRandom(G1);
+  GaussianRandom(G2);
+  lapack::Orth(k1, num_pre, G1.Data(), k1);
+  lapack::Orth(k2, num_pre, G2.Data(), k2);
+  std::memcpy(g1, G1.Data(), sizeof(double) * (size_t)k1 * num_pre);
+  std::memcpy(g2, G2.Data(), sizeof(double) * (size_t)k2 * num_pre);
+}
+
+// The raw Gaussian draws (before Orth), same order.
+void ref_qrcp_gaussians(int k1, int k2, int num_pre, long seed, double* g1, double* g2) {
+  srand48(seed);
+  DblNumMat G1(k1, num_pre), G2(k2, num_pre);
+  GaussianRandom(G1);
+  GaussianRandom(G2);
+  std::memcpy(g1, G1.Data(), sizeof(double) * (size_t)k1 * num_pre);
+  std::memcpy(g2, G2.Data(), sizeof(double) * (size_t)k2 * num_pre);
+}
+
 // The reference's integer rounding IRound (include/common/utility.hpp:18-23),
 // used for the default mu and the QRCP sketch width.
 int ref_iround(double a) { return IRound(a); }
