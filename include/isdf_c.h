@@ -123,6 +123,17 @@ int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, i
              int nc2, int rk, const int* piv, double* d_theta, int precision, int refine_steps,
              int* chol_info, void* stream);
 
+/* The check of the reference (src/common/checkcode.cpp:54-313, called by
+ * src/common/isdf.cpp:193-206 when check = true): the pair-density fit error
+ * ||rho - theta C||_F / ||rho||_F and the relative truncated-Coulomb (R = 5)
+ * 4-index error of the ISDF form, here with cuFFT D2Z half spectra. The
+ * reference prints both; here they are returned. Cost O(Ng * Npair^2), Npair =
+ * (nv1+nc1)(nv2+nc2): sizes whose pair spectra exceed the device budget
+ * return ISDF_ERR_UNSUPPORTED. piv: host, first rk entries used. */
+int isdf_check(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, int nv1,
+               int nc1, int nv2, int nc2, int rk, const int* piv, const double* d_theta,
+               double* fit_err, double* coul_err, void* stream);
+
 /* Size of the fixed device scratch array behind isdf_fit_noalloc(). */
 #define ISDF_NOALLOC_SCRATCH_BYTES (8u << 20)
 

@@ -156,6 +156,8 @@ def lib() -> ctypes.CDLL:
         L.isdf_kmeans_select.restype = I
         L.isdf_fit.argtypes = [P, LL, I, I, I, I, I, I, I, P, P, I, I, P, P]
         L.isdf_fit.restype = I
+        L.isdf_check.argtypes = [ctypes.POINTER(_Domain), P, I, I, I, I, I, I, I, P, P, P, P, P]
+        L.isdf_check.restype = I
         L.isdf_last_error.restype = ctypes.c_char_p
         L.isdf_status_string.argtypes = [I]
         L.isdf_status_string.restype = ctypes.c_char_p
@@ -244,6 +246,19 @@ def fit(d_psi, ng: int, nstate: int, nocc: int, nv1: int, nc1: int, nv2: int, nc
                         stream or None)
     _check(rc)
     return info.value
+
+
+def check(domain: Domain, d_psi, nocc: int, nstate: int, nv1: int, nc1: int, nv2: int, nc2: int,
+          rk: int, piv: np.ndarray, d_theta, stream: int = 0):
+    """(fit error, Coulomb error) of theta, as the reference's checkcode computes them."""
+    piv = np.ascontiguousarray(piv, dtype=np.int32)
+    fe = ctypes.c_double(0.0)
+    ce = ctypes.c_double(0.0)
+    d = domain._c()
+    _check(lib().isdf_check(ctypes.byref(d), _dptr(d_psi), nocc, nstate, nv1, nc1, nv2, nc2, rk,
+                            piv.ctypes.data, _dptr(d_theta), ctypes.addressof(fe),
+                            ctypes.addressof(ce), stream or None))
+    return fe.value, ce.value
 
 
 def workspace_bytes(ng: int, nstate: int, mu: int, selector: int = SELECT_KMEANS,

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "arena.h"
+#include "check.h"
 #include "common.cuh"
 #include "fit.h"
 #include "kmeans.h"
@@ -117,17 +118,21 @@ int check_state_ranges(int nocc, int nstate, int nv1, int nc1, int nv2, int nc2)
   return ISDF_OK;
 }
 
+constexpr size_t kCheckMaxBytes = 48ull << 30;
+
 size_t solve_workspace_bytes(long long ng, int nstate, int mu, int selector, int precision,
-                             int check, double qrcp_factor) {
+                             int check, double qrcp_factor, const int* num_grid, int npair) {
   (void)precision;
-  (void)check;
   Arena a;
   a.counting = true;
   a.take<double>((size_t)ng);  // weight
   size_t sel = selector == ISDF_SELECT_QRCP ? qrcp_workspace_bytes(ng, nstate, mu, qrcp_factor)
                                             : kmeans_workspace_bytes(ng, mu);
   size_t fit = fit_workspace_bytes(ng, nstate, mu);
-  return a.off + (sel > fit ? sel : fit) + 4096;
+  size_t chk = (check && num_grid) ? check_workspace_bytes(num_grid, nstate, mu, npair) : 0;
+  size_t big = sel > fit ? sel : fit;
+  if (chk > big) big = chk;
+  return a.off + big + 4096;
 }
 
 int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, int nv1, int nc1,
@@ -151,7 +156,10 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
     return record_error(ISDF_ERR_ARG, "unknown selector");
   if (opt.precision != ISDF_PRECISION_FP64)
     return record_error(ISDF_ERR_UNSUPPORTED, "mixed precision not built yet");
-  if (check) return record_error(ISDF_ERR_UNSUPPORTED, "check not built yet");
+  if (check && check_workspace_bytes(dom->num_grid, nstate, rk, (nv1 + nc1) * (nv2 + nc2)) >
+                   kCheckMaxBytes)
+    return record_error(ISDF_ERR_UNSUPPORTED,
+                        "check: O(Ng * Npair) pair spectra exceed the device budget at this size");
   if (selector == ISDF_SELECT_KMEANS && rk > kKmeansMaxMu)
     return record_error(ISDF_ERR_UNSUPPORTED, "mu above the K-means limit");
   if (selector == ISDF_SELECT_QRCP && !(opt.qrcp_oversample > 0.0))
@@ -162,7 +170,8 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
   Arena arena;
   cudaStream_t lib_stream;
   ISDF_TRY(acquire_workspace(
-      solve_workspace_bytes(ng, nstate, rk, selector, opt.precision, check, opt.qrcp_oversample),
+      solve_workspace_bytes(ng, nstate, rk, selector, opt.precision, check, opt.qrcp_oversample,
+                            dom->num_grid, (nv1 + nc1) * (nv2 + nc2)),
       &arena, &lib_stream));
   cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : lib_stream;
   double* d_w = arena.take<double>((size_t)ng);
@@ -249,6 +258,28 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
                               sizeof(double) * (size_t)(rk - rk_fit) * ng, s));
   ISDF_CUDA(cudaStreamSynchronize(s));
   rep.t_fit_ms = ms_since(t1);
+  if (check) {
+    // (e) the check of src/common/isdf.cpp:193-206 -> checkcode.cpp
+    auto t2 = std::chrono::steady_clock::now();
+    arena.off = mark;
+    CheckArgs ca;
+    ca.d_psi = d_psi;
+    for (int i = 0; i < 3; ++i) {
+      ca.num_grid[i] = dom->num_grid[i];
+      ca.length[i] = dom->length[i];
+    }
+    ca.nstate = nstate;
+    ca.nocc = nocc;
+    ca.nv1 = nv1;
+    ca.nc1 = nc1;
+    ca.nv2 = nv2;
+    ca.nc2 = nc2;
+    ca.rk = rk_fit;
+    ca.piv = piv;
+    ca.d_theta = d_theta;
+    ISDF_TRY(check_run(ca, arena, s, &rep.fit_err, &rep.coul_err));
+    rep.t_check_ms = ms_since(t2);
+  }
   rep.t_total_ms = ms_since(t0);
   if (rep_out) *rep_out = rep;
   return ISDF_OK;
@@ -365,6 +396,45 @@ int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, i
   }
 }
 
+int isdf_check(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, int nv1,
+               int nc1, int nv2, int nc2, int rk, const int* piv, const double* d_theta,
+               double* fit_err, double* coul_err, void* stream) {
+  try {
+    if (!dom || !d_psi || !d_theta || !piv || !fit_err || !coul_err)
+      return record_error(ISDF_ERR_ARG, "null pointer");
+    const long long ng = (long long)dom->num_grid[0] * dom->num_grid[1] * dom->num_grid[2];
+    if (ng <= 0 || rk <= 0 || rk > ng) return record_error(ISDF_ERR_ARG, "sizes");
+    ISDF_TRY(check_state_ranges(nocc, nstate, nv1, nc1, nv2, nc2));
+    for (int j = 0; j < rk; ++j)
+      if (piv[j] < 0 || piv[j] >= ng) return record_error(ISDF_ERR_ARG, "pivot outside the grid");
+    const size_t need = check_workspace_bytes(dom->num_grid, nstate, rk, (nv1 + nc1) * (nv2 + nc2));
+    if (need > kCheckMaxBytes)
+      return record_error(ISDF_ERR_UNSUPPORTED, "check: pair spectra exceed the device budget");
+    std::lock_guard<std::mutex> lock(workspace_mutex());
+    Arena arena;
+    cudaStream_t ls;
+    ISDF_TRY(acquire_workspace(need + 4096, &arena, &ls));
+    CheckArgs ca;
+    ca.d_psi = d_psi;
+    for (int i = 0; i < 3; ++i) {
+      ca.num_grid[i] = dom->num_grid[i];
+      ca.length[i] = dom->length[i];
+    }
+    ca.nstate = nstate;
+    ca.nocc = nocc;
+    ca.nv1 = nv1;
+    ca.nc1 = nc1;
+    ca.nv2 = nv2;
+    ca.nc2 = nc2;
+    ca.rk = rk;
+    ca.piv = piv;
+    ca.d_theta = d_theta;
+    return check_run(ca, arena, stream ? (cudaStream_t)stream : ls, fit_err, coul_err);
+  } catch (const std::exception& e) {
+    return record_error(ISDF_ERR_NOMEM, e.what());
+  }
+}
+
 const char* isdf_last_error(void) { return last_error_message(); }
 
 const char* isdf_status_string(int code) {
@@ -384,7 +454,7 @@ const char* isdf_status_string(int code) {
 
 size_t isdf_workspace_bytes(long long ng, int nstate, int mu, int selector, int precision,
                             int check) {
-  return solve_workspace_bytes(ng, nstate, mu, selector, precision, check, 1.5);
+  return solve_workspace_bytes(ng, nstate, mu, selector, precision, 0, 1.5, nullptr, 0);
 }
 
 void isdf_release_workspace(void) {

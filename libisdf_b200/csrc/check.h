@@ -1,0 +1,25 @@
+// Host-side entry points of the check (check.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "arena.h"
+
+namespace isdf_b200 {
+
+struct CheckArgs {
+  const double* d_psi;  // Ng x nstate, ld = Ng
+  int num_grid[3];
+  double length[3];
+  int nstate, nocc, nv1, nc1, nv2, nc2;
+  int rk;
+  const int* piv;        // host, first rk entries
+  const double* d_theta;  // Ng x rk, ld = Ng
+};
+
+size_t check_workspace_bytes(const int* num_grid, int nstate, int rk, int npair);
+int check_run(const CheckArgs& args, Arena& arena, cudaStream_t s, double* fit_err,
+              double* coul_err);
+
+}  // namespace isdf_b200

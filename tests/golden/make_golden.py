@@ -105,7 +105,7 @@ def main():
     raw = rng.standard_normal((10 * 12 * 14, 6)) * np.exp(
         -0.5 * rng.uniform(0, 3, size=(10 * 12 * 14, 1)))
     psi = np.asfortranarray(np.linalg.qr(raw)[0])
-    save("small_mu0", psi, (10, 12, 14), (9.0, 10.0, 11.0), 3, 3, 3, 3, 3, 0, 30)
+    save("small_mu0", psi, (10, 12, 14), (9.0, 10.0, 11.0), 3, 3, 3, 3, 3, 0, 30, check=True)
 
     # 4. KmeansMaxIter = 0: the initial assignment feeds the final argmin.
     psi = synth.orbitals(10, 1, 8, seed=13)
