@@ -44,7 +44,7 @@ extern "C" {
 #define ISDF_SELECT_QRCP 1
 
 #define ISDF_PRECISION_FP64 0  /* the reference's FP64 method */
-#define ISDF_PRECISION_MIXED 1 /* split-BF16 tensor-core GEMMs + FP64 refinement */
+#define ISDF_PRECISION_MIXED 1 /* INT8-sliced tcgen05 GEMMs, FP64 Cholesky / inverse */
 
 /* Layout-compatible with the numeric fields of the reference's Domain
  * (include/common/domain.hpp:8-36); the MPI communicators are not needed
@@ -64,7 +64,8 @@ typedef struct isdf_options_t {
   long long rand_seed;    /* >= 0: srand() before K-means (only its npt < mu branch
                              draws from rand()); < 0: keep the process state */
   void* stream;           /* cudaStream_t to run on; NULL = library stream */
-  int reserved[8];
+  int mixed_slices;       /* mixed precision: INT8 slices per FP64 operand, 5..7 (default 6) */
+  int reserved[7];
 } isdf_options_t;
 
 typedef struct isdf_report_t {

@@ -60,7 +60,7 @@ class _Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("refine_steps", ctypes.c_int),
                 ("qrcp_oversample", ctypes.c_double), ("qrcp_seed", ctypes.c_longlong),
                 ("rand_seed", ctypes.c_longlong), ("stream", ctypes.c_void_p),
-                ("reserved", ctypes.c_int * 8)]
+                ("mixed_slices", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
 
 
 class _Report(ctypes.Structure):
@@ -104,6 +104,7 @@ class Options:
     qrcp_seed: int = 41
     rand_seed: int = -1
     stream: int = 0
+    mixed_slices: int = 6
 
     def _c(self) -> _Options:
         o = _Options()
@@ -113,6 +114,7 @@ class Options:
         o.qrcp_seed = self.qrcp_seed
         o.rand_seed = self.rand_seed
         o.stream = self.stream or None
+        o.mixed_slices = self.mixed_slices
         return o
 
 

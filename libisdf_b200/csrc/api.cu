@@ -128,7 +128,8 @@ size_t solve_workspace_bytes(long long ng, int nstate, int mu, int selector, int
   a.take<double>((size_t)ng);  // weight
   size_t sel = selector == ISDF_SELECT_QRCP ? qrcp_workspace_bytes(ng, nstate, mu, qrcp_factor)
                                             : kmeans_workspace_bytes(ng, mu);
-  size_t fit = fit_workspace_bytes(ng, nstate, mu);
+  size_t fit = precision == ISDF_PRECISION_MIXED ? fit_mixed_workspace_bytes(ng, nstate, mu, 7)
+                                                 : fit_workspace_bytes(ng, nstate, mu);
   size_t chk = (check && num_grid) ? check_workspace_bytes(num_grid, nstate, mu, npair) : 0;
   size_t big = sel > fit ? sel : fit;
   if (chk > big) big = chk;
@@ -154,8 +155,10 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
   if (rk <= 0 || rk > ng) return record_error(ISDF_ERR_ARG, "mu outside [1, Ng]");
   if (selector != ISDF_SELECT_KMEANS && selector != ISDF_SELECT_QRCP)
     return record_error(ISDF_ERR_ARG, "unknown selector");
-  if (opt.precision != ISDF_PRECISION_FP64)
-    return record_error(ISDF_ERR_UNSUPPORTED, "mixed precision not built yet");
+  if (opt.precision != ISDF_PRECISION_FP64 && opt.precision != ISDF_PRECISION_MIXED)
+    return record_error(ISDF_ERR_ARG, "unknown precision");
+  if (opt.precision == ISDF_PRECISION_MIXED && (opt.mixed_slices < 5 || opt.mixed_slices > 7))
+    return record_error(ISDF_ERR_ARG, "mixed_slices must be 5, 6 or 7");
   if (check && check_workspace_bytes(dom->num_grid, nstate, rk, (nv1 + nc1) * (nv2 + nc2)) >
                    kCheckMaxBytes)
     return record_error(ISDF_ERR_UNSUPPORTED,
@@ -243,7 +246,8 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
   fa.piv = piv;
   fa.d_theta = d_theta;
   FitResult fr;
-  int rc = fit_fp64(fa, arena, s, &fr);
+  int rc = opt.precision == ISDF_PRECISION_MIXED ? fit_mixed(fa, arena, s, &fr, opt.mixed_slices)
+                                                 : fit_fp64(fa, arena, s, &fr);
   rep.chol_info = fr.chol_info;
   rep.kernel_launches += fr.launches;
   rep.t_zct_ms = fr.t_zct_ms;
@@ -300,6 +304,7 @@ void isdf_default_options(isdf_options_t* opt) {
   opt->qrcp_seed = 41;
   opt->rand_seed = -1;
   opt->stream = nullptr;
+  opt->mixed_slices = 6;
 }
 
 int isdf_solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, int nv1,
@@ -367,12 +372,15 @@ int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, i
     ISDF_TRY(check_state_ranges(nocc, nstate, nv1, nc1, nv2, nc2));
     for (int j = 0; j < rk; ++j)
       if (piv[j] < 0 || piv[j] >= ng) return record_error(ISDF_ERR_ARG, "pivot outside the grid");
-    if (precision != ISDF_PRECISION_FP64)
-      return record_error(ISDF_ERR_UNSUPPORTED, "mixed precision not built yet");
+    if (precision != ISDF_PRECISION_FP64 && precision != ISDF_PRECISION_MIXED)
+      return record_error(ISDF_ERR_ARG, "unknown precision");
     std::lock_guard<std::mutex> lock(workspace_mutex());
     Arena arena;
     cudaStream_t ls;
-    ISDF_TRY(acquire_workspace(fit_workspace_bytes(ng, nstate, rk) + 4096, &arena, &ls));
+    const size_t need = precision == ISDF_PRECISION_MIXED
+                            ? fit_mixed_workspace_bytes(ng, nstate, rk, 7)
+                            : fit_workspace_bytes(ng, nstate, rk);
+    ISDF_TRY(acquire_workspace(need + 4096, &arena, &ls));
     FitArgs fa;
     fa.d_psi = d_psi;
     fa.ng = ng;
@@ -387,7 +395,8 @@ int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, i
     fa.d_theta = d_theta;
     FitResult fr;
     cudaStream_t s = stream ? (cudaStream_t)stream : ls;
-    int rc = fit_fp64(fa, arena, s, &fr);
+    int rc = precision == ISDF_PRECISION_MIXED ? fit_mixed(fa, arena, s, &fr, 6)
+                                               : fit_fp64(fa, arena, s, &fr);
     if (chol_info) *chol_info = fr.chol_info;
     if (rc == ISDF_OK) ISDF_CUDA(cudaStreamSynchronize(s));
     return rc;

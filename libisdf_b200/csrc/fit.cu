@@ -34,6 +34,7 @@
 #include "common.cuh"
 #include "dgemm.cuh"
 #include "fit.h"
+#include "ozaki.cuh"
 
 namespace isdf_b200 {
 
@@ -466,6 +467,240 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
   ISDF_CUDA(cudaEventElapsedTime(&res->t_chol_ms, ev.e[1], ev.e[2]));
   ISDF_CUDA(cudaEventElapsedTime(&res->t_solve_ms, ev.e[2], ev.e[3]));
   return ISDF_OK;
+}
+
+
+// ===================================================================== mixed
+// Mixed-precision form: the three large products (Z C^T, Y = Z L^{-T},
+// theta = Y L^{-1}) as INT8-sliced GEMMs on the tcgen05 tensor cores
+// (ozaki.cuh); C C^T, the Cholesky factorisation and L^{-T} stay FP64.
+// theta = (Z C^T L^{-T}) L^{-1} with explicit triangular inverses, whose
+// rounding is that of two FP64 TRMMs when S >= 7 slices.
+
+namespace {
+
+constexpr int kSliceTile = 64;  // rows per slicing tile
+constexpr int kSliceK = 32;     // K bytes per slicing tile
+
+// Row-scaled slicing of an M x K FP64 operand, element (m, k) at
+// X[m*rs + k*ks], into S planes P[t*plane + m*ldk + k] of int8 (rows padded to
+// mp, columns to kp, zeros there) and exponents e[m] (|x| 2^-e < 1/2).
+__global__ void k_row_exponent(const double* __restrict__ X, long long rs, long long ks, int M,
+                               int K, int* __restrict__ e) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
+    double mx = 0.0;
+    for (int k = 0; k < K; ++k) mx = fmax(mx, fabs(X[m * rs + k * ks]));
+    e[m] = mx > 0.0 ? ilogb(mx) + 2 : 0;
+  }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) k_slice(const double* __restrict__ X, long long rs,
+                                               long long ks, int M, int K, int mp, int kp,
+                                               const int* __restrict__ e, int8_t* __restrict__ P,
+                                               long long plane, int ldk) {
+  __shared__ double xs[kSliceTile][kSliceK + 1];
+  __shared__ __align__(16) int8_t qs[S][kSliceTile][kSliceK];
+  const int m0 = blockIdx.y * kSliceTile, k0 = blockIdx.x * kSliceK;
+  const bool mfast = rs == 1;
+  for (int i = threadIdx.x; i < kSliceTile * kSliceK; i += 256) {
+    const int mi = mfast ? i % kSliceTile : i / kSliceK;
+    const int ki = mfast ? i / kSliceTile : i % kSliceK;
+    const int m = m0 + mi, k = k0 + ki;
+    xs[mi][ki] = (m < M && k < K) ? X[(long long)m * rs + (long long)k * ks] : 0.0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kSliceTile * kSliceK; i += 256) {
+    const int mi = i / kSliceK, ki = i % kSliceK;
+    const int m = m0 + mi;
+    double r = (m < M) ? ldexp(xs[mi][ki], -e[m]) : 0.0;
+#pragma unroll
+    for (int t = 0; t < S; ++t) {
+      r *= 128.0;
+      const double q = rint(r);
+      r -= q;
+      qs[t][mi][ki] = (int8_t)q;
+    }
+  }
+  __syncthreads();
+  // 16-byte stores: S planes x 64 rows x 2 chunks
+  for (int i = threadIdx.x; i < S * kSliceTile * 2; i += 256) {
+    const int t = i / (kSliceTile * 2), rem = i % (kSliceTile * 2);
+    const int mi = rem / 2, c = rem % 2;
+    const int m = m0 + mi;
+    if (m < mp && k0 + c * 16 < kp)
+      *reinterpret_cast<int4*>(P + t * plane + (long long)m * ldk + k0 + c * 16) =
+          *reinterpret_cast<const int4*>(&qs[t][mi][c * 16]);
+  }
+}
+
+__global__ void k_identity(double* __restrict__ X, int n) {
+  const long long total = (long long)n * n;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x)
+    X[e] = (e % n) == (e / n) ? 1.0 : 0.0;
+}
+
+inline int round_up(long long x, int a) { return (int)((x + a - 1) / a * a); }
+
+struct MixedBuffers {
+  int8_t *PA, *PB;
+  int *ea, *eb, *err;
+  double* MT;  // L^{-T}, column-major rk x rk
+  long long pa_plane, pb_plane;
+  int ldk;
+};
+
+MixedBuffers carve_mixed(Arena& a, long long ng, int nstate, int rk, int slices) {
+  MixedBuffers b;
+  const int kmax = round_up(nstate > rk ? nstate : rk, ozaki::BKB);
+  const long long mp = round_up(ng, ozaki::BM);
+  const int np = round_up(rk, 128);
+  b.ldk = kmax;
+  b.pa_plane = mp * kmax;
+  b.pb_plane = (long long)np * kmax;
+  b.PA = a.take<int8_t>((size_t)slices * b.pa_plane);
+  b.PB = a.take<int8_t>((size_t)slices * b.pb_plane);
+  b.ea = a.take<int>((size_t)mp);
+  b.eb = a.take<int>((size_t)np);
+  b.err = a.take<int>(1);
+  b.MT = a.take<double>((size_t)rk * rk);
+  return b;
+}
+
+template <int S>
+int slice_operand(const double* X, long long rs, long long ks, int M, int K, int mp, int kp,
+                  int* e, int8_t* P, long long plane, int ldk, cudaStream_t s) {
+  k_row_exponent<<<grid_for(M, 256), 256, 0, s>>>(X, rs, ks, M, K, e);
+  dim3 g((unsigned)(kp / kSliceK), (unsigned)((mp + kSliceTile - 1) / kSliceTile));
+  k_slice<S><<<g, 256, 0, s>>>(X, rs, ks, M, K, mp, kp, e, P, plane, ldk);
+  ISDF_CHECK_LAUNCH();
+  return ISDF_OK;
+}
+
+template <int S, int EPI, int KMODE>
+int ozaki_gemm(const MixedBuffers& b, int M, int N, int kp, double* C, long long ldc,
+               cudaStream_t s) {
+  auto kern = ozaki::k_ozaki_gemm<S, EPI, KMODE>;
+  static bool attr[64] = {};
+  int dev = 0;
+  ISDF_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && !attr[dev]) {
+    ISDF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   ozaki::Cfg<S>::SMEM));
+    attr[dev] = true;
+  }
+  dim3 g((unsigned)((N + ozaki::BN - 1) / ozaki::BN), (unsigned)((M + ozaki::BM - 1) / ozaki::BM));
+  kern<<<g, 128, ozaki::Cfg<S>::SMEM, s>>>(b.PA, b.pa_plane, b.ldk, b.PB, b.pb_plane, b.ldk,
+                                           b.ea, b.eb, M, N, kp, C, ldc, b.err);
+  ISDF_CHECK_LAUNCH();
+  return ISDF_OK;
+}
+
+template <int S>
+int fit_mixed_s(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res) {
+  const long long ng = args.ng;
+  const int rk = args.rk;
+  FitBuffers b = carve(arena, args.nstate, rk);
+  MixedBuffers mb = carve_mixed(arena, ng, args.nstate, rk, S);
+  if (arena.overflowed()) return record_error(ISDF_ERR_NOMEM, "mixed fit: workspace too small");
+  StageEvents ev;
+  ISDF_TRY(ev.create());
+  const int mp = round_up(ng, ozaki::BM);
+  const int np = round_up(rk, 128);
+  ISDF_CUDA(cudaMemcpyAsync(b.piv, args.piv, sizeof(int) * rk, cudaMemcpyHostToDevice, s));
+  ISDF_CUDA(cudaMemsetAsync(b.info, 0, sizeof(int), s));
+  ISDF_CUDA(cudaMemsetAsync(mb.err, 0, sizeof(int), s));
+  k_gather_psimu<<<grid_for((long long)args.nstate * rk, 256), 256, 0, s>>>(
+      args.d_psi, ng, args.nstate, b.piv, rk, b.Bm);
+  ISDF_CUDA(cudaEventRecord(ev.e[0], s));
+
+  // Z C^T = (psi_S1 psi_S1(mu)^T) o (psi_S2 psi_S2(mu)^T)
+  const bool same = (args.nv1 == args.nv2 && args.nc1 == args.nc2);
+  for (int f = 0; f < (same ? 1 : 2); ++f) {
+    const int lo = f == 0 ? args.nocc - args.nv1 : args.nocc - args.nv2;
+    const int K = f == 0 ? args.nv1 + args.nc1 : args.nv2 + args.nc2;
+    const int kp = round_up(K, ozaki::BKB);
+    ISDF_TRY(slice_operand<S>(args.d_psi + (long long)lo * ng, 1, ng, (int)ng, K, mp, kp, mb.ea,
+                              mb.PA, mb.pa_plane, mb.ldk, s));
+    ISDF_TRY(slice_operand<S>(b.Bm + (size_t)lo * rk, 1, rk, rk, K, np, kp, mb.eb, mb.PB,
+                              mb.pb_plane, mb.ldk, s));
+    if (same) ISDF_TRY((ozaki_gemm<S, 1, 0>(mb, (int)ng, rk, kp, args.d_theta, ng, s)));
+    else if (f == 0) ISDF_TRY((ozaki_gemm<S, 0, 0>(mb, (int)ng, rk, kp, args.d_theta, ng, s)));
+    else ISDF_TRY((ozaki_gemm<S, 2, 0>(mb, (int)ng, rk, kp, args.d_theta, ng, s)));
+  }
+  ISDF_CUDA(cudaEventRecord(ev.e[1], s));
+
+  // C C^T + eps I, Cholesky, L^{-T} (FP64)
+  k_gather_cct<<<grid_for((long long)rk * rk, 256), 256, 0, s>>>(args.d_theta, ng, b.piv, rk, b.P);
+  k_regularise<<<1, 256, 0, s>>>(b.P, rk, b.eps);
+  ISDF_TRY(cholesky(b, rk, s));
+  int info = 0;
+  ISDF_CUDA(cudaMemcpyAsync(&info, b.info, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ISDF_CUDA(cudaStreamSynchronize(s));
+  res->chol_info = info;
+  if (info != 0) return record_error(ISDF_ERR_NOT_SPD, "fit: C C^T + eps I is not positive definite");
+  // L^{-T}: the forward sweep X L^T = I on an rk x rk identity
+  k_identity<<<grid_for((long long)rk * rk, 256), 256, 0, s>>>(mb.MT, rk);
+  {
+    const int nblk = (rk + kNB - 1) / kNB;
+    const bool v2 = vec2_ok(mb.MT, rk, b.W, kNB);
+    const unsigned tg = (unsigned)((rk + CoreN::BM - 1) / CoreN::BM);
+    for (int kb = 0; kb < nblk; ++kb) {
+      const int c0 = kb * kNB, bs = min(kNB, rk - c0);
+      k_build_w<true><<<(c0 + bs + 3) / 4 < 1024 ? (c0 + bs + 3) / 4 : 1024, 256, 0, s>>>(
+          b.P, rk, c0, bs, b.dinvT + (size_t)kb * kNB * kNB, b.W);
+      if (v2) k_trsm_gemm<2><<<tg, 256, CoreN::SMEM_BYTES, s>>>(mb.MT, rk, c0, bs, 0, c0 + bs, b.W);
+      else k_trsm_gemm<1><<<tg, 256, CoreN::SMEM_BYTES, s>>>(mb.MT, rk, c0, bs, 0, c0 + bs, b.W);
+    }
+  }
+  ISDF_CUDA(cudaEventRecord(ev.e[2], s));
+
+  // Y = Z L^{-T} (L^{-T} upper), then theta = Y L^{-1} (L^{-1} lower), in place in theta
+  const int kp = round_up(rk, ozaki::BKB);
+  ISDF_TRY(slice_operand<S>(args.d_theta, 1, ng, (int)ng, rk, mp, kp, mb.ea, mb.PA, mb.pa_plane,
+                            mb.ldk, s));
+  ISDF_TRY(slice_operand<S>(mb.MT, rk, 1, rk, rk, np, kp, mb.eb, mb.PB, mb.pb_plane, mb.ldk, s));
+  ISDF_TRY((ozaki_gemm<S, 0, 1>(mb, (int)ng, rk, kp, args.d_theta, ng, s)));
+  ISDF_TRY(slice_operand<S>(args.d_theta, 1, ng, (int)ng, rk, mp, kp, mb.ea, mb.PA, mb.pa_plane,
+                            mb.ldk, s));
+  ISDF_TRY(slice_operand<S>(mb.MT, 1, rk, rk, rk, np, kp, mb.eb, mb.PB, mb.pb_plane, mb.ldk, s));
+  ISDF_TRY((ozaki_gemm<S, 0, 2>(mb, (int)ng, rk, kp, args.d_theta, ng, s)));
+  ISDF_CUDA(cudaEventRecord(ev.e[3], s));
+  int err = 0;
+  ISDF_CUDA(cudaMemcpyAsync(&err, mb.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ISDF_CUDA(cudaEventSynchronize(ev.e[3]));
+  ISDF_CUDA(cudaStreamSynchronize(s));
+  if (err) return record_error(ISDF_ERR_TIMEOUT, "mixed fit: a tensor-core pipeline wait timed out");
+  ISDF_CUDA(cudaEventElapsedTime(&res->t_zct_ms, ev.e[0], ev.e[1]));
+  ISDF_CUDA(cudaEventElapsedTime(&res->t_chol_ms, ev.e[1], ev.e[2]));
+  ISDF_CUDA(cudaEventElapsedTime(&res->t_solve_ms, ev.e[2], ev.e[3]));
+  const int nblk = (rk + kNB - 1) / kNB;
+  res->launches = 1 + (same ? 3 : 6) * 2 + 2 + (nblk + 2 * (nblk - 1) + 1) + 1 + 2 * nblk + 10;
+  return ISDF_OK;
+}
+
+}  // namespace
+
+size_t fit_mixed_workspace_bytes(long long ng, int nstate, int rk, int slices) {
+  Arena a;
+  a.counting = true;
+  carve(a, nstate, rk);
+  carve_mixed(a, ng, nstate, rk, slices);
+  return a.off;
+}
+
+int fit_mixed(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, int slices) {
+  if (args.ng <= 0 || args.rk <= 0 || args.nstate <= 0)
+    return record_error(ISDF_ERR_ARG, "fit: bad sizes");
+  if (args.ng > 0x7fffffffLL - 128) return record_error(ISDF_ERR_UNSUPPORTED, "mixed fit: Ng");
+  ISDF_TRY(set_smem_attrs());
+  switch (slices) {
+    case 5: return fit_mixed_s<5>(args, arena, s, res);
+    case 6: return fit_mixed_s<6>(args, arena, s, res);
+    case 7: return fit_mixed_s<7>(args, arena, s, res);
+    default: return record_error(ISDF_ERR_ARG, "mixed fit: slices must be 5, 6 or 7");
+  }
 }
 
 }  // namespace isdf_b200

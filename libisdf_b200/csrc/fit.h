@@ -25,6 +25,11 @@ struct FitResult {
 
 size_t fit_workspace_bytes(long long ng, int nstate, int rk);
 
+// Mixed-precision fit: the large products as INT8-sliced (`slices` = 5..7)
+// GEMMs on the tcgen05 tensor cores, FP64 Cholesky and triangular inverse.
+size_t fit_mixed_workspace_bytes(long long ng, int nstate, int rk, int slices);
+int fit_mixed(const FitArgs& args, Arena& arena, cudaStream_t stream, FitResult* res, int slices);
+
 // C = A * B on the FP64 tensor cores: A column-major (lda), B depth-major
 // (B(k, n) = B[k*ldb + n]), C column-major (ldc).
 int dgemm_store(int M, int N, int K, const double* A, long long lda, const double* B,

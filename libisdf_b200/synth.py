@@ -104,19 +104,19 @@ def raw_orbitals(n: int, cells: int, nstate: int, seed: int, device: str = "cpu"
     alphas = rng.uniform(0.3, 1.5, size=(nsite, per_site))
     coef = rng.standard_normal(size=(nsite * per_site, nstate))
     r = torch.from_numpy(grid_coords(n, length)).to(device)
-    phi = torch.empty((r.shape[0], nsite * per_site), dtype=torch.float64, device=device)
     al = torch.from_numpy(alphas).to(device)
+    cf = torch.from_numpy(coef).to(device)
+    kind = torch.arange(per_site, device=device) % 4
+    psi = torch.zeros((r.shape[0], nstate), dtype=torch.float64, device=device)
     for s in range(nsite):
         d = r - torch.from_numpy(sites[s]).to(device)
         d -= length * torch.round(d / length)  # minimum image
         d2 = (d * d).sum(dim=1, keepdim=True)
         g = torch.exp(-d2 * al[s].view(1, -1))  # (ng, per_site)
-        kind = torch.arange(per_site, device=device) % 4
-        poly = torch.ones_like(g)
         for k in (1, 2, 3):
-            poly[:, kind == k] = d[:, k - 1:k]
-        phi[:, s * per_site:(s + 1) * per_site] = g * poly
-    return phi @ torch.from_numpy(coef).to(device)
+            g[:, kind == k] *= d[:, k - 1:k]
+        psi.addmm_(g, cf[s * per_site:(s + 1) * per_site])
+    return psi
 
 
 def orbitals(n: int, cells: int, nstate: int, seed: int, device: str = "cpu") -> np.ndarray:
