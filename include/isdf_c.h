@@ -64,7 +64,7 @@ typedef struct isdf_options_t {
   long long rand_seed;    /* >= 0: srand() before K-means (only its npt < mu branch
                              draws from rand()); < 0: keep the process state */
   void* stream;           /* cudaStream_t to run on; NULL = library stream */
-  int mixed_slices;       /* mixed precision: INT8 slices per FP64 operand, 5..7 (default 6) */
+  int mixed_slices;       /* mixed precision: INT8 slices per FP64 operand, 5..7 (default 7) */
   int reserved[7];
 } isdf_options_t;
 

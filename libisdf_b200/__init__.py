@@ -104,7 +104,7 @@ class Options:
     qrcp_seed: int = 41
     rand_seed: int = -1
     stream: int = 0
-    mixed_slices: int = 6
+    mixed_slices: int = 7
 
     def _c(self) -> _Options:
         o = _Options()

@@ -304,7 +304,7 @@ void isdf_default_options(isdf_options_t* opt) {
   opt->qrcp_seed = 41;
   opt->rand_seed = -1;
   opt->stream = nullptr;
-  opt->mixed_slices = 6;
+  opt->mixed_slices = 7;
 }
 
 int isdf_solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, int nv1,
@@ -395,7 +395,7 @@ int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, i
     fa.d_theta = d_theta;
     FitResult fr;
     cudaStream_t s = stream ? (cudaStream_t)stream : ls;
-    int rc = precision == ISDF_PRECISION_MIXED ? fit_mixed(fa, arena, s, &fr, 6)
+    int rc = precision == ISDF_PRECISION_MIXED ? fit_mixed(fa, arena, s, &fr, 7)
                                                : fit_fp64(fa, arena, s, &fr);
     if (chol_info) *chol_info = fr.chol_info;
     if (rc == ISDF_OK) ISDF_CUDA(cudaStreamSynchronize(s));

@@ -631,8 +631,24 @@ int fit_mixed_s(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* re
   }
   ISDF_CUDA(cudaEventRecord(ev.e[1], s));
 
-  // C C^T + eps I, Cholesky, L^{-T} (FP64)
-  k_gather_cct<<<grid_for((long long)rk * rk, 256), 256, 0, s>>>(args.d_theta, ng, b.piv, rk, b.P);
+  // C C^T + eps I, Cholesky, L^{-T} (FP64). C C^T is formed here from psi(mu)
+  // on the FP64 tensor cores rather than gathered from the sliced Z C^T: the
+  // factorisation amplifies the error of C C^T by cond(C C^T) (~1e10), so it
+  // must carry FP64 rounding, as in the reference.
+  {
+    const int lo1 = args.nocc - args.nv1, K1 = args.nv1 + args.nc1;
+    const int lo2 = args.nocc - args.nv2, K2 = args.nv2 + args.nc2;
+    const double* B1 = b.Bm + (size_t)lo1 * rk;
+    const double* B2 = b.Bm + (size_t)lo2 * rk;
+    dim3 cg((unsigned)((rk + CoreZ::BN - 1) / CoreZ::BN), (unsigned)((rk + CoreZ::BM - 1) / CoreZ::BM));
+    const size_t zs = CoreZ::SMEM_BYTES;
+    if (same) {
+      k_gemm_z<0, 1><<<cg, 256, zs, s>>>(rk, rk, K1, B1, rk, B1, rk, b.P, rk);
+    } else {
+      k_gemm_z<1, 1><<<cg, 256, zs, s>>>(rk, rk, K1, B1, rk, B1, rk, b.P, rk);
+      k_gemm_z<2, 1><<<cg, 256, zs, s>>>(rk, rk, K2, B2, rk, B2, rk, b.P, rk);
+    }
+  }
   k_regularise<<<1, 256, 0, s>>>(b.P, rk, b.eps);
   ISDF_TRY(cholesky(b, rk, s));
   int info = 0;
