@@ -17,6 +17,7 @@
 //   label[p]  nearest centroid.
 // Centroids: double4 (x, y, z, 0) in cen[], rk on the device in st->rk.
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -32,6 +33,8 @@ namespace {
 constexpr int kTile = 4096;      // points per counting-sort tile
 constexpr int kFinalChunk = 4096;  // points per partial argmin chunk
 constexpr int kIterChunk = 8;    // Lloyd iterations launched between host checks
+constexpr int kMaxCellsPerDim = 20;  // centroid cell grid of the pruned assignment
+constexpr int kMaxCells = kMaxCellsPerDim * kMaxCellsPerDim * kMaxCellsPerDim;
 
 struct KmState {
   int s;        // Lloyd iterations completed
@@ -191,57 +194,125 @@ __global__ void k_points(const int* __restrict__ pidx, const double* __restrict_
 // ---------------------------------------------------------------- assign
 // d = ((dx*dx + dy*dy) + dz*dz) with dx = point - centroid (pdist2,
 // utility.cpp:598-615); label = first centroid reaching the minimum
-// (findMin Dim=1, utility.cpp:579-595). Centroids are staged in shared memory
-// in chunks; each thread owns kPPT points.
+// (findMin Dim=1, utility.cpp:579-595).
 constexpr int kAssignThreads = 256;
-constexpr int kPPT = 2;
-constexpr int kCenChunk = 1024;
 
-__global__ void __launch_bounds__(kAssignThreads) k_assign(
+// ---------------------------------------------------------------- pruned assign
+// Exact spatial pruning: centroids are binned into a uniform nc^3 cell grid
+// over the box; a point visits cells in Chebyshev rings around its own cell
+// and skips a cell only when the squared distance from the point to the
+// cell's box, shrunk by a relative 2e-14 safety factor (well above the
+// rounding of both the box bound and the distance formula), is strictly
+// greater than the best distance found. Every skipped centroid would have
+// computed a strictly larger distance, so the result - the first centroid in
+// index order reaching the minimum computed distance, compared as (d, index)
+// pairs - is the brute-force result bit for bit.
+struct CellGrid {
+  int nc;
+  double h[3];
+  double tol;
+};
+
+// One block: cell of each centroid, counting sort into cell order.
+__global__ void __launch_bounds__(1024) k_build_cells(const double4* __restrict__ cen,
+                                                      const KmState* st, CellGrid g,
+                                                      int* __restrict__ cell_start,
+                                                      double4* __restrict__ cell_cen,
+                                                      int* __restrict__ cell_of) {
+  if (st->done) return;
+  extern __shared__ int sc[];  // ncells + 1 counters
+  const int rk = st->rk;
+  const int ncells = g.nc * g.nc * g.nc;
+  for (int c = threadIdx.x; c <= ncells; c += blockDim.x) sc[c] = 0;
+  __syncthreads();
+  for (int j = threadIdx.x; j < rk; j += blockDim.x) {
+    const double4 c = cen[j];
+    const int ci = min(g.nc - 1, max(0, (int)floor(c.x / g.h[0])));
+    const int cj = min(g.nc - 1, max(0, (int)floor(c.y / g.h[1])));
+    const int ck = min(g.nc - 1, max(0, (int)floor(c.z / g.h[2])));
+    const int id = ci + g.nc * (cj + g.nc * ck);
+    cell_of[j] = id;
+    atomicAdd(&sc[id + 1], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int c = 1; c <= ncells; ++c) sc[c] += sc[c - 1];
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c <= ncells; c += blockDim.x) cell_start[c] = sc[c];
+  __syncthreads();
+  // placement inside a cell is arbitrary: the search compares (d, index) pairs
+  for (int j = threadIdx.x; j < rk; j += blockDim.x) {
+    const int slot = atomicAdd(&sc[cell_of[j]], 1);
+    const double4 c = cen[j];
+    cell_cen[slot] = make_double4(c.x, c.y, c.z, (double)j);
+  }
+}
+
+__global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
     const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
-    int n, const double4* __restrict__ cen, KmState* st, int* __restrict__ label, int count) {
+    int n, const double4* __restrict__ cen, const int* __restrict__ cell_start,
+    const double4* __restrict__ cell_cen, CellGrid g, KmState* st, int* __restrict__ label,
+    int count) {
   if (st->done) return;
   const int rk = st->rk;
-  __shared__ double4 sc[kCenChunk];
-  double x[kPPT], y[kPPT], z[kPPT], best[kPPT];
-  int bj[kPPT];
-  const int p0 = blockIdx.x * kAssignThreads * kPPT + threadIdx.x;
-#pragma unroll
-  for (int k = 0; k < kPPT; ++k) {
-    int p = p0 + k * kAssignThreads;
-    bool ok = p < n;
-    x[k] = ok ? px[p] : 0.0;
-    y[k] = ok ? py[p] : 0.0;
-    z[k] = ok ? pz[p] : 0.0;
-    best[k] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
-    bj[k] = 0;
-  }
-  for (int c0 = 0; c0 < rk; c0 += kCenChunk) {
-    const int m = min(kCenChunk, rk - c0);
-    __syncthreads();
-    for (int j = threadIdx.x; j < m; j += kAssignThreads) sc[j] = cen[c0 + j];
-    __syncthreads();
-    for (int j = 0; j < m; ++j) {
-      const double4 c = sc[j];
-#pragma unroll
-      for (int k = 0; k < kPPT; ++k) {
-        double d1 = rsub(x[k], c.x), d2 = rsub(y[k], c.y), d3 = rsub(z[k], c.z);
-        double d = radd(radd(rmul(d1, d1), rmul(d2, d2)), rmul(d3, d3));
-        if (d < best[k]) {
-          best[k] = d;
-          bj[k] = c0 + j;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  int changed = 0;
+  if (p < n) {
+    const double x = px[p], y = py[p], z = pz[p];
+    double best = __longlong_as_double(0x7ff0000000000000LL);
+    int bj = 0x7fffffff;
+    const int old = count ? label[p] : -1;
+    if (old >= 0 && old < rk) {  // seed with the previous centroid (any centroid is a valid start)
+      const double4 c = cen[old];
+      double d1 = rsub(x, c.x), d2 = rsub(y, c.y), d3 = rsub(z, c.z);
+      best = radd(radd(rmul(d1, d1), rmul(d2, d2)), rmul(d3, d3));
+      bj = old;
+    }
+    const int pi = min(g.nc - 1, max(0, (int)floor(x / g.h[0])));
+    const int pj = min(g.nc - 1, max(0, (int)floor(y / g.h[1])));
+    const int pk = min(g.nc - 1, max(0, (int)floor(z / g.h[2])));
+    const double hmin = fmin(g.h[0], fmin(g.h[1], g.h[2]));
+    const double shrink = 1.0 - 2e-14;
+    for (int r = 0; r <= g.nc; ++r) {
+      if (r >= 2) {
+        const double lb = (r - 1) * hmin - g.tol;
+        if (lb > 0.0 && lb * lb * shrink > best) break;
+      }
+      for (int dk = -r; dk <= r; ++dk) {
+        const int ck = pk + dk;
+        if (ck < 0 || ck >= g.nc) continue;
+        for (int dj = -r; dj <= r; ++dj) {
+          const int cj = pj + dj;
+          if (cj < 0 || cj >= g.nc) continue;
+          for (int di = -r; di <= r; ++di) {
+            if (max(abs(di), max(abs(dj), abs(dk))) != r) continue;
+            const int ci = pi + di;
+            if (ci < 0 || ci >= g.nc) continue;
+            // box lower bound (box widened by tol)
+            const double bx = fmax(0.0, fmax(ci * g.h[0] - g.tol - x, x - (ci + 1) * g.h[0] - g.tol));
+            const double by = fmax(0.0, fmax(cj * g.h[1] - g.tol - y, y - (cj + 1) * g.h[1] - g.tol));
+            const double bz = fmax(0.0, fmax(ck * g.h[2] - g.tol - z, z - (ck + 1) * g.h[2] - g.tol));
+            const double lb = bx * bx + by * by + bz * bz;
+            if (lb * shrink > best) continue;
+            const int id = ci + g.nc * (cj + g.nc * ck);
+            const int e = cell_start[id + 1];
+            for (int q = cell_start[id]; q < e; ++q) {
+              const double4 c = cell_cen[q];
+              double d1 = rsub(x, c.x), d2 = rsub(y, c.y), d3 = rsub(z, c.z);
+              double d = radd(radd(rmul(d1, d1), rmul(d2, d2)), rmul(d3, d3));
+              const int j = (int)c.w;
+              if (d < best || (d == best && j < bj)) {
+                best = d;
+                bj = j;
+              }
+            }
+          }
         }
       }
     }
-  }
-  int changed = 0;
-#pragma unroll
-  for (int k = 0; k < kPPT; ++k) {
-    int p = p0 + k * kAssignThreads;
-    if (p < n) {
-      if (count && label[p] != bj[k]) ++changed;
-      label[p] = bj[k];
-    }
+    if (count && old != bj) ++changed;
+    label[p] = bj;
   }
   if (count) {
     for (int o = 16; o > 0; o >>= 1) changed += __shfl_xor_sync(0xffffffffu, changed, o);
@@ -589,6 +660,9 @@ struct KmBuffers {
   int* part_i;
   int* sel;
   KmState* st;
+  int* cell_start;
+  double4* cell_cen;
+  int* cell_of;
 };
 
 KmBuffers carve(Arena& a, int n, int mu) {
@@ -613,6 +687,9 @@ KmBuffers carve(Arena& a, int n, int mu) {
   b.part_i = a.take<int>((size_t)nchunks * mu);
   b.sel = a.take<int>(mu);
   b.st = a.take<KmState>(1);
+  b.cell_start = a.take<int>((size_t)kMaxCells + 1);
+  b.cell_cen = a.take<double4>(mu);
+  b.cell_of = a.take<int>(mu);
   return b;
 }
 
@@ -710,8 +787,24 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     init.maxw_bits = hst.maxw_bits;
     ISDF_CUDA(cudaMemcpyAsync(b.st, &init, sizeof(KmState), cudaMemcpyHostToDevice, stream));
   }
-  const unsigned agrid = grid_for(n, kAssignThreads, kPPT);
-  k_assign<<<agrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.st, b.label, 0);
+  CellGrid cg;
+  {
+    int nc = (int)std::lround(std::cbrt(mu / 1.5));
+    nc = std::max(1, std::min(nc, kMaxCellsPerDim));
+    cg.nc = nc;
+    double lmax = 0.0;
+    for (int i = 0; i < 3; ++i) {
+      cg.h[i] = args.length[i] / nc;
+      lmax = std::max(lmax, std::fabs(args.length[i]));
+    }
+    cg.tol = 1e-9 * lmax;
+  }
+  const size_t cell_smem = sizeof(int) * ((size_t)cg.nc * cg.nc * cg.nc + 1);
+  const unsigned pgrid = grid_for(n, kAssignThreads);
+  k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
+                                                b.cell_of);
+  k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.cell_start,
+                                                      b.cell_cen, cg, b.st, b.label, 0);
   ISDF_CHECK_LAUNCH();
 
   const double max_f = 1e-5 * n;  // KmeansTolerance * n (utility.cpp:812)
@@ -731,8 +824,11 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
       k_segsum<<<grid_for(mu, 8), 256, 0, stream>>>(b.sorted, b.start, b.members, b.px, b.py,
                                                     b.pz, b.pw, b.label, n, b.st, b.sums);
       k_centroids<<<1, 1024, 0, stream>>>(b.sums, b.st, b.cen);
-      k_assign<<<agrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.st, b.label,
-                                                     1);
+      k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
+                                                    b.cell_of);
+      k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen,
+                                                          b.cell_start, b.cell_cen, cg, b.st,
+                                                          b.label, 1);
       k_iter_end<<<1, 1, 0, stream>>>(b.st);
     }
     ISDF_CHECK_LAUNCH();
@@ -742,7 +838,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     if (++chunks > max_chunks) return record_error(ISDF_ERR_CUDA, "kmeans: loop did not stop");
   }
   res->iters = hst.s;
-  res->launches = 4 + 2 + (chunks + 1) * kIterChunk * 9 + 2;
+  res->launches = 4 + 3 + (chunks + 1) * kIterChunk * 10 + 2;
   const int rk = hst.rk;
 
   dim3 fgrid((unsigned)((rk + 127) / 128), (unsigned)nchunks);

@@ -95,3 +95,21 @@ def test_select_heavy_zero_tail(torch_cuda, seed):
     assert npt < n / 2 + n / 10
     assert (rk, it) == (rk_o, it_o)
     assert np.array_equal(piv, piv_o)
+
+
+@pytest.mark.parametrize("mu,seed", [(500, 3), (1, 4), (2000, 5)])
+def test_select_random_weights(torch_cuda, mu, seed):
+    """Random weights on an anisotropic grid: many centroids per cell ring,
+    equal-distance ties between lattice points, the pruned search against
+    the brute-force restatement."""
+    torch = torch_cuda
+    rng = np.random.default_rng(seed)
+    ng = (30, 25, 20)
+    n = int(np.prod(ng))
+    w = rng.uniform(0.0, 1.0, size=n) ** 4
+    length = (12.0, 7.5, 9.0)
+    piv_o, rk_o, it_o = port.kmeans(w, ng, length, mu, 40)
+    piv, rk, it, npt = isdf.kmeans_select(isdf.Domain(length=length, num_grid=ng),
+                                          torch.from_numpy(w).cuda(), mu, 40)
+    assert (rk, it) == (rk_o, it_o)
+    assert np.array_equal(piv, piv_o)
