@@ -157,6 +157,59 @@ int isdf_fit_noalloc(const double* d_psi, long long ng, int nstate, int nocc, in
                      int nv2, int nc2, int rk, const int* piv, double* d_theta, int* chol_info,
                      void* stream);
 
+/* ---------------------------------------------------------------- serving
+ * No counterpart in the reference (one system per ISDF() call). A
+ * continuous-batching server: requests for systems of any size arrive at any
+ * time; `slots` solves run concurrently on their own streams (their kernels
+ * overlap on the GPU); a request starts when its device workspace fits in
+ * what the budget has left (small requests may pass a large head until it
+ * has been passed `max_skips` times); psi / theta / piv stay the caller's
+ * buffers (device, device, host) and must stay valid until the request is
+ * done. Results are the same as isdf_solve() on the same request. */
+typedef struct isdf_server_config_t {
+  int device;              /* CUDA device of the server (default 0) */
+  int slots;               /* concurrent solves (default 4) */
+  size_t hbm_budget_bytes; /* workspace budget; 0 = half of the free memory at creation */
+  int max_queue;           /* pending requests before submit returns ISDF_ERR_BUSY (4096) */
+  int max_skips;           /* times a waiting head may be passed by smaller requests (64) */
+  int reserved[4];
+} isdf_server_config_t;
+
+typedef struct isdf_request_t {
+  isdf_domain_t dom;
+  const double* d_psi;
+  int nocc, nstate, nv1, nc1, nv2, nc2, mu_points;
+  double* d_theta;
+  int* piv;
+  int kmeans_max_iter;
+  int selector;
+  int check;
+  isdf_options_t opt; /* opt.stream is ignored: each slot has its own stream */
+} isdf_request_t;
+
+typedef struct isdf_server_stats_t {
+  long long submitted, completed, failed, cancelled;
+  double p50_ms, p99_ms, mean_ms; /* submit-to-completion latency of completed requests */
+  double solves_per_s;            /* completed / (last completion - first submit) */
+  int peak_concurrency, queued, running, reserved0;
+  size_t peak_bytes; /* largest workspace total in use at once */
+} isdf_server_stats_t;
+
+void isdf_server_default_config(isdf_server_config_t* cfg);
+int isdf_server_create(const isdf_server_config_t* cfg, void** server);
+/* Queues a request; *ticket identifies it. ISDF_ERR_BUSY when the queue is full. */
+int isdf_server_submit(void* server, const isdf_request_t* req, long long* ticket);
+/* *state: 0 queued, 1 running, 2 done; *status: the solve's return code once done. */
+int isdf_server_poll(void* server, long long ticket, int* state, int* status, isdf_report_t* rep);
+/* Blocks until done (timeout_ms < 0: no limit; else ISDF_ERR_TIMEOUT when it runs out). */
+int isdf_server_wait(void* server, long long ticket, double timeout_ms, int* status,
+                     isdf_report_t* rep);
+/* Removes a request that has not started (its status becomes ISDF_ERR_CANCELLED). */
+int isdf_server_cancel(void* server, long long ticket);
+int isdf_server_stats(void* server, isdf_server_stats_t* stats);
+/* Cancels queued requests, waits for running ones, frees the server. */
+int isdf_server_destroy(void* server);
+
 /* Message for the last error on this thread ("" if none). */
 const char* isdf_last_error(void);
 const char* isdf_status_string(int code);

@@ -74,6 +74,31 @@ class _Report(ctypes.Structure):
                 ("kernel_launches", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
 
 
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int),
+                ("hbm_budget_bytes", ctypes.c_size_t), ("max_queue", ctypes.c_int),
+                ("max_skips", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
+
+
+class _Request(ctypes.Structure):
+    _fields_ = [("dom", _Domain), ("d_psi", ctypes.c_void_p), ("nocc", ctypes.c_int),
+                ("nstate", ctypes.c_int), ("nv1", ctypes.c_int), ("nc1", ctypes.c_int),
+                ("nv2", ctypes.c_int), ("nc2", ctypes.c_int), ("mu_points", ctypes.c_int),
+                ("d_theta", ctypes.c_void_p), ("piv", ctypes.c_void_p),
+                ("kmeans_max_iter", ctypes.c_int), ("selector", ctypes.c_int),
+                ("check", ctypes.c_int), ("opt", _Options)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+                ("failed", ctypes.c_longlong), ("cancelled", ctypes.c_longlong),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("solves_per_s", ctypes.c_double),
+                ("peak_concurrency", ctypes.c_int), ("queued", ctypes.c_int),
+                ("running", ctypes.c_int), ("reserved0", ctypes.c_int),
+                ("peak_bytes", ctypes.c_size_t)]
+
+
 @dataclass
 class Domain:
     """Numeric fields of the reference's Domain (include/common/domain.hpp:8-36)."""
@@ -261,6 +286,95 @@ def check(domain: Domain, d_psi, nocc: int, nstate: int, nv1: int, nc1: int, nv2
                             piv.ctypes.data, _dptr(d_theta), ctypes.addressof(fe),
                             ctypes.addressof(ce), stream or None))
     return fe.value, ce.value
+
+
+def _report(r: _Report) -> Report:
+    return Report(r.rk_requested, r.rk_eff, r.kmeans_iters, r.npt, r.fit_err, r.coul_err,
+                  r.t_select_ms, r.t_fit_ms, r.t_zct_ms, r.t_chol_ms, r.t_solve_ms, r.t_check_ms,
+                  r.t_total_ms, r.chol_info, r.kernel_launches)
+
+
+class Server:
+    """Continuous-batching ISDF server (isdf_server_* C ABI). Requests keep
+    references to the caller's buffers (psi, theta on the device, piv on the
+    host) until they are done."""
+
+    def __init__(self, slots: int = 4, hbm_budget_bytes: int = 0, device: int = 0,
+                 max_skips: int = 64, max_queue: int = 4096):
+        L = lib()
+        P, I, LL = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong
+        L.isdf_server_create.argtypes = [ctypes.POINTER(_ServerConfig), ctypes.POINTER(P)]
+        L.isdf_server_submit.argtypes = [P, ctypes.POINTER(_Request), ctypes.POINTER(LL)]
+        L.isdf_server_wait.argtypes = [P, LL, ctypes.c_double, ctypes.POINTER(I),
+                                       ctypes.POINTER(_Report)]
+        L.isdf_server_poll.argtypes = [P, LL, ctypes.POINTER(I), ctypes.POINTER(I),
+                                       ctypes.POINTER(_Report)]
+        L.isdf_server_cancel.argtypes = [P, LL]
+        L.isdf_server_stats.argtypes = [P, ctypes.POINTER(_ServerStats)]
+        L.isdf_server_destroy.argtypes = [P]
+        cfg = _ServerConfig()
+        cfg.device, cfg.slots, cfg.hbm_budget_bytes = device, slots, hbm_budget_bytes
+        cfg.max_queue, cfg.max_skips = max_queue, max_skips
+        self._h = ctypes.c_void_p()
+        _check(L.isdf_server_create(ctypes.byref(cfg), ctypes.byref(self._h)))
+        self._keep = {}
+
+    def submit(self, d_psirow, domain: Domain, nocc, nstate, nv1, nc1, nv2, nc2, mu_points,
+               d_thetaCol, piv: np.ndarray, KmeansMaxIter_ISDF: int, s1: str = "Kmeans",
+               check: bool = False, options: Options | None = None) -> int:
+        n = domain.NumGridTotal()
+        piv = _host_int32(piv, n)
+        r = _Request()
+        r.dom = domain._c()
+        r.d_psi = _dptr(d_psirow)
+        r.nocc, r.nstate, r.nv1, r.nc1, r.nv2, r.nc2 = nocc, nstate, nv1, nc1, nv2, nc2
+        r.mu_points = mu_points
+        r.d_theta = _dptr(d_thetaCol)
+        r.piv = piv.ctypes.data
+        r.kmeans_max_iter = KmeansMaxIter_ISDF
+        r.selector = {"Kmeans": SELECT_KMEANS, "QRCP": SELECT_QRCP}[s1]
+        r.check = int(bool(check))
+        r.opt = (options or Options())._c()
+        t = ctypes.c_longlong(0)
+        _check(lib().isdf_server_submit(self._h, ctypes.byref(r), ctypes.byref(t)))
+        self._keep[t.value] = (d_psirow, d_thetaCol, piv)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: float = -1.0):
+        """(status, Report) once the request is done."""
+        st = ctypes.c_int(0)
+        rep = _Report()
+        _check(lib().isdf_server_wait(self._h, ticket, timeout_ms, ctypes.byref(st),
+                                      ctypes.byref(rep)))
+        self._keep.pop(ticket, None)
+        return st.value, _report(rep)
+
+    def poll(self, ticket: int):
+        state, st = ctypes.c_int(0), ctypes.c_int(0)
+        rep = _Report()
+        _check(lib().isdf_server_poll(self._h, ticket, ctypes.byref(state), ctypes.byref(st),
+                                      ctypes.byref(rep)))
+        return state.value, st.value
+
+    def cancel(self, ticket: int):
+        _check(lib().isdf_server_cancel(self._h, ticket))
+
+    def stats(self) -> dict:
+        s = _ServerStats()
+        _check(lib().isdf_server_stats(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in _ServerStats._fields_ if k != "reserved0"}
+
+    def close(self):
+        if self._h:
+            lib().isdf_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def workspace_bytes(ng: int, nstate: int, mu: int, selector: int = SELECT_KMEANS,

@@ -53,7 +53,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
         if src.endswith(".cpp"):
-            cmd = [NVCC] + FLAGS + ["-x", "c++", "-c", src, "-o", obj]
+            cmd = [NVCC, "-Wno-deprecated-gpu-targets"] + FLAGS + ["-x", "c++", "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))

@@ -136,9 +136,24 @@ size_t solve_workspace_bytes(long long ng, int nstate, int mu, int selector, int
   return a.off + big + 4096;
 }
 
+std::mutex& attr_mutex() {
+  static std::mutex m;
+  return m;
+}
+
+size_t request_footprint(const isdf_domain_t* dom, int nstate, int nv1, int nc1, int nv2, int nc2,
+                         int mu_points, int selector, int check, const isdf_options_t* opt) {
+  const long long ng = (long long)dom->num_grid[0] * dom->num_grid[1] * dom->num_grid[2];
+  const int rk = mu_points == 0 ? default_mu(nv1, nc1, nv2, nc2) : mu_points;
+  return solve_workspace_bytes(ng, nstate, rk, selector, opt ? opt->precision : 0, check,
+                               opt ? opt->qrcp_oversample : 1.5, dom->num_grid,
+                               (nv1 + nc1) * (nv2 + nc2));
+}
+
 int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, int nv1, int nc1,
           int nv2, int nc2, int mu_points, double* d_theta, int* piv, int kmeans_max_iter,
-          int selector, int check, const isdf_options_t* opt_in, isdf_report_t* rep_out) {
+          int selector, int check, const isdf_options_t* opt_in, isdf_report_t* rep_out,
+          const SolveResources* res) {
   auto t0 = std::chrono::steady_clock::now();
   isdf_options_t opt;
   isdf_default_options(&opt);
@@ -169,14 +184,24 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
     return record_error(ISDF_ERR_ARG, "QRCP oversampling factor must be positive");
   rep.rk_requested = rk;
 
-  std::lock_guard<std::mutex> lock(workspace_mutex());
+  const size_t need = solve_workspace_bytes(ng, nstate, rk, selector, opt.precision, check,
+                                            opt.qrcp_oversample, dom->num_grid,
+                                            (nv1 + nc1) * (nv2 + nc2));
+  std::unique_lock<std::mutex> lock;
   Arena arena;
-  cudaStream_t lib_stream;
-  ISDF_TRY(acquire_workspace(
-      solve_workspace_bytes(ng, nstate, rk, selector, opt.precision, check, opt.qrcp_oversample,
-                            dom->num_grid, (nv1 + nc1) * (nv2 + nc2)),
-      &arena, &lib_stream));
-  cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : lib_stream;
+  cudaStream_t s;
+  if (res) {  // the caller's workspace and stream (the serving loop)
+    if (res->cap < need) return record_error(ISDF_ERR_NOMEM, "solve: workspace below footprint");
+    arena.base = res->base;
+    arena.cap = res->cap;
+    arena.off = 0;
+    s = res->stream;
+  } else {
+    lock = std::unique_lock<std::mutex>(workspace_mutex());
+    cudaStream_t lib_stream;
+    ISDF_TRY(acquire_workspace(need, &arena, &lib_stream));
+    s = opt.stream ? (cudaStream_t)opt.stream : lib_stream;
+  }
   double* d_w = arena.take<double>((size_t)ng);
   const size_t mark = arena.off;
 
@@ -313,7 +338,7 @@ int isdf_solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nsta
                isdf_report_t* rep) {
   try {
     return solve(dom, d_psi, nocc, nstate, nv1, nc1, nv2, nc2, mu_points, d_theta, piv,
-                 kmeans_max_iter, selector, check, opt, rep);
+                 kmeans_max_iter, selector, check, opt, rep, nullptr);
   } catch (const std::exception& e) {
     return record_error(ISDF_ERR_NOMEM, e.what());
   } catch (...) {

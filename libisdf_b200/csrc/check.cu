@@ -17,6 +17,7 @@
 #include <cufft.h>
 
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "arena.h"
@@ -24,6 +25,7 @@
 #include "common.cuh"
 #include "dgemm.cuh"
 #include "fit.h"
+#include "solve.h"
 
 namespace isdf_b200 {
 
@@ -235,6 +237,7 @@ int check_run(const CheckArgs& args, Arena& arena, cudaStream_t s, double* fit_e
     static bool attr_set[64] = {};
     int dev = 0;
     ISDF_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> attr_lock(attr_mutex());
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
       ISDF_CUDA(cudaFuncSetAttribute(k_fit_err, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)CoreC::SMEM_BYTES));

@@ -28,10 +28,12 @@
 // diagonal blocks are inverted explicitly; every other block takes part by
 // substitution, as in a blocked dtrsm.
 // theta is column-major Ng x rk (ld = Ng), overwritten in place.
+#include <mutex>
 #include <vector>
 
 #include "arena.h"
 #include "common.cuh"
+#include "solve.h"
 #include "dgemm.cuh"
 #include "fit.h"
 #include "ozaki.cuh"
@@ -272,6 +274,7 @@ int set_attr(K kernel, size_t bytes) {
 }
 
 int set_smem_attrs() {
+  std::lock_guard<std::mutex> attr_lock(attr_mutex());
   static bool done_dev[64] = {};
   int dev = 0;
   ISDF_CUDA(cudaGetDevice(&dev));
@@ -585,6 +588,7 @@ int ozaki_gemm(const MixedBuffers& b, int M, int N, int kp, double* C, long long
   static bool attr[64] = {};
   int dev = 0;
   ISDF_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> attr_lock(attr_mutex());
   if (dev >= 0 && dev < 64 && !attr[dev]) {
     ISDF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    ozaki::Cfg<S>::SMEM));

@@ -16,6 +16,7 @@
 //   pw        weight w[pidx[p]];
 //   label[p]  nearest centroid.
 // Centroids: double4 (x, y, z, 0) in cen[], rk on the device in st->rk.
+#include <mutex>
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -24,6 +25,7 @@
 
 #include "arena.h"
 #include "common.cuh"
+#include "solve.h"
 #include "kmeans.h"
 
 namespace isdf_b200 {
@@ -633,6 +635,7 @@ __global__ void k_final_reduce(const double* __restrict__ part_d, const int* __r
 
 // Dynamic shared memory above 48 KB needs an opt-in per kernel and device.
 int set_kmeans_smem_attrs() {
+  std::lock_guard<std::mutex> attr_lock(attr_mutex());
   static bool done[64] = {};
   int dev = 0;
   ISDF_CUDA(cudaGetDevice(&dev));
@@ -813,7 +816,12 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
   ISDF_TRY(set_kmeans_smem_attrs());
   int chunks = 0;
   const int max_chunks = args.max_iter / kIterChunk + 2;
-  for (;;) {
+  // One chunk = kIterChunk Lloyd iterations (10 launches each; every kernel
+  // returns at once when the loop has stopped). The chunk is captured once
+  // into a CUDA graph and replayed, which removes the per-launch host cost
+  // that dominates small solves; direct launches are the fallback when the
+  // stream cannot be captured.
+  auto launch_chunk = [&]() {
     for (int it = 0; it < kIterChunk; ++it) {
       k_iter_begin<<<1, 1, 0, stream>>>(b.st, max_f, args.max_iter);
       k_hist<<<ntiles, 256, hist_smem, stream>>>(b.label, n, b.st, b.hist);
@@ -831,6 +839,28 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
                                                           b.label, 1);
       k_iter_end<<<1, 1, 0, stream>>>(b.st);
     }
+  };
+  cudaGraphExec_t exec = nullptr;
+  {
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      launch_chunk();
+      if (cudaStreamEndCapture(stream, &graph) == cudaSuccess && graph) {
+        if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) exec = nullptr;
+        cudaGraphDestroy(graph);
+      }
+    }
+    (void)cudaGetLastError();  // a refused capture leaves an error to clear
+  }
+  struct ExecGuard {
+    cudaGraphExec_t e;
+    ~ExecGuard() {
+      if (e) cudaGraphExecDestroy(e);
+    }
+  } guard{exec};
+  for (;;) {
+    if (exec) ISDF_CUDA(cudaGraphLaunch(exec, stream));
+    else launch_chunk();
     ISDF_CHECK_LAUNCH();
     ISDF_CUDA(cudaMemcpyAsync(&hst, b.st, sizeof(KmState), cudaMemcpyDeviceToHost, stream));
     ISDF_CUDA(cudaStreamSynchronize(stream));

@@ -24,6 +24,7 @@
 // Orthonormalising G by Householder QR instead of the reference's dgesvd
 // changes G1, G2 by orthogonal factors: MG changes by an orthogonal matrix on
 // its left, which leaves the column norms and the pivot sequence unchanged.
+#include <mutex>
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -438,6 +439,7 @@ QrBuffers carve(Arena& a, long long n, int p, int k1, int k2, int kmax) {
 }
 
 int set_update_attrs() {
+  std::lock_guard<std::mutex> attr_lock(attr_mutex());
   static bool done[64] = {};
   int dev = 0;
   ISDF_CUDA(cudaGetDevice(&dev));

@@ -1,0 +1,343 @@
+// Continuous-batching ISDF server (isdf_server_* in include/isdf_c.h).
+//
+// No counterpart in the reference, which solves one system per call. The
+// server keeps a queue of requests and `slots` workers; each worker owns a
+// CUDA stream and takes its workspace from a private stream-ordered memory
+// pool, so solves on different slots run concurrently and their kernels
+// overlap on the GPU. psi and theta stay in the caller's device buffers.
+//
+// Admission is by device footprint: a request starts only when its
+// workspace fits in what the budget has left. A free slot takes the oldest
+// queued request that fits; smaller requests may start ahead of a large head
+// that does not fit yet, but only until the head has been passed over
+// `max_skips` times, after which nothing new starts until it fits. Latency
+// is measured from submit to completion; p50 / p99 and solves/s are
+// reported by isdf_server_stats().
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/isdf_c.h"
+#include "arena.h"
+#include "solve.h"
+
+namespace isdf_b200 {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Job {
+  long long ticket;
+  isdf_request_t req;
+  size_t footprint;
+  int state = 0;  // 0 queued, 1 running, 2 done
+  int status = ISDF_OK;
+  int skips = 0;
+  isdf_report_t rep;
+  Clock::time_point submit, start, finish;
+};
+
+struct Server {
+  isdf_server_config_t cfg;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<long long> queue;
+  std::map<long long, Job> jobs;
+  long long next_ticket = 1;
+  size_t in_use = 0, peak_bytes = 0;
+  int running = 0, peak_running = 0;
+  bool stopping = false;
+  std::vector<std::thread> workers;
+  cudaMemPool_t pool = nullptr;
+  std::vector<double> latencies_ms;
+  Clock::time_point first_submit, last_finish;
+  bool any_submit = false;
+  long long completed = 0, failed = 0, cancelled = 0;
+};
+
+int set_err(int code, const char* msg);
+
+// Next job a free slot may start (under the lock), or -1.
+long long pick(Server* s) {
+  const size_t left = s->cfg.hbm_budget_bytes > s->in_use ? s->cfg.hbm_budget_bytes - s->in_use : 0;
+  for (size_t i = 0; i < s->queue.size(); ++i) {
+    Job& j = s->jobs[s->queue[i]];
+    if (j.footprint <= left) {
+      if (i > 0) {
+        Job& head = s->jobs[s->queue[0]];
+        if (head.skips >= s->cfg.max_skips) return -1;  // the head waits for room; nothing passes it
+        head.skips++;
+      }
+      long long t = s->queue[i];
+      s->queue.erase(s->queue.begin() + (long)i);
+      return t;
+    }
+  }
+  return -1;
+}
+
+void worker(Server* s, int slot) {
+  cudaSetDevice(s->cfg.device);
+  cudaStream_t stream = nullptr;
+  cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+  (void)slot;
+  for (;;) {
+    long long t = -1;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_work.wait(lk, [&] {
+        if (s->stopping) return true;
+        return (t = pick(s)) >= 0;
+      });
+      if (t < 0) break;  // stopping and nothing startable
+      Job& j = s->jobs[t];
+      j.state = 1;
+      j.start = Clock::now();
+      s->in_use += j.footprint;
+      s->peak_bytes = std::max(s->peak_bytes, s->in_use);
+      s->running++;
+      s->peak_running = std::max(s->peak_running, s->running);
+    }
+    Job* jp;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      jp = &s->jobs[t];
+    }
+    isdf_request_t req = jp->req;
+    isdf_report_t rep;
+    std::memset(&rep, 0, sizeof(rep));
+    int rc = ISDF_OK;
+    void* ws = nullptr;
+    if (cudaMallocFromPoolAsync(&ws, jp->footprint, s->pool, stream) != cudaSuccess) {
+      (void)cudaGetLastError();
+      rc = set_err(ISDF_ERR_NOMEM, "server: workspace allocation failed");
+    } else {
+      SolveResources res{static_cast<char*>(ws), jp->footprint, stream};
+      rc = solve(&req.dom, req.d_psi, req.nocc, req.nstate, req.nv1, req.nc1, req.nv2, req.nc2,
+                 req.mu_points, req.d_theta, req.piv, req.kmeans_max_iter, req.selector, req.check,
+                 &req.opt, &rep, &res);
+      cudaFreeAsync(ws, stream);
+      cudaStreamSynchronize(stream);
+    }
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      Job& j = s->jobs[t];
+      j.state = 2;
+      j.status = rc;
+      j.rep = rep;
+      j.finish = Clock::now();
+      s->in_use -= j.footprint;
+      s->running--;
+      s->last_finish = j.finish;
+      if (rc == ISDF_OK) {
+        s->completed++;
+        s->latencies_ms.push_back(
+            std::chrono::duration<double, std::milli>(j.finish - j.submit).count());
+      } else {
+        s->failed++;
+      }
+    }
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+  }
+  cudaStreamDestroy(stream);
+}
+
+double percentile(std::vector<double> v, double q) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  const double pos = q * (double)(v.size() - 1);
+  const size_t lo = (size_t)pos;
+  const size_t hi = std::min(lo + 1, v.size() - 1);
+  return v[lo] + (v[hi] - v[lo]) * (pos - (double)lo);
+}
+
+}  // namespace
+}  // namespace isdf_b200
+
+using namespace isdf_b200;
+
+namespace isdf_b200 {
+namespace {
+int set_err(int code, const char* msg) { return record_error(code, msg); }
+}  // namespace
+}  // namespace isdf_b200
+
+extern "C" {
+
+void isdf_server_default_config(isdf_server_config_t* cfg) {
+  if (!cfg) return;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->device = 0;
+  cfg->slots = 4;
+  cfg->hbm_budget_bytes = 0;
+  cfg->max_queue = 4096;
+  cfg->max_skips = 64;
+}
+
+int isdf_server_create(const isdf_server_config_t* cfg_in, void** out) {
+  if (!out) return record_error(ISDF_ERR_ARG, "server: null output");
+  isdf_server_config_t cfg;
+  isdf_server_default_config(&cfg);
+  if (cfg_in) cfg = *cfg_in;
+  if (cfg.slots < 1 || cfg.slots > 64) return record_error(ISDF_ERR_ARG, "server: slots in [1, 64]");
+  if (cudaSetDevice(cfg.device) != cudaSuccess) return record_error(ISDF_ERR_ARG, "server: device");
+  if (cfg.hbm_budget_bytes == 0) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess)
+      return record_error(ISDF_ERR_CUDA, "server: cudaMemGetInfo failed");
+    cfg.hbm_budget_bytes = free_b / 2;
+  }
+  Server* s = new Server();
+  s->cfg = cfg;
+  cudaMemPoolProps props;
+  std::memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = cfg.device;
+  if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess) {
+    delete s;
+    return record_error(ISDF_ERR_CUDA, "server: cudaMemPoolCreate failed");
+  }
+  unsigned long long keep = cfg.hbm_budget_bytes;
+  cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  for (int i = 0; i < cfg.slots; ++i) s->workers.emplace_back(worker, s, i);
+  *out = s;
+  return ISDF_OK;
+}
+
+int isdf_server_submit(void* server, const isdf_request_t* req, long long* ticket) {
+  Server* s = static_cast<Server*>(server);
+  if (!s || !req || !ticket) return record_error(ISDF_ERR_ARG, "server: null argument");
+  if (!req->d_psi || !req->d_theta || !req->piv)
+    return record_error(ISDF_ERR_ARG, "server: request buffers");
+  const size_t fp = request_footprint(&req->dom, req->nstate, req->nv1, req->nc1, req->nv2,
+                                      req->nc2, req->mu_points, req->selector, req->check,
+                                      &req->opt);
+  if (fp > s->cfg.hbm_budget_bytes)
+    return record_error(ISDF_ERR_UNSUPPORTED, "server: request larger than the whole budget");
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stopping) return record_error(ISDF_ERR_CANCELLED, "server: stopping");
+    if ((int)s->queue.size() >= s->cfg.max_queue) return record_error(ISDF_ERR_BUSY, "server: queue full");
+    Job j;
+    j.ticket = s->next_ticket++;
+    j.req = *req;
+    j.req.opt.stream = nullptr;
+    j.footprint = fp;
+    j.submit = Clock::now();
+    std::memset(&j.rep, 0, sizeof(j.rep));
+    if (!s->any_submit) {
+      s->first_submit = j.submit;
+      s->any_submit = true;
+    }
+    *ticket = j.ticket;
+    s->jobs[j.ticket] = j;
+    s->queue.push_back(j.ticket);
+  }
+  s->cv_work.notify_one();
+  return ISDF_OK;
+}
+
+int isdf_server_poll(void* server, long long ticket, int* state, int* status, isdf_report_t* rep) {
+  Server* s = static_cast<Server*>(server);
+  if (!s) return record_error(ISDF_ERR_ARG, "server: null");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(ticket);
+  if (it == s->jobs.end()) return record_error(ISDF_ERR_ARG, "server: unknown ticket");
+  if (state) *state = it->second.state;
+  if (status) *status = it->second.status;
+  if (rep && it->second.state == 2) *rep = it->second.rep;
+  return ISDF_OK;
+}
+
+int isdf_server_wait(void* server, long long ticket, double timeout_ms, int* status,
+                     isdf_report_t* rep) {
+  Server* s = static_cast<Server*>(server);
+  if (!s) return record_error(ISDF_ERR_ARG, "server: null");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(ticket);
+  if (it == s->jobs.end()) return record_error(ISDF_ERR_ARG, "server: unknown ticket");
+  auto done = [&] { return s->jobs[ticket].state == 2; };
+  if (timeout_ms < 0) s->cv_done.wait(lk, done);
+  else if (!s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), done))
+    return record_error(ISDF_ERR_TIMEOUT, "server: wait timed out");
+  Job& j = s->jobs[ticket];
+  if (status) *status = j.status;
+  if (rep) *rep = j.rep;
+  return ISDF_OK;
+}
+
+int isdf_server_cancel(void* server, long long ticket) {
+  Server* s = static_cast<Server*>(server);
+  if (!s) return record_error(ISDF_ERR_ARG, "server: null");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = std::find(s->queue.begin(), s->queue.end(), ticket);
+  if (it == s->queue.end()) return record_error(ISDF_ERR_ARG, "server: not queued (running or done)");
+  s->queue.erase(it);
+  Job& j = s->jobs[ticket];
+  j.state = 2;
+  j.status = ISDF_ERR_CANCELLED;
+  j.finish = Clock::now();
+  s->cancelled++;
+  s->cv_done.notify_all();
+  return ISDF_OK;
+}
+
+int isdf_server_stats(void* server, isdf_server_stats_t* st) {
+  Server* s = static_cast<Server*>(server);
+  if (!s || !st) return record_error(ISDF_ERR_ARG, "server: null");
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::memset(st, 0, sizeof(*st));
+  st->submitted = s->next_ticket - 1;
+  st->completed = s->completed;
+  st->failed = s->failed;
+  st->cancelled = s->cancelled;
+  st->p50_ms = percentile(s->latencies_ms, 0.50);
+  st->p99_ms = percentile(s->latencies_ms, 0.99);
+  double sum = 0;
+  for (double v : s->latencies_ms) sum += v;
+  st->mean_ms = s->latencies_ms.empty() ? 0.0 : sum / (double)s->latencies_ms.size();
+  const double span = s->any_submit && s->completed
+                          ? std::chrono::duration<double>(s->last_finish - s->first_submit).count()
+                          : 0.0;
+  st->solves_per_s = span > 0 ? (double)s->completed / span : 0.0;
+  st->peak_concurrency = s->peak_running;
+  st->peak_bytes = s->peak_bytes;
+  st->queued = (int)s->queue.size();
+  st->running = s->running;
+  return ISDF_OK;
+}
+
+int isdf_server_destroy(void* server) {
+  Server* s = static_cast<Server*>(server);
+  if (!s) return ISDF_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (long long t : s->queue) {
+      Job& j = s->jobs[t];
+      j.state = 2;
+      j.status = ISDF_ERR_CANCELLED;
+      s->cancelled++;
+    }
+    s->queue.clear();
+    s->stopping = true;
+  }
+  s->cv_work.notify_all();
+  s->cv_done.notify_all();
+  for (auto& w : s->workers) w.join();
+  if (s->pool) cudaMemPoolDestroy(s->pool);
+  delete s;
+  return ISDF_OK;
+}
+
+}  // extern "C"

@@ -6,6 +6,7 @@
 
 #include <mutex>
 
+#include "../../include/isdf_c.h"
 #include "arena.h"
 
 namespace isdf_b200 {
@@ -16,5 +17,25 @@ size_t solve_workspace_bytes(long long ng, int nstate, int mu, int selector, int
                              int check, double qrcp_factor, const int* num_grid, int npair);
 int acquire_workspace(size_t bytes, Arena* arena, cudaStream_t* lib_stream);
 std::mutex& workspace_mutex();
+int record_error(int code, const char* msg);
+
+// Guards the one-time per-device kernel attribute settings.
+std::mutex& attr_mutex();
+
+// A caller-owned workspace and stream for one solve (the serving loop's slots).
+struct SolveResources {
+  char* base;
+  size_t cap;
+  cudaStream_t stream;
+};
+
+// Device workspace one solve with these parameters needs.
+size_t request_footprint(const isdf_domain_t* dom, int nstate, int nv1, int nc1, int nv2, int nc2,
+                         int mu_points, int selector, int check, const isdf_options_t* opt);
+
+int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, int nv1, int nc1,
+          int nv2, int nc2, int mu_points, double* d_theta, int* piv, int kmeans_max_iter,
+          int selector, int check, const isdf_options_t* opt, isdf_report_t* rep,
+          const SolveResources* res);
 
 }  // namespace isdf_b200
