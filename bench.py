@@ -119,6 +119,23 @@ def _fp64_peak_tflops(torch):
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
+def max_over_ranks(x: float, dist=None, device="cpu") -> float:
+    """The slowest rank's figure: every rank calls this at the same point."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world: int, steps: int, t_ms: float) -> float:
+    """Whole-job solves/s: every rank ran `steps` independent solves; t_ms is
+    the max over ranks of the timed region."""
+    return world * steps / (t_ms * 1e-3)
+
+
 # ------------------------------------------------------------------ reference arm
 def reference_sample(shape, iters: int, repeats: int = 1):
     """Seconds per solve of the reference's CPU path, from a bounded sample:
@@ -232,11 +249,8 @@ def run_ours(args, shape):
                 launches.append(rep.kernel_launches)
             e_end.record(stream)
             torch.cuda.synchronize()
-        t_ms = e_start.elapsed_time(e_end)
+        t_ms = max_over_ranks(e_start.elapsed_time(e_end), dist, "cuda")
         if dist:
-            tt = torch.tensor([t_ms], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t_ms = float(tt.item())
             dist.barrier()
 
         # end to end from host buffers: H2D psi, solve, D2H theta
@@ -254,22 +268,28 @@ def run_ours(args, shape):
             h_theta.copy_(d_theta, non_blocking=True)
         e1.record(stream)
         torch.cuda.synchronize()
-        e2e_ms = e0.elapsed_time(e1)
-        if dist:
-            tt = torch.tensor([e2e_ms], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_ms = float(tt.item())
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
 
     if dist:
         dist.destroy_process_group()
     if rank != 0:
         return
     peaks, peak_src = _measured_peaks()
-    v = world * args.steps / (t_ms * 1e-3)
-    # dominant kernel: the triangular-solve stage (FP64), 2*Ng*rk^2 flops per solve
+    v = replica_value(world, args.steps, t_ms)
+    # Dominant kernel: k_trsm_gemm, the two triangular sweeps as in-place FP64
+    # tensor-core GEMMs. Algorithmic flops per solve: 2*Ng*rk^2 (Ng*rk^2 per
+    # sweep). Its time is the triangular-solve stage on the solve stream
+    # (CUDA events in the library around the stage: the k_trsm_gemm launches
+    # plus the small k_build_w launches between them), so the rate is a
+    # slight underestimate of the kernel's own.
     rk = rep.rk_eff
     t_solve_ms = float(np.median([s[2] for s in stage]))
     achieved = 2.0 * ng * rk * rk / (t_solve_ms * 1e-3) / 1e12 if t_solve_ms > 0 else None
+    # DRAM traffic of one launch: 8.37 B per grid row and solved column
+    # (dram__bytes_read.sum + dram__bytes_write.sum of ncu on the 40^3-grid
+    # case), times the mean solved width of a launch over both sweeps
+    # (rk/2 + 32 columns).
+    traffic = 8.37 * ng * (rk / 2 + 32)
     line = {
         "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": t_ms / args.steps,
@@ -278,20 +298,25 @@ def run_ours(args, shape):
         "config": {"workload": shape.name, "ng": ng, "nstate": shape.nstate, "mu": mu,
                    "rk_eff": rk, "kmeans_iters": rep.kmeans_iters, "selector": "Kmeans",
                    "precision": args.precision, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (psi 1.05 GB, theta 8.4 GB)"},
+                   "l2": (f"inputs larger than L2 (psi {ng * shape.nstate * 8 / 1e9:.2f} GB, "
+                          f"theta {ng * mu * 8 / 1e9:.2f} GB; L2 126 MB)")},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "stages_ms": {"select_wall": float(np.median([s[0] for s in stage])),
                       "fit_wall": float(np.median([s[1] for s in stage])),
                       "zct_gemm": float(np.median([s[3] for s in stage])),
                       "cct_cholesky": float(np.median([s[4] for s in stage])),
                       "triangular_solve": t_solve_ms},
-        "roofline": {"kernel": "k_trsm_step (both sweeps of the triangular solve)",
+        "roofline": {"kernel": "k_trsm_gemm (both sweeps of the triangular solve)",
                      "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
                      "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved else None,
-                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64; "
-                                    f"MEASURED_PEAKS.json has no FP64 figure, {peak_src})",
-                     "traffic": None},
-        "e2e": {"value": world * e2e_steps / (e2e_ms * 1e-3), "unit": "solves/s",
+                     "peak_source": ("cuBLAS DGEMM 8192^3 measured in this run: the FP64 "
+                                     "denominator (the measured-peaks file holds HBM and BF16 "
+                                     f"figures only; HBM {peaks.get('hbm_gbs')} GB/s from "
+                                     f"{peak_src})"),
+                     "traffic": traffic,
+                     "traffic_note": "bytes per launch (mean over the sweep), scaled from the "
+                                     "ncu capture at Ng = 64000 by rows x solved columns"},
+        "e2e": {"value": replica_value(world, e2e_steps, e2e_ms), "unit": "solves/s",
                 "h2d_bytes_per_step": int(h_psi.numel() * 8),
                 "d2h_bytes_per_step": int(h_theta.numel() * 8 + piv.nbytes)},
         "gpu_launches": int(sum(launches)),
@@ -307,21 +332,62 @@ def run_ours(args, shape):
     print(json.dumps(line), flush=True)
 
 
+def run_select(args, shape):
+    """--stage select: the K-means selection alone (weight computed once),
+    selections/s; a small-footprint command for profiling the K-means kernels
+    at full grid size (psi, the weight and the K-means workspace only)."""
+    import torch
+
+    import libisdf_b200 as isdf
+    from libisdf_b200 import synth
+
+    torch.cuda.set_device(0)
+    psi = synth.shape_orbitals(shape, 1, device="cuda")
+    d_psi = torch.from_numpy(np.ascontiguousarray(psi.T)).cuda()
+    d_w = torch.empty(shape.ng, dtype=torch.float64, device="cuda")
+    dom = isdf.Domain(length=(shape.length,) * 3, num_grid=(shape.n,) * 3)
+    stream = torch.cuda.Stream()
+    isdf.kmeans_weight(d_psi, shape.ng, shape.nstate, shape.nocc, shape.nv1, shape.nc1, shape.nv2,
+                       shape.nc2, d_w, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    for _ in range(max(3, args.warmup)):
+        isdf.kmeans_select(dom, d_w, shape.mu, shape.kmeans_iters, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        _, rk, iters, npt = isdf.kmeans_select(dom, d_w, shape.mu, shape.kmeans_iters,
+                                               stream=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_ms = e0.elapsed_time(e1)
+    print(json.dumps({"metric": "K-means selections/s", "value": args.steps / (t_ms * 1e-3),
+                      "unit": "selections/s", "n_gpus": 1, "steps": args.steps,
+                      "warmup": max(3, args.warmup), "ms_per_step": t_ms / args.steps,
+                      "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": shape.name, "ng": shape.ng, "mu": shape.mu,
+                                 "rk_eff": rk, "kmeans_iters": iters, "npt": npt}}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["si8", "si64", "si216"], default="si64")
+    ap.add_argument("--config", choices=["si8", "si64", "si216", "si64c"], default="si64")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--stage", choices=["solve", "select"], default="solve",
+                    help="select: time the K-means selection alone (profiling aid)")
     args = ap.parse_args()
     from libisdf_b200 import synth
 
     shape = synth.SHAPES[args.config]
     if args.impl == "reference":
         run_reference(args, shape)
+    elif args.stage == "select":
+        run_select(args, shape)
     else:
         run_ours(args, shape)
 

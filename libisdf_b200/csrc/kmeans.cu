@@ -401,11 +401,17 @@ __global__ void __launch_bounds__(1024) k_label_start(const int* __restrict__ me
 
 // One tile per block: 128 threads stage the tile's labels in shared memory,
 // then one warp walks them in order and scatters every point to its stable
-// position (peers with equal labels share one running offset).
+// position (peers with equal labels share one running offset). What lands
+// there is the point's (w x, w y, w z, w), so that the per-cluster fold reads
+// its members contiguously.
 __global__ void __launch_bounds__(128) k_scatter(const int* __restrict__ label, int n,
                                                  const KmState* st, const int* __restrict__ hist,
                                                  const int* __restrict__ start,
-                                                 int* __restrict__ sorted) {
+                                                 const double* __restrict__ px,
+                                                 const double* __restrict__ py,
+                                                 const double* __restrict__ pz,
+                                                 const double* __restrict__ pw,
+                                                 double4* __restrict__ sorted) {
   if (st->done) return;
   extern __shared__ int sm_scatter[];
   const int rk = st->rk;
@@ -428,7 +434,9 @@ __global__ void __launch_bounds__(128) k_scatter(const int* __restrict__ label, 
     __syncwarp();
     if (ok) {
       const int r = __popc(peers & ((1u << lane) - 1u));
-      sorted[b + r] = base + k;
+      const int p = base + k;
+      const double w = pw[p];
+      sorted[b + r] = make_double4(rmul(w, px[p]), rmul(w, py[p]), rmul(w, pz[p]), w);
       if (lane == __ffs(peers) - 1) run[l] = b + __popc(peers);
     }
     __syncwarp();
@@ -480,8 +488,21 @@ __device__ double repeat_add(double acc, double c, long long m) {
 // One warp per cluster: sequential fold over the members (in index order).
 // The zero-tail points p >= npt are identical copies of grid point 0 (weight
 // w[0], coordinates (0, 0, 0)) and come last in their cluster's member list,
-// so their part of the fold is a repeated addition of one value.
-__global__ void __launch_bounds__(256) k_segsum(const int* __restrict__ sorted,
+// so their part of the fold is a repeated addition of one value. The members'
+// (w x, w y, w z, w) are read contiguously, kSegBatches batches of 32 ahead
+// of the fold, so that the load latency hides behind the dependent additions.
+constexpr int kSegBatches = 4;
+
+__device__ __forceinline__ void seg_load(const double4* __restrict__ v, int q, int m, int lane,
+                                         double4 (&out)[kSegBatches]) {
+#pragma unroll
+  for (int j = 0; j < kSegBatches; ++j) {
+    const int i = q + j * 32 + lane;
+    out[j] = i < m ? v[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_segsum(const double4* __restrict__ sorted,
                                                 const int* __restrict__ start,
                                                 const int* __restrict__ members,
                                                 const double* __restrict__ px,
@@ -496,7 +517,7 @@ __global__ void __launch_bounds__(256) k_segsum(const int* __restrict__ sorted,
   const int lane = threadIdx.x & 31;
   if (c >= rk) return;
   const int npt = st->npt;
-  const int s0 = start[c];
+  const double4* v = sorted + start[c];
   int m = members[c];
   long long tail = 0;
   if (npt < n && label[npt] == c) {
@@ -504,22 +525,32 @@ __global__ void __launch_bounds__(256) k_segsum(const int* __restrict__ sorted,
     m -= (int)tail;
   }
   double aw = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
-  for (int q = 0; q < m; q += 32) {
-    double vw = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
-    if (q + lane < m) {
-      const int p = sorted[s0 + q + lane];
-      vw = pw[p];
-      vx = rmul(vw, px[p]);
-      vy = rmul(vw, py[p]);
-      vz = rmul(vw, pz[p]);
+  double4 cur[kSegBatches], nxt[kSegBatches];
+  seg_load(v, 0, m, lane, cur);
+  for (int q = 0; q < m; q += 32 * kSegBatches) {
+    if (q + 32 * kSegBatches < m) seg_load(v, q + 32 * kSegBatches, m, lane, nxt);
+#pragma unroll
+    for (int j = 0; j < kSegBatches; ++j) {
+      const int cnt = min(32, m - (q + 32 * j));  // warp-uniform
+      if (cnt == 32) {
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+          aw = radd(aw, __shfl_sync(0xffffffffu, cur[j].w, k));
+          ax = radd(ax, __shfl_sync(0xffffffffu, cur[j].x, k));
+          ay = radd(ay, __shfl_sync(0xffffffffu, cur[j].y, k));
+          az = radd(az, __shfl_sync(0xffffffffu, cur[j].z, k));
+        }
+      } else {
+        for (int k = 0; k < cnt; ++k) {
+          aw = radd(aw, __shfl_sync(0xffffffffu, cur[j].w, k));
+          ax = radd(ax, __shfl_sync(0xffffffffu, cur[j].x, k));
+          ay = radd(ay, __shfl_sync(0xffffffffu, cur[j].y, k));
+          az = radd(az, __shfl_sync(0xffffffffu, cur[j].z, k));
+        }
+      }
     }
-    const int cnt = min(32, m - q);
-    for (int k = 0; k < cnt; ++k) {
-      aw = radd(aw, __shfl_sync(0xffffffffu, vw, k));
-      ax = radd(ax, __shfl_sync(0xffffffffu, vx, k));
-      ay = radd(ay, __shfl_sync(0xffffffffu, vy, k));
-      az = radd(az, __shfl_sync(0xffffffffu, vz, k));
-    }
+#pragma unroll
+    for (int j = 0; j < kSegBatches; ++j) cur[j] = nxt[j];
   }
   if (lane == 0) {
     if (tail) {
@@ -652,7 +683,7 @@ struct KmBuffers {
   int* pidx;
   double *px, *py, *pz, *pw;
   int* label;
-  int* sorted;
+  double4* sorted;  // (w x, w y, w z, w) in cluster order
   int* hist;
   int* members;
   int* start;
@@ -679,7 +710,7 @@ KmBuffers carve(Arena& a, int n, int mu) {
   b.pz = a.take<double>(n);
   b.pw = a.take<double>(n);
   b.label = a.take<int>(n);
-  b.sorted = a.take<int>(n);
+  b.sorted = a.take<double4>(n);
   b.hist = a.take<int>((size_t)ntiles * mu);
   b.members = a.take<int>(mu);
   b.start = a.take<int>(mu);
@@ -827,8 +858,8 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
       k_hist<<<ntiles, 256, hist_smem, stream>>>(b.label, n, b.st, b.hist);
       k_hist_scan<<<grid_for(mu, 256), 256, 0, stream>>>(b.hist, ntiles, b.st, b.members);
       k_label_start<<<1, 1024, 0, stream>>>(b.members, b.st, b.start);
-      k_scatter<<<ntiles, 128, scatter_smem, stream>>>(b.label, n, b.st, b.hist, b.start,
-                                                       b.sorted);
+      k_scatter<<<ntiles, 128, scatter_smem, stream>>>(b.label, n, b.st, b.hist, b.start, b.px,
+                                                       b.py, b.pz, b.pw, b.sorted);
       k_segsum<<<grid_for(mu, 8), 256, 0, stream>>>(b.sorted, b.start, b.members, b.px, b.py,
                                                     b.pz, b.pw, b.label, n, b.st, b.sums);
       k_centroids<<<1, 1024, 0, stream>>>(b.sums, b.st, b.cen);

@@ -67,7 +67,10 @@ class Shape:
 SI8 = Shape("Si8-like 40^3", 1, 40, 32, 16, 16, 16, 16, 16, 320)
 SI64 = Shape("Si64-like 80^3", 2, 80, 256, 128, 128, 128, 128, 128, 2048)
 SI216 = Shape("Si216-like 108^3", 3, 108, 864, 432, 432, 432, 432, 432, 4320)
-SHAPES = {"si8": SI8, "si64": SI64, "si216": SI216}
+# Si64's states and mu on a 40^3 grid: the profiling size (theta 1 GB, larger
+# than L2, a few GB on the device in all).
+SI64C = Shape("Si64-like on 40^3 (profiling)", 2, 40, 256, 128, 128, 128, 128, 128, 2048)
+SHAPES = {"si8": SI8, "si64": SI64, "si216": SI216, "si64c": SI64C}
 
 
 def diamond_sites(cells: int) -> np.ndarray:
