@@ -189,6 +189,59 @@ def run_reference(args, shape):
     print(json.dumps(line), flush=True)
 
 
+def _int8_peak_tops(torch):
+    """cuBLASLt INT8 GEMM (torch._int_mm, 8192^3, best of 5): the INT8
+    tensor-core denominator for the mixed form's GEMMs."""
+    try:
+        a = torch.randint(-127, 128, (8192, 8192), dtype=torch.int8, device="cuda")
+        b = torch.randint(-127, 128, (8192, 8192), dtype=torch.int8, device="cuda").t()
+        for _ in range(2):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        torch.cuda.empty_cache()
+        return 2 * 8192 ** 3 / (best * 1e-3) / 1e12, "cuBLASLt INT8 GEMM 8192^3 measured in this run"
+    except Exception as e:  # noqa: BLE001
+        peaks, _ = _measured_peaks()
+        return 2.0 * peaks["bf16_tflops"], f"2 x measured dense BF16 (INT8 GEMM unavailable: {e})"
+
+
+def mixed_vs_fp64(torch, shape, psi, d_theta, piv, rk, solve_fp64, n_rows=2048, n_pairs=1024,
+                  seed=0):
+    """Accuracy of the mixed-precision result in d_theta against the FP64
+    form on the same inputs: relative Frobenius error of the fitted pair
+    densities theta C (and of theta) on sampled grid rows and pairs. Runs one
+    FP64 solve into d_theta (outside any timed region)."""
+    rng = np.random.default_rng(seed)
+    ng = psi.shape[0]
+    rows = np.sort(rng.choice(ng, size=min(n_rows, ng), replace=False))
+    idx = torch.from_numpy(rows).cuda()
+    th_m = d_theta[:rk].index_select(1, idx).T.cpu().numpy()
+    piv_m = piv[:rk].copy()
+    solve_fp64()
+    th_f = d_theta[:rk].index_select(1, idx).T.cpu().numpy()
+    if not np.array_equal(piv_m, piv[:rk]):
+        return {"error": "piv differs between the forms"}
+    lo1, lo2 = shape.nocc - shape.nv1, shape.nocc - shape.nv2
+    i = lo1 + rng.integers(0, shape.nv1 + shape.nc1, size=n_pairs)
+    j = lo2 + rng.integers(0, shape.nv2 + shape.nc2, size=n_pairs)
+    pm = psi[piv_m]  # rk x nstate
+    C = pm[:, i] * pm[:, j]
+    fd_m, fd_f = th_m @ C, th_f @ C
+    return {"fitted_densities_rel": float(np.linalg.norm(fd_m - fd_f) / np.linalg.norm(fd_f)),
+            "theta_rel": float(np.linalg.norm(th_m - th_f) / np.linalg.norm(th_f)),
+            "rows": int(len(rows)), "pairs": int(n_pairs),
+            "against": "the FP64 form on the same inputs (parity-tested against the oracle)"}
+
+
 # ------------------------------------------------------------------ our arm
 def run_ours(args, shape):
     import torch
@@ -222,6 +275,7 @@ def run_ours(args, shape):
                          shape.nc2, mu, d_theta, piv, shape.kmeans_iters, options=opts)
 
     fp64_peak = _fp64_peak_tflops(torch)
+    int8_peak = _int8_peak_tops(torch) if args.precision == "mixed" else None
     with torch.cuda.stream(stream):
         for _ in range(max(3, args.warmup)):
             rep = solve()
@@ -245,7 +299,7 @@ def run_ours(args, shape):
                 e1.synchronize()
                 lat.append(e0.elapsed_time(e1))
                 stage.append((rep.t_select_ms, rep.t_fit_ms, rep.t_solve_ms, rep.t_zct_ms,
-                              rep.t_chol_ms))
+                              rep.t_chol_ms, rep.t_gemm_ms))
                 launches.append(rep.kernel_launches)
             e_end.record(stream)
             torch.cuda.synchronize()
@@ -274,22 +328,60 @@ def run_ours(args, shape):
         dist.destroy_process_group()
     if rank != 0:
         return
+    accuracy = None
+    if args.precision == "mixed":
+        opts64 = isdf.Options(stream=stream.cuda_stream, precision=isdf.PRECISION_FP64)
+
+        def solve_fp64():
+            with torch.cuda.stream(stream):
+                isdf.ISDF(d_psi, dom, shape.nocc, shape.nstate, shape.nv1, shape.nc1, shape.nv2,
+                          shape.nc2, mu, d_theta, piv, shape.kmeans_iters, options=opts64)
+            torch.cuda.synchronize()
+
+        accuracy = mixed_vs_fp64(torch, shape, psi, d_theta, piv, rep.rk_eff, solve_fp64)
     peaks, peak_src = _measured_peaks()
     v = replica_value(world, args.steps, t_ms)
-    # Dominant kernel: k_trsm_gemm, the two triangular sweeps as in-place FP64
-    # tensor-core GEMMs. Algorithmic flops per solve: 2*Ng*rk^2 (Ng*rk^2 per
-    # sweep). Its time is the triangular-solve stage on the solve stream
-    # (CUDA events in the library around the stage: the k_trsm_gemm launches
-    # plus the small k_build_w launches between them), so the rate is a
-    # slight underestimate of the kernel's own.
     rk = rep.rk_eff
     t_solve_ms = float(np.median([s[2] for s in stage]))
-    achieved = 2.0 * ng * rk * rk / (t_solve_ms * 1e-3) / 1e12 if t_solve_ms > 0 else None
-    # DRAM traffic of one launch: 8.37 B per grid row and solved column
-    # (dram__bytes_read.sum + dram__bytes_write.sum of ncu on the 40^3-grid
-    # case), times the mean solved width of a launch over both sweeps
-    # (rk/2 + 32 columns).
-    traffic = 8.37 * ng * (rk / 2 + 32)
+    t_gemm_ms = float(np.median([s[5] for s in stage]))
+    if args.precision == "mixed":
+        # Dominant kernel: k_ozaki_gemm, the two triangular products
+        # Y = Z L^-T and theta = Y L^-1 as INT8 digit-pair GEMMs; issued INT8
+        # ops per solve: 2 GEMMs x 2 x Ng x rk x (rk/2 + 32) x S(S+1)/2 (each
+        # tile runs the K range its triangular factor leaves nonzero). Time:
+        # CUDA events around the two launches on the solve stream.
+        S = isdf.Options().mixed_slices
+        ops = 2 * 2.0 * ng * rk * (rk / 2 + 32) * S * (S + 1) / 2
+        achieved = ops / (t_gemm_ms * 1e-3) / 1e12 if t_gemm_ms > 0 else None
+        roofline = {"kernel": "k_ozaki_gemm (Y = Z L^-T and theta = Y L^-1, INT8 digit pairs)",
+                    "bound": "tensor", "achieved": achieved, "peak": int8_peak[0],
+                    "unit": "TOPS (INT8)", "frac": (achieved / int8_peak[0]) if achieved else None,
+                    "peak_source": int8_peak[1],
+                    "emulated_fp64_tflops": (2.0 * 2 * ng * rk * (rk / 2 + 32) /
+                                             (t_gemm_ms * 1e-3) / 1e12) if t_gemm_ms > 0 else None,
+                    "traffic": None}
+    else:
+        # Dominant kernel: k_trsm_gemm, the two triangular sweeps as in-place
+        # FP64 tensor-core GEMMs. Algorithmic flops per solve: 2*Ng*rk^2
+        # (Ng*rk^2 per sweep). Its time is the triangular-solve stage on the
+        # solve stream (CUDA events in the library around the stage: the
+        # k_trsm_gemm launches plus the small k_build_w launches between
+        # them), so the rate is a slight underestimate of the kernel's own.
+        achieved = 2.0 * ng * rk * rk / (t_solve_ms * 1e-3) / 1e12 if t_solve_ms > 0 else None
+        # DRAM traffic of one launch: 8.37 B per grid row and solved column
+        # (dram__bytes_read.sum + dram__bytes_write.sum of ncu on the 40^3-grid
+        # case), times the mean solved width of a launch over both sweeps
+        # (rk/2 + 32 columns).
+        roofline = {"kernel": "k_trsm_gemm (both sweeps of the triangular solve)",
+                    "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
+                    "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved else None,
+                    "peak_source": ("cuBLAS DGEMM 8192^3 measured in this run: the FP64 "
+                                    "denominator (the measured-peaks file holds HBM and BF16 "
+                                    f"figures only; HBM {peaks.get('hbm_gbs')} GB/s from "
+                                    f"{peak_src})"),
+                    "traffic": 8.37 * ng * (rk / 2 + 32),
+                    "traffic_note": "bytes per launch (mean over the sweep), scaled from the "
+                                    "ncu capture at Ng = 64000 by rows x solved columns"}
     line = {
         "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": t_ms / args.steps,
@@ -305,21 +397,14 @@ def run_ours(args, shape):
                       "fit_wall": float(np.median([s[1] for s in stage])),
                       "zct_gemm": float(np.median([s[3] for s in stage])),
                       "cct_cholesky": float(np.median([s[4] for s in stage])),
-                      "triangular_solve": t_solve_ms},
-        "roofline": {"kernel": "k_trsm_gemm (both sweeps of the triangular solve)",
-                     "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
-                     "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved else None,
-                     "peak_source": ("cuBLAS DGEMM 8192^3 measured in this run: the FP64 "
-                                     "denominator (the measured-peaks file holds HBM and BF16 "
-                                     f"figures only; HBM {peaks.get('hbm_gbs')} GB/s from "
-                                     f"{peak_src})"),
-                     "traffic": traffic,
-                     "traffic_note": "bytes per launch (mean over the sweep), scaled from the "
-                                     "ncu capture at Ng = 64000 by rows x solved columns"},
+                      "triangular_solve": t_solve_ms,
+                      "triangular_gemms": t_gemm_ms},
+        "roofline": roofline,
         "e2e": {"value": replica_value(world, e2e_steps, e2e_ms), "unit": "solves/s",
                 "h2d_bytes_per_step": int(h_psi.numel() * 8),
                 "d2h_bytes_per_step": int(h_theta.numel() * 8 + piv.nbytes)},
         "gpu_launches": int(sum(launches)),
+        "mixed_vs_fp64": accuracy,
         "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
@@ -369,6 +454,121 @@ def run_select(args, shape):
                                  "rk_eff": rk, "kmeans_iters": iters, "npt": npt}}), flush=True)
 
 
+def run_serve(args):
+    """--serve: the serving mix (60 % Si8-like, 30 % Si64-like, 10 % Si216-like
+    requests, K-means, --precision) arriving as a Poisson process at --rate
+    requests/s, through the continuous-batching server (isdf_server_*).
+    Latency is arrival -> completion as the client sees it (it includes any
+    wait for a free output buffer); throughput is requests / (last completion
+    - first arrival). psi comes from a small pool per shape (seeds 100, 101,
+    ...), the request index picking the seed; every in-flight request has its
+    own theta and piv."""
+    import threading
+
+    import torch
+
+    import libisdf_b200 as isdf
+    from libisdf_b200 import synth
+
+    torch.cuda.set_device(0)
+    shapes = [synth.SI8, synth.SI64, synth.SI216]
+    pool_seeds = [4, 2, 1]
+    theta_bufs = [8, 4, 1]
+    rng = np.random.default_rng(args.serve_seed)
+    n_req = args.requests
+    kinds = rng.choice(3, size=n_req, p=[0.6, 0.3, 0.1])
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, size=n_req))
+    prec = isdf.PRECISION_MIXED if args.precision == "mixed" else isdf.PRECISION_FP64
+    opts = isdf.Options(precision=prec)
+    psi = {k: [torch.from_numpy(np.ascontiguousarray(
+        synth.shape_orbitals(shapes[k], 100 + j, device="cuda").T)).cuda()
+        for j in range(pool_seeds[k])] for k in range(3)}
+    free = {k: [torch.empty((shapes[k].mu, shapes[k].ng), dtype=torch.float64, device="cuda")
+                for _ in range(theta_bufs[k])] for k in range(3)}
+    doms = [isdf.Domain(length=(sh.length,) * 3, num_grid=(sh.n,) * 3) for sh in shapes]
+    torch.cuda.synchronize()
+
+    srv = isdf.Server(slots=args.slots)
+    lock = threading.Condition()
+    inflight = {}  # ticket -> (kind, theta, arrival index)
+    done_at = np.zeros(n_req)
+
+    def submit(k, i, theta):
+        sh = shapes[k]
+        piv = np.zeros(sh.ng, dtype=np.int32)
+        return srv.submit(psi[k][i % pool_seeds[k]], doms[k], sh.nocc, sh.nstate, sh.nv1, sh.nc1,
+                          sh.nv2, sh.nc2, sh.mu, theta, piv, sh.kmeans_iters, options=opts)
+
+    # warm-up: one request of each shape (workspaces, graphs)
+    for k in range(3):
+        st, _ = srv.wait(submit(k, 0, free[k][0]))
+        assert st == 0, isdf.lib().isdf_last_error()
+
+    stop = threading.Event()
+
+    def poller():
+        while not stop.is_set() or inflight:
+            with lock:
+                items = list(inflight.items())
+            finished = []
+            for t, (k, th, i) in items:
+                state, st = srv.poll(t)
+                if state == 2:
+                    done_at[i] = time.perf_counter()
+                    finished.append((t, k, th, st))
+            if finished:
+                with lock:
+                    for t, k, th, st in finished:
+                        srv.wait(t)
+                        del inflight[t]
+                        free[k].append(th)
+                        if st != 0:
+                            inflight_errors.append(t)
+                    lock.notify_all()
+            time.sleep(0.0005)
+
+    inflight_errors = []
+    th_poll = threading.Thread(target=poller, daemon=True)
+    th_poll.start()
+    t0 = time.perf_counter()
+    arr_at = t0 + arrivals
+    with ClockSampler(0) as clk:
+        for i in range(n_req):
+            k = int(kinds[i])
+            dt = arr_at[i] - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            with lock:
+                while not free[k]:
+                    lock.wait()
+                theta = free[k].pop()
+                t = submit(k, i, theta)
+                inflight[t] = (k, theta, i)
+        stop.set()
+        th_poll.join()
+    stats = srv.stats()
+    srv.close()
+    lat = (done_at - arr_at) * 1e3
+    span = done_at.max() - arr_at[0]
+    line = {"metric": "served ISDF solves/s (serving mix)", "value": n_req / span,
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic", "precision": args.precision,
+            "config": {"workload": "serving mix: 60 % Si8-like, 30 % Si64-like, 10 % Si216-like, "
+                                   "K-means", "requests": n_req, "rate_per_s": args.rate,
+                       "slots": args.slots, "psi_pool_seeds": pool_seeds,
+                       "theta_buffers": theta_bufs,
+                       "mix_counts": [int((kinds == k).sum()) for k in range(3)]},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                           "p99": float(np.percentile(lat, 99)),
+                           "p50_by_shape": {shapes[k].name: float(np.percentile(lat[kinds == k], 50))
+                                            for k in range(3) if (kinds == k).any()}},
+            "errors": len(inflight_errors),
+            "server": {k: stats[k] for k in stats if k in ("completed", "peak_concurrency",
+                                                              "p50_ms", "p99_ms", "peak_bytes")},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -380,12 +580,20 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--stage", choices=["solve", "select"], default="solve",
                     help="select: time the K-means selection alone (profiling aid)")
+    ap.add_argument("--serve", action="store_true",
+                    help="the serving mix through isdf_server_* (Poisson arrivals)")
+    ap.add_argument("--requests", type=int, default=128)
+    ap.add_argument("--rate", type=float, default=4.0, help="arrivals per second (--serve)")
+    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--serve-seed", type=int, default=7)
     args = ap.parse_args()
     from libisdf_b200 import synth
 
     shape = synth.SHAPES[args.config]
     if args.impl == "reference":
         run_reference(args, shape)
+    elif args.serve:
+        run_serve(args)
     elif args.stage == "select":
         run_select(args, shape)
     else:

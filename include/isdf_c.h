@@ -64,7 +64,7 @@ typedef struct isdf_options_t {
   long long rand_seed;    /* >= 0: srand() before K-means (only its npt < mu branch
                              draws from rand()); < 0: keep the process state */
   void* stream;           /* cudaStream_t to run on; NULL = library stream */
-  int mixed_slices;       /* mixed precision: INT8 slices per FP64 operand, 5..7 (default 7) */
+  int mixed_slices;       /* mixed precision: base-254 INT8 digits per FP64 operand, 5..7 (default 6) */
   int reserved[7];
 } isdf_options_t;
 
@@ -84,7 +84,8 @@ typedef struct isdf_report_t {
   double t_total_ms;
   int chol_info;       /* > 0: leading minor that failed */
   int kernel_launches; /* kernels this library launched for the solve */
-  int reserved[6];
+  float t_gemm_ms;     /* GEMM launches of the triangular stage alone (FP64: the whole stage) */
+  int reserved[5];
 } isdf_report_t;
 
 /* Fills *opt with the reference's defaults. */

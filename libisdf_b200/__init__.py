@@ -71,7 +71,8 @@ class _Report(ctypes.Structure):
                 ("t_zct_ms", ctypes.c_double), ("t_chol_ms", ctypes.c_double),
                 ("t_solve_ms", ctypes.c_double), ("t_check_ms", ctypes.c_double),
                 ("t_total_ms", ctypes.c_double), ("chol_info", ctypes.c_int),
-                ("kernel_launches", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+                ("kernel_launches", ctypes.c_int), ("t_gemm_ms", ctypes.c_float),
+                ("reserved", ctypes.c_int * 5)]
 
 
 class _ServerConfig(ctypes.Structure):
@@ -129,7 +130,7 @@ class Options:
     qrcp_seed: int = 41
     rand_seed: int = -1
     stream: int = 0
-    mixed_slices: int = 7
+    mixed_slices: int = 6
 
     def _c(self) -> _Options:
         o = _Options()
@@ -160,6 +161,7 @@ class Report:
     t_total_ms: float
     chol_info: int
     kernel_launches: int
+    t_gemm_ms: float = 0.0
 
 
 _lib = None
@@ -239,7 +241,7 @@ def ISDF(d_psirow, domain: Domain, nocc: int, nstate: int, nv1: int, nc1: int, n
     _check(rc)
     return Report(r.rk_requested, r.rk_eff, r.kmeans_iters, r.npt, r.fit_err, r.coul_err,
                   r.t_select_ms, r.t_fit_ms, r.t_zct_ms, r.t_chol_ms, r.t_solve_ms, r.t_check_ms,
-                  r.t_total_ms, r.chol_info, r.kernel_launches)
+                  r.t_total_ms, r.chol_info, r.kernel_launches, r.t_gemm_ms)
 
 
 def kmeans_weight(d_psi, ng: int, nstate: int, nocc: int, nv1: int, nc1: int, nv2: int, nc2: int,
@@ -291,7 +293,7 @@ def check(domain: Domain, d_psi, nocc: int, nstate: int, nv1: int, nc1: int, nv2
 def _report(r: _Report) -> Report:
     return Report(r.rk_requested, r.rk_eff, r.kmeans_iters, r.npt, r.fit_err, r.coul_err,
                   r.t_select_ms, r.t_fit_ms, r.t_zct_ms, r.t_chol_ms, r.t_solve_ms, r.t_check_ms,
-                  r.t_total_ms, r.chol_info, r.kernel_launches)
+                  r.t_total_ms, r.chol_info, r.kernel_launches, r.t_gemm_ms)
 
 
 class Server:

@@ -278,6 +278,7 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
   rep.t_zct_ms = fr.t_zct_ms;
   rep.t_chol_ms = fr.t_chol_ms;
   rep.t_solve_ms = fr.t_solve_ms;
+  rep.t_gemm_ms = fr.t_gemm_ms > 0.f ? fr.t_gemm_ms : fr.t_solve_ms;
   if (rc != ISDF_OK) {
     if (rep_out) *rep_out = rep;
     return rc;
@@ -329,7 +330,7 @@ void isdf_default_options(isdf_options_t* opt) {
   opt->qrcp_seed = 41;
   opt->rand_seed = -1;
   opt->stream = nullptr;
-  opt->mixed_slices = 7;
+  opt->mixed_slices = kDefaultMixedSlices;
 }
 
 int isdf_solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, int nv1,
@@ -403,7 +404,7 @@ int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, i
     Arena arena;
     cudaStream_t ls;
     const size_t need = precision == ISDF_PRECISION_MIXED
-                            ? fit_mixed_workspace_bytes(ng, nstate, rk, 7)
+                            ? fit_mixed_workspace_bytes(ng, nstate, rk, kDefaultMixedSlices)
                             : fit_workspace_bytes(ng, nstate, rk);
     ISDF_TRY(acquire_workspace(need + 4096, &arena, &ls));
     FitArgs fa;
@@ -420,7 +421,7 @@ int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, i
     fa.d_theta = d_theta;
     FitResult fr;
     cudaStream_t s = stream ? (cudaStream_t)stream : ls;
-    int rc = precision == ISDF_PRECISION_MIXED ? fit_mixed(fa, arena, s, &fr, 7)
+    int rc = precision == ISDF_PRECISION_MIXED ? fit_mixed(fa, arena, s, &fr, kDefaultMixedSlices)
                                                : fit_fp64(fa, arena, s, &fr);
     if (chol_info) *chol_info = fr.chol_info;
     if (rc == ISDF_OK) ISDF_CUDA(cudaStreamSynchronize(s));

@@ -374,7 +374,7 @@ static int cholesky(const FitBuffers& b, int rk, cudaStream_t s) {
 
 // Stage timers: CUDA events on the solve stream.
 struct StageEvents {
-  cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t e[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   ~StageEvents() {
     for (auto& x : e)
       if (x) cudaEventDestroy(x);
@@ -478,7 +478,8 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
 // theta = Y L^{-1}) as INT8-sliced GEMMs on the tcgen05 tensor cores
 // (ozaki.cuh); C C^T, the Cholesky factorisation and L^{-T} stay FP64.
 // theta = (Z C^T L^{-T}) L^{-1} with explicit triangular inverses, whose
-// rounding is that of two FP64 TRMMs when S >= 7 slices.
+// truncation (2^-47 of the operand scales at S = 6) stays below the
+// conditioning of the fit.
 
 namespace {
 
@@ -486,8 +487,10 @@ constexpr int kSliceTile = 64;  // rows per slicing tile
 constexpr int kSliceK = 32;     // K bytes per slicing tile
 
 // Row-scaled slicing of an M x K FP64 operand, element (m, k) at
-// X[m*rs + k*ks], into S planes P[t*plane + m*ldk + k] of int8 (rows padded to
-// mp, columns to kp, zeros there) and exponents e[m] (|x| 2^-e < 1/2).
+// X[m*rs + k*ks], into S int8 slices written in the pre-tiled layout of the
+// Ozaki GEMM (ozaki::tiled_offset: blocks of R rows, 32-byte K blocks; the A
+// side unstacked with R = 128, the B side stacked with R = 64), rows padded to
+// mp and K to kp with zeros, and exponents e[m] (|x| 2^-e < 1/2).
 __global__ void k_row_exponent(const double* __restrict__ X, long long rs, long long ks, int M,
                                int K, int* __restrict__ e) {
   for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x) {
@@ -497,11 +500,17 @@ __global__ void k_row_exponent(const double* __restrict__ X, long long rs, long 
   }
 }
 
-template <int S>
+// Row exponents from the binade maxima the GEMM epilogue gathered: the same
+// e as k_row_exponent computes from the stored values.
+__global__ void k_exp_from_max(int* __restrict__ e, int M) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < M; m += gridDim.x * blockDim.x)
+    e[m] = e[m] == ozaki::kNoExponent ? 0 : e[m] + 2;
+}
+
+template <int S, int R, bool STACKED>
 __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ X, long long rs,
                                                long long ks, int M, int K, int mp, int kp,
-                                               const int* __restrict__ e, int8_t* __restrict__ P,
-                                               long long plane, int ldk) {
+                                               const int* __restrict__ e, int8_t* __restrict__ P) {
   __shared__ double xs[kSliceTile][kSliceK + 1];
   __shared__ __align__(16) int8_t qs[S][kSliceTile][kSliceK];
   const int m0 = blockIdx.y * kSliceTile, k0 = blockIdx.x * kSliceK;
@@ -519,7 +528,7 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ X, lon
     double r = (m < M) ? ldexp(xs[mi][ki], -e[m]) : 0.0;
 #pragma unroll
     for (int t = 0; t < S; ++t) {
-      r *= 128.0;
+      r *= ozaki::kBase;
       const double q = rint(r);
       r -= q;
       qs[t][mi][ki] = (int8_t)q;
@@ -532,7 +541,9 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ X, lon
     const int mi = rem / 2, c = rem % 2;
     const int m = m0 + mi;
     if (m < mp && k0 + c * 16 < kp)
-      *reinterpret_cast<int4*>(P + t * plane + (long long)m * ldk + k0 + c * 16) =
+      *reinterpret_cast<int4*>(P + ozaki::tiled_offset<S, R, STACKED>(m / R, k0 / ozaki::BKB,
+                                                                     kp / ozaki::BKB, t, c,
+                                                                     m % R)) =
           *reinterpret_cast<const int4*>(&qs[t][mi][c * 16]);
   }
 }
@@ -547,11 +558,10 @@ __global__ void k_identity(double* __restrict__ X, int n) {
 inline int round_up(long long x, int a) { return (int)((x + a - 1) / a * a); }
 
 struct MixedBuffers {
-  int8_t *PA, *PB;
+  int8_t *PA, *PB;  // pre-tiled slices of the A (grid rows) and B operands
   int *ea, *eb, *err;
+  int *ez, *ey;     // row exponents of Z C^T and Y, gathered by the GEMM epilogues
   double* MT;  // L^{-T}, column-major rk x rk
-  long long pa_plane, pb_plane;
-  int ldk;
 };
 
 MixedBuffers carve_mixed(Arena& a, long long ng, int nstate, int rk, int slices) {
@@ -559,31 +569,35 @@ MixedBuffers carve_mixed(Arena& a, long long ng, int nstate, int rk, int slices)
   const int kmax = round_up(nstate > rk ? nstate : rk, ozaki::BKB);
   const long long mp = round_up(ng, ozaki::BM);
   const int np = round_up(rk, 128);
-  b.ldk = kmax;
-  b.pa_plane = mp * kmax;
-  b.pb_plane = (long long)np * kmax;
-  b.PA = a.take<int8_t>((size_t)slices * b.pa_plane);
-  b.PB = a.take<int8_t>((size_t)slices * b.pb_plane);
+  b.PA = a.take<int8_t>((size_t)slices * mp * kmax);
+  b.PB = a.take<int8_t>((size_t)slices * np * kmax);
   b.ea = a.take<int>((size_t)mp);
+  b.ez = a.take<int>((size_t)mp);
+  b.ey = a.take<int>((size_t)mp);
   b.eb = a.take<int>((size_t)np);
   b.err = a.take<int>(1);
   b.MT = a.take<double>((size_t)rk * rk);
   return b;
 }
 
-template <int S>
+// A side: R = 128 row blocks; B side: the stacked 64-column blocks.
+// gathered = true: e holds the binade maxima from the producing GEMM's
+// epilogue, and the pass over X that k_row_exponent makes is saved.
+template <int S, bool B_SIDE>
 int slice_operand(const double* X, long long rs, long long ks, int M, int K, int mp, int kp,
-                  int* e, int8_t* P, long long plane, int ldk, cudaStream_t s) {
-  k_row_exponent<<<grid_for(M, 256), 256, 0, s>>>(X, rs, ks, M, K, e);
+                  int* e, int8_t* P, cudaStream_t s, bool gathered = false) {
+  if (gathered) k_exp_from_max<<<grid_for(M, 256), 256, 0, s>>>(e, M);
+  else k_row_exponent<<<grid_for(M, 256), 256, 0, s>>>(X, rs, ks, M, K, e);
   dim3 g((unsigned)(kp / kSliceK), (unsigned)((mp + kSliceTile - 1) / kSliceTile));
-  k_slice<S><<<g, 256, 0, s>>>(X, rs, ks, M, K, mp, kp, e, P, plane, ldk);
+  if (B_SIDE) k_slice<S, ozaki::BN, true><<<g, 256, 0, s>>>(X, rs, ks, M, K, mp, kp, e, P);
+  else k_slice<S, ozaki::BM, false><<<g, 256, 0, s>>>(X, rs, ks, M, K, mp, kp, e, P);
   ISDF_CHECK_LAUNCH();
   return ISDF_OK;
 }
 
 template <int S, int EPI, int KMODE>
-int ozaki_gemm(const MixedBuffers& b, int M, int N, int kp, double* C, long long ldc,
-               cudaStream_t s) {
+int ozaki_gemm(const MixedBuffers& b, const int* ea, int M, int N, int kp, double* C,
+               long long ldc, int* rowmax, cudaStream_t s) {
   auto kern = ozaki::k_ozaki_gemm<S, EPI, KMODE>;
   static bool attr[64] = {};
   int dev = 0;
@@ -594,9 +608,19 @@ int ozaki_gemm(const MixedBuffers& b, int M, int N, int kp, double* C, long long
                                    ozaki::Cfg<S>::SMEM));
     attr[dev] = true;
   }
-  dim3 g((unsigned)((N + ozaki::BN - 1) / ozaki::BN), (unsigned)((M + ozaki::BM - 1) / ozaki::BM));
-  kern<<<g, 128, ozaki::Cfg<S>::SMEM, s>>>(b.PA, b.pa_plane, b.ldk, b.PB, b.pb_plane, b.ldk,
-                                           b.ea, b.eb, M, N, kp, C, ldc, b.err);
+  if (kp > ozaki::kMaxK)
+    return record_error(ISDF_ERR_UNSUPPORTED, "mixed fit: K beyond the INT32-exact limit (16384)");
+  const long long tiles =
+      (long long)((N + ozaki::BN - 1) / ozaki::BN) * ((M + ozaki::BM - 1) / ozaki::BM);
+  if (tiles > 0x7fffffffLL) return record_error(ISDF_ERR_UNSUPPORTED, "mixed fit: too many tiles");
+  static int sms[64] = {};
+  if (dev >= 0 && dev < 64 && !sms[dev])
+    ISDF_CUDA(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
+  const int nsm = (dev >= 0 && dev < 64 && sms[dev] > 0) ? sms[dev] : kNumSMs;
+  const unsigned grid = (unsigned)(tiles < nsm ? tiles : nsm);  // persistent: one CTA per SM
+  if (rowmax) ISDF_CUDA(cudaMemsetAsync(rowmax, 0x80, sizeof(int) * (size_t)M, s));
+  kern<<<grid, ozaki::kThreads, ozaki::Cfg<S>::SMEM, s>>>(b.PA, b.PB, ea, b.eb, M, N, kp, C, ldc,
+                                                          rowmax, b.err);
   ISDF_CHECK_LAUNCH();
   return ISDF_OK;
 }
@@ -625,13 +649,16 @@ int fit_mixed_s(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* re
     const int lo = f == 0 ? args.nocc - args.nv1 : args.nocc - args.nv2;
     const int K = f == 0 ? args.nv1 + args.nc1 : args.nv2 + args.nc2;
     const int kp = round_up(K, ozaki::BKB);
-    ISDF_TRY(slice_operand<S>(args.d_psi + (long long)lo * ng, 1, ng, (int)ng, K, mp, kp, mb.ea,
-                              mb.PA, mb.pa_plane, mb.ldk, s));
-    ISDF_TRY(slice_operand<S>(b.Bm + (size_t)lo * rk, 1, rk, rk, K, np, kp, mb.eb, mb.PB,
-                              mb.pb_plane, mb.ldk, s));
-    if (same) ISDF_TRY((ozaki_gemm<S, 1, 0>(mb, (int)ng, rk, kp, args.d_theta, ng, s)));
-    else if (f == 0) ISDF_TRY((ozaki_gemm<S, 0, 0>(mb, (int)ng, rk, kp, args.d_theta, ng, s)));
-    else ISDF_TRY((ozaki_gemm<S, 2, 0>(mb, (int)ng, rk, kp, args.d_theta, ng, s)));
+    ISDF_TRY((slice_operand<S, false>(args.d_psi + (long long)lo * ng, 1, ng, (int)ng, K, mp, kp,
+                                      mb.ea, mb.PA, s)));
+    ISDF_TRY((slice_operand<S, true>(b.Bm + (size_t)lo * rk, 1, rk, rk, K, np, kp, mb.eb, mb.PB,
+                                     s)));
+    if (same)
+      ISDF_TRY((ozaki_gemm<S, 1, 0>(mb, mb.ea, (int)ng, rk, kp, args.d_theta, ng, mb.ez, s)));
+    else if (f == 0)
+      ISDF_TRY((ozaki_gemm<S, 0, 0>(mb, mb.ea, (int)ng, rk, kp, args.d_theta, ng, nullptr, s)));
+    else
+      ISDF_TRY((ozaki_gemm<S, 2, 0>(mb, mb.ea, (int)ng, rk, kp, args.d_theta, ng, mb.ez, s)));
   }
   ISDF_CUDA(cudaEventRecord(ev.e[1], s));
 
@@ -678,14 +705,18 @@ int fit_mixed_s(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* re
 
   // Y = Z L^{-T} (L^{-T} upper), then theta = Y L^{-1} (L^{-1} lower), in place in theta
   const int kp = round_up(rk, ozaki::BKB);
-  ISDF_TRY(slice_operand<S>(args.d_theta, 1, ng, (int)ng, rk, mp, kp, mb.ea, mb.PA, mb.pa_plane,
-                            mb.ldk, s));
-  ISDF_TRY(slice_operand<S>(mb.MT, rk, 1, rk, rk, np, kp, mb.eb, mb.PB, mb.pb_plane, mb.ldk, s));
-  ISDF_TRY((ozaki_gemm<S, 0, 1>(mb, (int)ng, rk, kp, args.d_theta, ng, s)));
-  ISDF_TRY(slice_operand<S>(args.d_theta, 1, ng, (int)ng, rk, mp, kp, mb.ea, mb.PA, mb.pa_plane,
-                            mb.ldk, s));
-  ISDF_TRY(slice_operand<S>(mb.MT, 1, rk, rk, rk, np, kp, mb.eb, mb.PB, mb.pb_plane, mb.ldk, s));
-  ISDF_TRY((ozaki_gemm<S, 0, 2>(mb, (int)ng, rk, kp, args.d_theta, ng, s)));
+  ISDF_TRY((slice_operand<S, false>(args.d_theta, 1, ng, (int)ng, rk, mp, kp, mb.ez, mb.PA, s,
+                                    true)));
+  ISDF_TRY((slice_operand<S, true>(mb.MT, rk, 1, rk, rk, np, kp, mb.eb, mb.PB, s)));
+  ISDF_CUDA(cudaEventRecord(ev.e[4], s));
+  ISDF_TRY((ozaki_gemm<S, 0, 1>(mb, mb.ez, (int)ng, rk, kp, args.d_theta, ng, mb.ey, s)));
+  ISDF_CUDA(cudaEventRecord(ev.e[5], s));
+  ISDF_TRY((slice_operand<S, false>(args.d_theta, 1, ng, (int)ng, rk, mp, kp, mb.ey, mb.PA, s,
+                                    true)));
+  ISDF_TRY((slice_operand<S, true>(mb.MT, 1, rk, rk, rk, np, kp, mb.eb, mb.PB, s)));
+  ISDF_CUDA(cudaEventRecord(ev.e[6], s));
+  ISDF_TRY((ozaki_gemm<S, 0, 2>(mb, mb.ey, (int)ng, rk, kp, args.d_theta, ng, nullptr, s)));
+  ISDF_CUDA(cudaEventRecord(ev.e[7], s));
   ISDF_CUDA(cudaEventRecord(ev.e[3], s));
   int err = 0;
   ISDF_CUDA(cudaMemcpyAsync(&err, mb.err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -695,6 +726,10 @@ int fit_mixed_s(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* re
   ISDF_CUDA(cudaEventElapsedTime(&res->t_zct_ms, ev.e[0], ev.e[1]));
   ISDF_CUDA(cudaEventElapsedTime(&res->t_chol_ms, ev.e[1], ev.e[2]));
   ISDF_CUDA(cudaEventElapsedTime(&res->t_solve_ms, ev.e[2], ev.e[3]));
+  float g1 = 0.f, g2 = 0.f;
+  ISDF_CUDA(cudaEventElapsedTime(&g1, ev.e[4], ev.e[5]));
+  ISDF_CUDA(cudaEventElapsedTime(&g2, ev.e[6], ev.e[7]));
+  res->t_gemm_ms = g1 + g2;
   const int nblk = (rk + kNB - 1) / kNB;
   res->launches = 1 + (same ? 3 : 6) * 2 + 2 + (nblk + 2 * (nblk - 1) + 1) + 1 + 2 * nblk + 10;
   return ISDF_OK;

@@ -21,6 +21,7 @@ struct FitResult {
   int chol_info = 0;
   int launches = 0;
   float t_zct_ms = 0, t_chol_ms = 0, t_solve_ms = 0;  // CUDA-event stage times
+  float t_gemm_ms = 0;  // the triangular stage's GEMM launches alone (0: not timed apart)
 };
 
 size_t fit_workspace_bytes(long long ng, int nstate, int rk);

@@ -11,6 +11,9 @@
 
 namespace isdf_b200 {
 
+// Base-254 INT8 digits per FP64 operand in the mixed-precision GEMMs.
+constexpr int kDefaultMixedSlices = 6;
+
 int iround(double a);
 int default_mu(int nv1, int nc1, int nv2, int nc2);
 size_t solve_workspace_bytes(long long ng, int nstate, int mu, int selector, int precision,
