@@ -46,8 +46,9 @@ struct KmState {
   int rk;       // current number of centroids
   int npt;      // kept points
   int any_empty;
-  int pad;
+  int reset_bounds;  // centroid indices moved (empty-cluster compaction): bounds invalid
   unsigned long long maxw_bits;
+  unsigned long long maxshift_bits;  // largest centroid move of this iteration (bit pattern)
 };
 
 // ---------------------------------------------------------------- weight
@@ -215,6 +216,29 @@ struct CellGrid {
   double tol;
 };
 
+// Thread -> point map of the assignment. When every grid point is kept
+// (npt = Ng, point p = grid point p), each warp takes a 4 x 4 x 2 brick of
+// grid points instead of 32 points along x, so that its lanes search nearly
+// the same cells; otherwise thread t takes point t. Either way every point
+// is assigned once and the result does not depend on the map.
+struct AssignMap {
+  int brick;  // 0: linear
+  int nx, ny, nz;
+  int nbx, nby;  // bricks along x and y
+};
+
+__device__ __forceinline__ int assign_point(long long t, const AssignMap& am) {
+  if (!am.brick) return (int)t;
+  const long long b = t >> 5;
+  const int l = (int)(t & 31);
+  const int bx = (int)(b % am.nbx);
+  const long long r = b / am.nbx;
+  const int by = (int)(r % am.nby), bz = (int)(r / am.nby);
+  const int ix = bx * 4 + (l & 3), iy = by * 4 + ((l >> 2) & 3), iz = bz * 2 + (l >> 4);
+  if (ix >= am.nx || iy >= am.ny || iz >= am.nz) return -1;
+  return ix + am.nx * (iy + am.ny * iz);
+}
+
 // One block: cell of each centroid, counting sort into cell order.
 __global__ void __launch_bounds__(1024) k_build_cells(const double4* __restrict__ cen,
                                                       const KmState* st, CellGrid g,
@@ -251,67 +275,116 @@ __global__ void __launch_bounds__(1024) k_build_cells(const double4* __restrict_
   }
 }
 
+// Squared distance in the reference's rounding (pdist2, utility.cpp:598-615).
+__device__ __forceinline__ double ref_dist2(double x, double y, double z, const double4& c) {
+  const double d1 = rsub(x, c.x), d2 = rsub(y, c.y), d3 = rsub(z, c.z);
+  return radd(radd(rmul(d1, d1), rmul(d2, d2)), rmul(d3, d3));
+}
+
+// Distance bounds (Hamerly): bnd[p] = (u, l), u >= the true distance from p
+// to its assigned centroid, l <= the true distance to every other centroid.
+// Moving centroids move them by at most shift[label] and the largest shift.
+// When u (1 + 1e-12) < l, the assigned centroid is strictly nearest with a
+// margin far above the relative error of the rounded squared distances
+// (~1e-15), so the reference's argmin (first minimum of the rounded
+// distances) is the assigned label and the search is skipped. Otherwise the
+// exact ring search runs and the bounds are rebuilt from it: u from the
+// best distance, l from the second best seen, the box bounds of skipped
+// cells and the ring at which the search stopped.
+constexpr double kBoundMargin = 1.0 + 1e-12;
+constexpr double kRoundUp = 1.0 + 1e-13;
+constexpr double kRoundDown = 1.0 - 1e-13;
+
 __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
     const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
     int n, const double4* __restrict__ cen, const int* __restrict__ cell_start,
-    const double4* __restrict__ cell_cen, CellGrid g, KmState* st, int* __restrict__ label,
-    int count) {
+    const double4* __restrict__ cell_cen, CellGrid g, AssignMap am, KmState* st,
+    int* __restrict__ label, int count, double2* __restrict__ bnd,
+    const double* __restrict__ shift) {
   if (st->done) return;
   const int rk = st->rk;
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = assign_point((long long)blockIdx.x * blockDim.x + threadIdx.x, am);
   int changed = 0;
-  if (p < n) {
+  if (p >= 0 && p < n) {
     const double x = px[p], y = py[p], z = pz[p];
-    double best = __longlong_as_double(0x7ff0000000000000LL);
+    const double inf = __longlong_as_double(0x7ff0000000000000LL);
+    double best = inf;
     int bj = 0x7fffffff;
     const int old = count ? label[p] : -1;
+    bool settled = false;
     if (old >= 0 && old < rk) {  // seed with the previous centroid (any centroid is a valid start)
-      const double4 c = cen[old];
-      double d1 = rsub(x, c.x), d2 = rsub(y, c.y), d3 = rsub(z, c.z);
-      best = radd(radd(rmul(d1, d1), rmul(d2, d2)), rmul(d3, d3));
+      best = ref_dist2(x, y, z, cen[old]);
       bj = old;
-    }
-    const int pi = min(g.nc - 1, max(0, (int)floor(x / g.h[0])));
-    const int pj = min(g.nc - 1, max(0, (int)floor(y / g.h[1])));
-    const int pk = min(g.nc - 1, max(0, (int)floor(z / g.h[2])));
-    const double hmin = fmin(g.h[0], fmin(g.h[1], g.h[2]));
-    const double shrink = 1.0 - 2e-14;
-    for (int r = 0; r <= g.nc; ++r) {
-      if (r >= 2) {
-        const double lb = (r - 1) * hmin - g.tol;
-        if (lb > 0.0 && lb * lb * shrink > best) break;
+      if (count && !st->reset_bounds) {
+        const double2 b = bnd[p];
+        const double lo = fmax(0.0, __dsub_rd(b.y, __longlong_as_double(
+                                                     (long long)st->maxshift_bits)));
+        double up = __dadd_ru(b.x, shift[old]);
+        if (!(up * kBoundMargin < lo)) up = __dmul_ru(__dsqrt_ru(best), kRoundUp);
+        if (up * kBoundMargin < lo) {
+          bnd[p] = make_double2(up, lo);
+          settled = true;
+        }
       }
-      for (int dk = -r; dk <= r; ++dk) {
-        const int ck = pk + dk;
-        if (ck < 0 || ck >= g.nc) continue;
-        for (int dj = -r; dj <= r; ++dj) {
-          const int cj = pj + dj;
-          if (cj < 0 || cj >= g.nc) continue;
-          for (int di = -r; di <= r; ++di) {
-            if (max(abs(di), max(abs(dj), abs(dk))) != r) continue;
-            const int ci = pi + di;
-            if (ci < 0 || ci >= g.nc) continue;
-            // box lower bound (box widened by tol)
-            const double bx = fmax(0.0, fmax(ci * g.h[0] - g.tol - x, x - (ci + 1) * g.h[0] - g.tol));
-            const double by = fmax(0.0, fmax(cj * g.h[1] - g.tol - y, y - (cj + 1) * g.h[1] - g.tol));
-            const double bz = fmax(0.0, fmax(ck * g.h[2] - g.tol - z, z - (ck + 1) * g.h[2] - g.tol));
-            const double lb = bx * bx + by * by + bz * bz;
-            if (lb * shrink > best) continue;
-            const int id = ci + g.nc * (cj + g.nc * ck);
-            const int e = cell_start[id + 1];
-            for (int q = cell_start[id]; q < e; ++q) {
-              const double4 c = cell_cen[q];
-              double d1 = rsub(x, c.x), d2 = rsub(y, c.y), d3 = rsub(z, c.z);
-              double d = radd(radd(rmul(d1, d1), rmul(d2, d2)), rmul(d3, d3));
-              const int j = (int)c.w;
-              if (d < best || (d == best && j < bj)) {
-                best = d;
-                bj = j;
+    }
+    if (!settled) {
+      double second = inf;  // second-best squared distance seen
+      double floor2 = inf;  // lower bound (squared) on every centroid not seen
+      const int pi = min(g.nc - 1, max(0, (int)floor(x / g.h[0])));
+      const int pj = min(g.nc - 1, max(0, (int)floor(y / g.h[1])));
+      const int pk = min(g.nc - 1, max(0, (int)floor(z / g.h[2])));
+      const double hmin = fmin(g.h[0], fmin(g.h[1], g.h[2]));
+      const double shrink = 1.0 - 2e-14;
+      for (int r = 0; r <= g.nc; ++r) {
+        if (r >= 2) {
+          const double lb = (r - 1) * hmin - g.tol;
+          if (lb > 0.0 && lb * lb * shrink > best) {
+            floor2 = fmin(floor2, lb * lb * shrink);
+            break;
+          }
+        }
+        for (int dk = -r; dk <= r; ++dk) {
+          const int ck = pk + dk;
+          if (ck < 0 || ck >= g.nc) continue;
+          for (int dj = -r; dj <= r; ++dj) {
+            const int cj = pj + dj;
+            if (cj < 0 || cj >= g.nc) continue;
+            for (int di = -r; di <= r; ++di) {
+              if (max(abs(di), max(abs(dj), abs(dk))) != r) continue;
+              const int ci = pi + di;
+              if (ci < 0 || ci >= g.nc) continue;
+              // box lower bound (box widened by tol)
+              const double bx =
+                  fmax(0.0, fmax(ci * g.h[0] - g.tol - x, x - (ci + 1) * g.h[0] - g.tol));
+              const double by =
+                  fmax(0.0, fmax(cj * g.h[1] - g.tol - y, y - (cj + 1) * g.h[1] - g.tol));
+              const double bz =
+                  fmax(0.0, fmax(ck * g.h[2] - g.tol - z, z - (ck + 1) * g.h[2] - g.tol));
+              const double lb = bx * bx + by * by + bz * bz;
+              if (lb * shrink > best) {
+                floor2 = fmin(floor2, lb * shrink);
+                continue;
+              }
+              const int id = ci + g.nc * (cj + g.nc * ck);
+              const int e = cell_start[id + 1];
+              for (int q = cell_start[id]; q < e; ++q) {
+                const double4 c = cell_cen[q];
+                const double d = ref_dist2(x, y, z, c);
+                const int j = (int)c.w;
+                if (d < best || (d == best && j < bj)) {
+                  if (j != bj) second = best;
+                  best = d;
+                  bj = j;
+                } else if (j != bj) {
+                  second = fmin(second, d);
+                }
               }
             }
           }
         }
       }
+      bnd[p] = make_double2(__dmul_ru(__dsqrt_ru(best), kRoundUp),
+                            __dmul_rd(__dsqrt_rd(fmin(second, floor2)), kRoundDown));
     }
     if (count && old != bj) ++changed;
     label[p] = bj;
@@ -331,6 +404,8 @@ __global__ void k_iter_begin(KmState* st, double max_f, int max_iter) {
   }
   st->changed = 0;
   st->any_empty = 0;
+  st->reset_bounds = 0;
+  st->maxshift_bits = 0;
 }
 
 __global__ void k_iter_end(KmState* st) {
@@ -365,11 +440,19 @@ __global__ void __launch_bounds__(256) k_hist_scan(int* __restrict__ hist, int n
   const int rk = st->rk;
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= rk) return;
+  // loads batched ahead of the stores (in place: the compiler cannot reorder
+  // a load past an earlier store to the same array on its own)
+  constexpr int kB = 16;
   int run = 0;
-  for (int t = 0; t < ntiles; ++t) {
-    int v = hist[(size_t)t * rk + l];
-    hist[(size_t)t * rk + l] = run;
-    run += v;
+  for (int t0 = 0; t0 < ntiles; t0 += kB) {
+    int v[kB];
+#pragma unroll
+    for (int u = 0; u < kB; ++u) v[u] = t0 + u < ntiles ? hist[(size_t)(t0 + u) * rk + l] : 0;
+#pragma unroll
+    for (int u = 0; u < kB; ++u) {
+      if (t0 + u < ntiles) hist[(size_t)(t0 + u) * rk + l] = run;
+      run += v[u];
+    }
   }
   members[l] = run;
 }
@@ -425,18 +508,33 @@ __global__ void __launch_bounds__(128) k_scatter(const int* __restrict__ label, 
   __syncthreads();
   if (threadIdx.x >= 32) return;
   const int lane = threadIdx.x;
+  // the point values of the next 32 are loaded while this 32 is placed
+  double nw = 0.0, nx = 0.0, ny = 0.0, nz = 0.0;
+  if (lane < cnt) {
+    const int p = base + lane;
+    nw = pw[p];
+    nx = px[p];
+    ny = py[p];
+    nz = pz[p];
+  }
   for (int c = 0; c < cnt; c += 32) {
     const int k = c + lane;
     const bool ok = k < cnt;
+    const double w = nw, x = nx, y = ny, z = nz;
+    if (k + 32 < cnt) {
+      const int p = base + k + 32;
+      nw = pw[p];
+      nx = px[p];
+      ny = py[p];
+      nz = pz[p];
+    }
     const int l = ok ? lab[k] : -1;
     const unsigned peers = __match_any_sync(0xffffffffu, l);
     const int b = ok ? run[l] : 0;
     __syncwarp();
     if (ok) {
       const int r = __popc(peers & ((1u << lane) - 1u));
-      const int p = base + k;
-      const double w = pw[p];
-      sorted[b + r] = make_double4(rmul(w, px[p]), rmul(w, py[p]), rmul(w, pz[p]), w);
+      sorted[b + r] = make_double4(rmul(w, x), rmul(w, y), rmul(w, z), w);
       if (lane == __ffs(peers) - 1) run[l] = b + __popc(peers);
     }
     __syncwarp();
@@ -524,34 +622,37 @@ __global__ void __launch_bounds__(256) k_segsum(const double4* __restrict__ sort
     tail = n - npt;
     m -= (int)tail;
   }
-  double aw = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
+  // lanes 0..3 each fold one component (w x, w y, w z, w) from the warp's
+  // shared-memory copy of the batch: one load and one dependent addition per
+  // member instead of four broadcasts and four additions
+  __shared__ double4 stage[8][32 * kSegBatches];
+  double4* st_w = stage[threadIdx.x >> 5];
+  double acc = 0.0;
   double4 cur[kSegBatches], nxt[kSegBatches];
   seg_load(v, 0, m, lane, cur);
   for (int q = 0; q < m; q += 32 * kSegBatches) {
+#pragma unroll
+    for (int j = 0; j < kSegBatches; ++j) st_w[j * 32 + lane] = cur[j];
+    __syncwarp();
     if (q + 32 * kSegBatches < m) seg_load(v, q + 32 * kSegBatches, m, lane, nxt);
+    const int cnt = min(32 * kSegBatches, m - q);
+    if (lane < 4) {
+      const double* comp = reinterpret_cast<const double*>(st_w) + lane;
+      int e = 0;
+      for (; e + 8 <= cnt; e += 8) {
 #pragma unroll
-    for (int j = 0; j < kSegBatches; ++j) {
-      const int cnt = min(32, m - (q + 32 * j));  // warp-uniform
-      if (cnt == 32) {
-#pragma unroll
-        for (int k = 0; k < 32; ++k) {
-          aw = radd(aw, __shfl_sync(0xffffffffu, cur[j].w, k));
-          ax = radd(ax, __shfl_sync(0xffffffffu, cur[j].x, k));
-          ay = radd(ay, __shfl_sync(0xffffffffu, cur[j].y, k));
-          az = radd(az, __shfl_sync(0xffffffffu, cur[j].z, k));
-        }
-      } else {
-        for (int k = 0; k < cnt; ++k) {
-          aw = radd(aw, __shfl_sync(0xffffffffu, cur[j].w, k));
-          ax = radd(ax, __shfl_sync(0xffffffffu, cur[j].x, k));
-          ay = radd(ay, __shfl_sync(0xffffffffu, cur[j].y, k));
-          az = radd(az, __shfl_sync(0xffffffffu, cur[j].z, k));
-        }
+        for (int u = 0; u < 8; ++u) acc = radd(acc, comp[(e + u) * 4]);
       }
+      for (; e < cnt; ++e) acc = radd(acc, comp[e * 4]);
     }
+    __syncwarp();
 #pragma unroll
     for (int j = 0; j < kSegBatches; ++j) cur[j] = nxt[j];
   }
+  double ax = __shfl_sync(0xffffffffu, acc, 0);
+  double ay = __shfl_sync(0xffffffffu, acc, 1);
+  double az = __shfl_sync(0xffffffffu, acc, 2);
+  double aw = __shfl_sync(0xffffffffu, acc, 3);
   if (lane == 0) {
     if (tail) {
       const double w0 = pw[npt];
@@ -568,17 +669,27 @@ __global__ void __launch_bounds__(256) k_segsum(const double4* __restrict__ sort
 // New centroids = sums / count; an empty cluster takes the last centroid's
 // sums and rk shrinks (utility.cpp:831-853).
 __global__ void __launch_bounds__(1024) k_centroids(double4* __restrict__ sums, KmState* st,
-                                                    double4* __restrict__ cen) {
+                                                    double4* __restrict__ cen,
+                                                    double* __restrict__ shift) {
   if (st->done) return;
   int rk = st->rk;
   if (!st->any_empty) {
     for (int i = threadIdx.x; i < rk; i += blockDim.x) {
       double4 s = sums[i];
-      cen[i] = make_double4(rdiv(s.x, s.w), rdiv(s.y, s.w), rdiv(s.z, s.w), 0.0);
+      const double4 o = cen[i];
+      const double4 c = make_double4(rdiv(s.x, s.w), rdiv(s.y, s.w), rdiv(s.z, s.w), 0.0);
+      cen[i] = c;
+      // upper bound on the distance the centroid moved (rounded upward)
+      const double dx = fabs(c.x - o.x), dy = fabs(c.y - o.y), dz = fabs(c.z - o.z);
+      const double d2 = __dadd_ru(__dadd_ru(__dmul_ru(dx, dx), __dmul_ru(dy, dy)), __dmul_ru(dz, dz));
+      const double sh = __dmul_ru(__dsqrt_ru(d2), 1.0 + 1e-13);
+      shift[i] = sh;
+      atomicMax(&st->maxshift_bits, (unsigned long long)__double_as_longlong(sh));
     }
     return;
   }
   if (threadIdx.x != 0) return;
+  st->reset_bounds = 1;
   for (int i = 0; i < rk; i++) {
     double4 s = sums[i];
     if (s.w != 0.0) {
@@ -690,6 +801,8 @@ struct KmBuffers {
   int* tile_cnt;
   double4* cen;
   double4* sums;
+  double2* bnd;    // per point (upper, lower) distance bounds
+  double* shift;   // per centroid: distance moved in the last update
   double* part_d;
   int* part_i;
   int* sel;
@@ -717,6 +830,8 @@ KmBuffers carve(Arena& a, int n, int mu) {
   b.tile_cnt = a.take<int>(nfilter);
   b.cen = a.take<double4>(mu);
   b.sums = a.take<double4>(mu);
+  b.bnd = a.take<double2>(n);
+  b.shift = a.take<double>(mu);
   b.part_d = a.take<double>((size_t)nchunks * mu);
   b.part_i = a.take<int>((size_t)nchunks * mu);
   b.sel = a.take<int>(mu);
@@ -834,11 +949,21 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     cg.tol = 1e-9 * lmax;
   }
   const size_t cell_smem = sizeof(int) * ((size_t)cg.nc * cg.nc * cg.nc + 1);
-  const unsigned pgrid = grid_for(n, kAssignThreads);
+  AssignMap am{};
+  am.nx = args.num_grid[0];
+  am.ny = args.num_grid[1];
+  am.nz = args.num_grid[2];
+  am.nbx = (am.nx + 3) / 4;
+  am.nby = (am.ny + 3) / 4;
+  const long long nbricks = (long long)am.nbx * am.nby * ((am.nz + 1) / 2);
+  am.brick = (npt == n && (long long)am.nx * am.ny * am.nz == n && nbricks * 32 < 0x7fffffffLL);
+  const unsigned pgrid = am.brick ? grid_for(nbricks * 32, kAssignThreads)
+                                  : grid_for(n, kAssignThreads);
   k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
                                                 b.cell_of);
   k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.cell_start,
-                                                      b.cell_cen, cg, b.st, b.label, 0);
+                                                      b.cell_cen, cg, am, b.st, b.label, 0,
+                                                      b.bnd, b.shift);
   ISDF_CHECK_LAUNCH();
 
   const double max_f = 1e-5 * n;  // KmeansTolerance * n (utility.cpp:812)
@@ -862,12 +987,12 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
                                                        b.py, b.pz, b.pw, b.sorted);
       k_segsum<<<grid_for(mu, 8), 256, 0, stream>>>(b.sorted, b.start, b.members, b.px, b.py,
                                                     b.pz, b.pw, b.label, n, b.st, b.sums);
-      k_centroids<<<1, 1024, 0, stream>>>(b.sums, b.st, b.cen);
+      k_centroids<<<1, 1024, 0, stream>>>(b.sums, b.st, b.cen, b.shift);
       k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
                                                     b.cell_of);
       k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen,
-                                                          b.cell_start, b.cell_cen, cg, b.st,
-                                                          b.label, 1);
+                                                          b.cell_start, b.cell_cen, cg, am, b.st,
+                                                          b.label, 1, b.bnd, b.shift);
       k_iter_end<<<1, 1, 0, stream>>>(b.st);
     }
   };
