@@ -268,11 +268,13 @@ def run_ours(args, shape):
     dom = isdf.Domain(length=(shape.length,) * 3, num_grid=(shape.n,) * 3)
     stream = torch.cuda.Stream()
     prec = isdf.PRECISION_MIXED if args.precision == "mixed" else isdf.PRECISION_FP64
-    opts = isdf.Options(stream=stream.cuda_stream, precision=prec)
+    opts = isdf.Options(stream=stream.cuda_stream, precision=prec,
+                        qrcp_oversample=args.qrcp_factor, qrcp_seed=args.qrcp_seed)
+    s1 = "QRCP" if args.selector == "qrcp" else "Kmeans"
 
     def solve():
         return isdf.ISDF(d_psi, dom, shape.nocc, shape.nstate, shape.nv1, shape.nc1, shape.nv2,
-                         shape.nc2, mu, d_theta, piv, shape.kmeans_iters, options=opts)
+                         shape.nc2, mu, d_theta, piv, shape.kmeans_iters, s1=s1, options=opts)
 
     fp64_peak = _fp64_peak_tflops(torch)
     int8_peak = _int8_peak_tops(torch) if args.precision == "mixed" else None
@@ -330,12 +332,13 @@ def run_ours(args, shape):
         return
     accuracy = None
     if args.precision == "mixed":
-        opts64 = isdf.Options(stream=stream.cuda_stream, precision=isdf.PRECISION_FP64)
+        opts64 = isdf.Options(stream=stream.cuda_stream, precision=isdf.PRECISION_FP64,
+                              qrcp_oversample=args.qrcp_factor, qrcp_seed=args.qrcp_seed)
 
         def solve_fp64():
             with torch.cuda.stream(stream):
                 isdf.ISDF(d_psi, dom, shape.nocc, shape.nstate, shape.nv1, shape.nc1, shape.nv2,
-                          shape.nc2, mu, d_theta, piv, shape.kmeans_iters, options=opts64)
+                          shape.nc2, mu, d_theta, piv, shape.kmeans_iters, s1=s1, options=opts64)
             torch.cuda.synchronize()
 
         accuracy = mixed_vs_fp64(torch, shape, psi, d_theta, piv, rep.rk_eff, solve_fp64)
@@ -388,7 +391,10 @@ def run_ours(args, shape):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": shape.name, "ng": ng, "nstate": shape.nstate, "mu": mu,
-                   "rk_eff": rk, "kmeans_iters": rep.kmeans_iters, "selector": "Kmeans",
+                   "rk_eff": rk, "kmeans_iters": rep.kmeans_iters, "npt": rep.npt,
+                   "kmeans_search_frac": round(float(rep.kmeans_search_frac), 4), "selector": s1,
+                   **({"qrcp_oversample": args.qrcp_factor, "qrcp_seed": args.qrcp_seed}
+                      if s1 == "QRCP" else {}),
                    "precision": args.precision, "parallelism": f"replicas x{world}",
                    "l2": (f"inputs larger than L2 (psi {ng * shape.nstate * 8 / 1e9:.2f} GB, "
                           f"theta {ng * mu * 8 / 1e9:.2f} GB; L2 126 MB)")},
@@ -407,7 +413,11 @@ def run_ours(args, shape):
         "mixed_vs_fp64": accuracy,
         "clocks": clk.summary(),
     }
-    if world == 1 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline and s1 == "QRCP":
+        line["cpu_baseline"] = {"value": None, "unit": "solves/s",
+                                "unavailable": "the reference's QRCP selector runs ScaLAPACK "
+                                               "pdgeqpf, which cannot be built here"}
+    elif world == 1 and not args.no_cpu_baseline:
         try:
             t_cpu, info = reference_sample(shape, rep.kmeans_iters)
             line["cpu_baseline"] = dict(info, value=1.0 / t_cpu, unit="solves/s")
@@ -578,6 +588,10 @@ def main():
     ap.add_argument("--config", choices=["si8", "si64", "si216", "si64c"], default="si64")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--selector", choices=["kmeans", "qrcp"], default="kmeans")
+    ap.add_argument("--qrcp-factor", type=float, default=1.5,
+                    help="QRCP oversampling (numPre = round(sqrt(f mu)); the reference uses 1.5)")
+    ap.add_argument("--qrcp-seed", type=int, default=41)
     ap.add_argument("--stage", choices=["solve", "select"], default="solve",
                     help="select: time the K-means selection alone (profiling aid)")
     ap.add_argument("--serve", action="store_true",

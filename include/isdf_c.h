@@ -85,7 +85,8 @@ typedef struct isdf_report_t {
   int chol_info;       /* > 0: leading minor that failed */
   int kernel_launches; /* kernels this library launched for the solve */
   float t_gemm_ms;     /* GEMM launches of the triangular stage alone (FP64: the whole stage) */
-  int reserved[5];
+  float kmeans_search_frac; /* share of K-means point assignments that ran the cell search */
+  int reserved[4];
 } isdf_report_t;
 
 /* Fills *opt with the reference's defaults. */

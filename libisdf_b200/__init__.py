@@ -72,7 +72,7 @@ class _Report(ctypes.Structure):
                 ("t_solve_ms", ctypes.c_double), ("t_check_ms", ctypes.c_double),
                 ("t_total_ms", ctypes.c_double), ("chol_info", ctypes.c_int),
                 ("kernel_launches", ctypes.c_int), ("t_gemm_ms", ctypes.c_float),
-                ("reserved", ctypes.c_int * 5)]
+                ("kmeans_search_frac", ctypes.c_float), ("reserved", ctypes.c_int * 4)]
 
 
 class _ServerConfig(ctypes.Structure):
@@ -162,6 +162,7 @@ class Report:
     chol_info: int
     kernel_launches: int
     t_gemm_ms: float = 0.0
+    kmeans_search_frac: float = 0.0
 
 
 _lib = None
@@ -241,7 +242,8 @@ def ISDF(d_psirow, domain: Domain, nocc: int, nstate: int, nv1: int, nc1: int, n
     _check(rc)
     return Report(r.rk_requested, r.rk_eff, r.kmeans_iters, r.npt, r.fit_err, r.coul_err,
                   r.t_select_ms, r.t_fit_ms, r.t_zct_ms, r.t_chol_ms, r.t_solve_ms, r.t_check_ms,
-                  r.t_total_ms, r.chol_info, r.kernel_launches, r.t_gemm_ms)
+                  r.t_total_ms, r.chol_info, r.kernel_launches, r.t_gemm_ms,
+                  r.kmeans_search_frac)
 
 
 def kmeans_weight(d_psi, ng: int, nstate: int, nocc: int, nv1: int, nc1: int, nv2: int, nc2: int,
@@ -293,7 +295,8 @@ def check(domain: Domain, d_psi, nocc: int, nstate: int, nv1: int, nc1: int, nv2
 def _report(r: _Report) -> Report:
     return Report(r.rk_requested, r.rk_eff, r.kmeans_iters, r.npt, r.fit_err, r.coul_err,
                   r.t_select_ms, r.t_fit_ms, r.t_zct_ms, r.t_chol_ms, r.t_solve_ms, r.t_check_ms,
-                  r.t_total_ms, r.chol_info, r.kernel_launches, r.t_gemm_ms)
+                  r.t_total_ms, r.chol_info, r.kernel_launches, r.t_gemm_ms,
+                  r.kmeans_search_frac)
 
 
 class Server:

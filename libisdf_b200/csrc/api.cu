@@ -225,6 +225,7 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
     rep.rk_eff = kr.rk_eff;
     rep.kmeans_iters = kr.iters;
     rep.npt = kr.npt;
+    rep.kmeans_search_frac = (float)kr.search_frac;
     rep.kernel_launches = 1 + kr.launches;
     rk_fit = kr.rk_eff;
   } else {

@@ -265,6 +265,71 @@ __global__ void __launch_bounds__(256) k_trsm_gemm(double* theta, long long ng, 
   });
 }
 
+// ---- L^{-1} by blocked doubling (the mixed form's triangular factors).
+// X = L^{-1} is kept twice: Xr row-major (X(i, j) = Xr[i*n + j], which is
+// L^{-T} column-major) and Xc column-major. Level s joins the inverted
+// diagonal blocks A = [a0, a0+s) and D = [a0+s, a0+2s) pairwise:
+//   X(D, A) = -X(D, D) (L(D, A) X(A, A)),
+// two FP64 tensor-core GEMMs per pair (K ranges cut to the triangles), all
+// pairs of a level in one launch; the 64 x 64 diagonal-block inverses of the
+// Cholesky factorisation are level 0.
+__global__ void k_trinv_init(const double* __restrict__ dinv, int n, double* __restrict__ Xr,
+                             double* __restrict__ Xc) {
+  const int c0 = blockIdx.x * kNB, bs = min(kNB, n - c0);
+  const double* d = dinv + (size_t)blockIdx.x * kNB * kNB;
+  for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+    const int k = e / kNB, j = e % kNB;
+    if (k < bs && j < bs) {
+      const double v = d[e];  // X(c0 + k, c0 + j)
+      Xr[(long long)(c0 + k) * n + (c0 + j)] = v;
+      Xc[(c0 + k) + (long long)(c0 + j) * n] = v;
+    }
+  }
+}
+
+// T(r, c) = sum_{k >= c} L(d0 + r, a0 + k) X(a0 + k, a0 + c), into Tb at X(D, A)'s place.
+template <int VEC>
+__global__ void __launch_bounds__(256) k_trinv_t(const double* __restrict__ L,
+                                                 const double* __restrict__ Xr,
+                                                 double* __restrict__ Tb, int n, int s) {
+  extern __shared__ double smem[];
+  const int a0 = blockIdx.z * 2 * s, d0 = a0 + s;
+  if (d0 >= n) return;
+  const int a = s, d = min(s, n - d0);
+  const int c0 = blockIdx.x * CoreN::BN, r0 = blockIdx.y * CoreN::BM;
+  if (c0 >= a || r0 >= d) return;
+  CoreN core;
+  core.zero();
+  core.run<VEC>(smem, L + (d0 + r0) + (long long)a0 * n, n, Xr + (long long)a0 * n + (a0 + c0), n,
+                d - r0, a - c0, c0, a);
+  core.for_each([&](int r, int c, double v) {
+    if (r0 + r < d && c0 + c < a) Tb[(long long)(d0 + r0 + r) * n + (a0 + c0 + c)] = v;
+  });
+}
+
+// X(d0 + r, a0 + c) = -sum_{k <= r} X(d0 + r, d0 + k) T(k, c).
+template <int VEC>
+__global__ void __launch_bounds__(256) k_trinv_x(const double* __restrict__ Tb,
+                                                 double* __restrict__ Xr, double* Xc, int n,
+                                                 int s) {
+  extern __shared__ double smem[];
+  const int a0 = blockIdx.z * 2 * s, d0 = a0 + s;
+  if (d0 >= n) return;
+  const int a = s, d = min(s, n - d0);
+  const int c0 = blockIdx.x * CoreN::BN, r0 = blockIdx.y * CoreN::BM;
+  if (c0 >= a || r0 >= d) return;
+  CoreN core;
+  core.zero();
+  core.run<VEC>(smem, Xc + (d0 + r0) + (long long)d0 * n, n, Tb + (long long)d0 * n + (a0 + c0), n,
+                d - r0, a - c0, 0, min(d, r0 + CoreN::BM));
+  core.for_each([&](int r, int c, double v) {
+    if (r0 + r < d && c0 + c < a) {
+      Xr[(long long)(d0 + r0 + r) * n + (a0 + c0 + c)] = -v;
+      Xc[(d0 + r0 + r) + (long long)(a0 + c0 + c) * n] = -v;
+    }
+  });
+}
+
 constexpr size_t smem_bytes_potf2 = sizeof(double) * 2 * kNB * (kNB + 1);
 
 template <class K>
@@ -292,6 +357,10 @@ int set_smem_attrs() {
   ISDF_TRY(set_attr(k_chol_panel<2>, CoreN::SMEM_BYTES));
   ISDF_TRY(set_attr(k_trsm_gemm<1>, CoreN::SMEM_BYTES));
   ISDF_TRY(set_attr(k_trsm_gemm<2>, CoreN::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_trinv_t<1>, CoreN::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_trinv_t<2>, CoreN::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_trinv_x<1>, CoreN::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_trinv_x<2>, CoreN::SMEM_BYTES));
   if (dev >= 0 && dev < 64) done_dev[dev] = true;
   return ISDF_OK;
 }
@@ -548,12 +617,6 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ X, lon
   }
 }
 
-__global__ void k_identity(double* __restrict__ X, int n) {
-  const long long total = (long long)n * n;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x)
-    X[e] = (e % n) == (e / n) ? 1.0 : 0.0;
-}
 
 inline int round_up(long long x, int a) { return (int)((x + a - 1) / a * a); }
 
@@ -561,7 +624,8 @@ struct MixedBuffers {
   int8_t *PA, *PB;  // pre-tiled slices of the A (grid rows) and B operands
   int *ea, *eb, *err;
   int *ez, *ey;     // row exponents of Z C^T and Y, gathered by the GEMM epilogues
-  double* MT;  // L^{-T}, column-major rk x rk
+  double* MT;  // L^{-T}, column-major rk x rk (= L^{-1} row-major)
+  double *XC, *TB;  // L^{-1} column-major, and the doubling's scratch
 };
 
 MixedBuffers carve_mixed(Arena& a, long long ng, int nstate, int rk, int slices) {
@@ -577,6 +641,8 @@ MixedBuffers carve_mixed(Arena& a, long long ng, int nstate, int rk, int slices)
   b.eb = a.take<int>((size_t)np);
   b.err = a.take<int>(1);
   b.MT = a.take<double>((size_t)rk * rk);
+  b.XC = a.take<double>((size_t)rk * rk);
+  b.TB = a.take<double>((size_t)rk * rk);
   return b;
 }
 
@@ -687,19 +753,25 @@ int fit_mixed_s(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* re
   ISDF_CUDA(cudaStreamSynchronize(s));
   res->chol_info = info;
   if (info != 0) return record_error(ISDF_ERR_NOT_SPD, "fit: C C^T + eps I is not positive definite");
-  // L^{-T}: the forward sweep X L^T = I on an rk x rk identity
-  k_identity<<<grid_for((long long)rk * rk, 256), 256, 0, s>>>(mb.MT, rk);
+  // L^{-T} (= L^{-1} row-major) by blocked doubling from the diagonal-block inverses
   {
     const int nblk = (rk + kNB - 1) / kNB;
-    const bool v2 = vec2_ok(mb.MT, rk, b.W, kNB);
-    const unsigned tg = (unsigned)((rk + CoreN::BM - 1) / CoreN::BM);
-    for (int kb = 0; kb < nblk; ++kb) {
-      const int c0 = kb * kNB, bs = min(kNB, rk - c0);
-      k_build_w<true><<<(c0 + bs + 3) / 4 < 1024 ? (c0 + bs + 3) / 4 : 1024, 256, 0, s>>>(
-          b.P, rk, c0, bs, b.dinvT + (size_t)kb * kNB * kNB, b.W);
-      if (v2) k_trsm_gemm<2><<<tg, 256, CoreN::SMEM_BYTES, s>>>(mb.MT, rk, c0, bs, 0, c0 + bs, b.W);
-      else k_trsm_gemm<1><<<tg, 256, CoreN::SMEM_BYTES, s>>>(mb.MT, rk, c0, bs, 0, c0 + bs, b.W);
+    ISDF_CUDA(cudaMemsetAsync(mb.MT, 0, sizeof(double) * (size_t)rk * rk, s));
+    ISDF_CUDA(cudaMemsetAsync(mb.XC, 0, sizeof(double) * (size_t)rk * rk, s));
+    k_trinv_init<<<nblk, 256, 0, s>>>(b.dinv, rk, mb.MT, mb.XC);
+    const bool v2 = vec2_ok(mb.MT, rk, mb.TB, rk);
+    for (int lv = kNB; lv < rk; lv *= 2) {
+      dim3 g((unsigned)((lv + CoreN::BN - 1) / CoreN::BN), (unsigned)((lv + CoreN::BM - 1) / CoreN::BM),
+             (unsigned)((rk + 2 * lv - 1) / (2 * lv)));
+      if (v2) {
+        k_trinv_t<2><<<g, 256, CoreN::SMEM_BYTES, s>>>(b.P, mb.MT, mb.TB, rk, lv);
+        k_trinv_x<2><<<g, 256, CoreN::SMEM_BYTES, s>>>(mb.TB, mb.MT, mb.XC, rk, lv);
+      } else {
+        k_trinv_t<1><<<g, 256, CoreN::SMEM_BYTES, s>>>(b.P, mb.MT, mb.TB, rk, lv);
+        k_trinv_x<1><<<g, 256, CoreN::SMEM_BYTES, s>>>(mb.TB, mb.MT, mb.XC, rk, lv);
+      }
     }
+    ISDF_CHECK_LAUNCH();
   }
   ISDF_CUDA(cudaEventRecord(ev.e[2], s));
 
@@ -731,7 +803,9 @@ int fit_mixed_s(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* re
   ISDF_CUDA(cudaEventElapsedTime(&g2, ev.e[6], ev.e[7]));
   res->t_gemm_ms = g1 + g2;
   const int nblk = (rk + kNB - 1) / kNB;
-  res->launches = 1 + (same ? 3 : 6) * 2 + 2 + (nblk + 2 * (nblk - 1) + 1) + 1 + 2 * nblk + 10;
+  int levels = 0;
+  for (int lv = kNB; lv < rk; lv *= 2) ++levels;
+  res->launches = 1 + (same ? 3 : 6) * 2 + 2 + (nblk + 2 * (nblk - 1) + 1) + 1 + 2 * levels + 10;
   return ISDF_OK;
 }
 

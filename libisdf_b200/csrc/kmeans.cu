@@ -49,6 +49,7 @@ struct KmState {
   int reset_bounds;  // centroid indices moved (empty-cluster compaction): bounds invalid
   unsigned long long maxw_bits;
   unsigned long long maxshift_bits;  // largest centroid move of this iteration (bit pattern)
+  unsigned long long searches;       // assignments that ran the cell search (all iterations)
 };
 
 // ---------------------------------------------------------------- weight
@@ -216,19 +217,28 @@ struct CellGrid {
   double tol;
 };
 
-// Thread -> point map of the assignment. When every grid point is kept
-// (npt = Ng, point p = grid point p), each warp takes a 4 x 4 x 2 brick of
-// grid points instead of 32 points along x, so that its lanes search nearly
-// the same cells; otherwise thread t takes point t. Either way every point
-// is assigned once and the result does not depend on the map.
+// Thread -> point map of the assignment. Brick mode: each warp takes a
+// 4 x 4 x 2 brick of grid points instead of 32 points along the kept-point
+// list, so that its lanes search nearly the same cells; a grid point that
+// the weight filter dropped leaves its lane idle (g2p[g] = -1), and the
+// zero-tail points p >= npt (copies of grid point 0) follow the bricks one
+// per thread. Linear mode: thread t takes point t. Either way every point is
+// assigned once and the result does not depend on the map.
 struct AssignMap {
   int brick;  // 0: linear
   int nx, ny, nz;
-  int nbx, nby;  // bricks along x and y
+  int nbx, nby;    // bricks along x and y
+  long long nbt;   // brick threads: bricks x 32
+  int npt, n;
+  const int* g2p;  // grid index -> kept-point index (or -1); nullptr: identity
 };
 
 __device__ __forceinline__ int assign_point(long long t, const AssignMap& am) {
   if (!am.brick) return (int)t;
+  if (t >= am.nbt) {
+    const long long p = am.npt + (t - am.nbt);
+    return p < am.n ? (int)p : -1;
+  }
   const long long b = t >> 5;
   const int l = (int)(t & 31);
   const int bx = (int)(b % am.nbx);
@@ -236,7 +246,14 @@ __device__ __forceinline__ int assign_point(long long t, const AssignMap& am) {
   const int by = (int)(r % am.nby), bz = (int)(r / am.nby);
   const int ix = bx * 4 + (l & 3), iy = by * 4 + ((l >> 2) & 3), iz = bz * 2 + (l >> 4);
   if (ix >= am.nx || iy >= am.ny || iz >= am.nz) return -1;
-  return ix + am.nx * (iy + am.ny * iz);
+  const int g = ix + am.nx * (iy + am.ny * iz);
+  return am.g2p ? am.g2p[g] : g;
+}
+
+// Inverse of the kept-point list: g2p[pidx[p]] = p for p < npt (the rest -1).
+__global__ void k_grid_to_point(const int* __restrict__ pidx, int npt, int* __restrict__ g2p) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npt; p += gridDim.x * blockDim.x)
+    g2p[pidx[p]] = p;
 }
 
 // One block: cell of each centroid, counting sort into cell order.
@@ -300,11 +317,11 @@ __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
     int n, const double4* __restrict__ cen, const int* __restrict__ cell_start,
     const double4* __restrict__ cell_cen, CellGrid g, AssignMap am, KmState* st,
     int* __restrict__ label, int count, double2* __restrict__ bnd,
-    const double* __restrict__ shift) {
+    const double* __restrict__ shift, const float* __restrict__ nbshift) {
   if (st->done) return;
   const int rk = st->rk;
   const int p = assign_point((long long)blockIdx.x * blockDim.x + threadIdx.x, am);
-  int changed = 0;
+  int changed = 0, searched = 0;
   if (p >= 0 && p < n) {
     const double x = px[p], y = py[p], z = pz[p];
     const double inf = __longlong_as_double(0x7ff0000000000000LL);
@@ -312,13 +329,31 @@ __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
     int bj = 0x7fffffff;
     const int old = count ? label[p] : -1;
     bool settled = false;
+    const int pi = min(g.nc - 1, max(0, (int)floor(x / g.h[0])));
+    const int pj = min(g.nc - 1, max(0, (int)floor(y / g.h[1])));
+    const int pk = min(g.nc - 1, max(0, (int)floor(z / g.h[2])));
     if (old >= 0 && old < rk) {  // seed with the previous centroid (any centroid is a valid start)
       best = ref_dist2(x, y, z, cen[old]);
       bj = old;
       if (count && !st->reset_bounds) {
         const double2 b = bnd[p];
-        const double lo = fmax(0.0, __dsub_rd(b.y, __longlong_as_double(
-                                                     (long long)st->maxshift_bits)));
+        // Every other centroid moved closer by at most its shift. Those that
+        // sat in the 27 cells around p moved at most nbshift; the others were
+        // at least D away (D: distance from p to the outside of those cells,
+        // no bound across the domain's faces), so when D - (largest shift)
+        // stays above the lowered bound they cannot undercut it either.
+        const double gmax = __longlong_as_double((long long)st->maxshift_bits);
+        const double near = (double)nbshift[pi + g.nc * (pj + g.nc * pk)];
+        double D = inf;
+        if (pi >= 2) D = fmin(D, x - (pi - 1) * g.h[0]);
+        if (pi + 2 <= g.nc - 1) D = fmin(D, (pi + 2) * g.h[0] - x);
+        if (pj >= 2) D = fmin(D, y - (pj - 1) * g.h[1]);
+        if (pj + 2 <= g.nc - 1) D = fmin(D, (pj + 2) * g.h[1] - y);
+        if (pk >= 2) D = fmin(D, z - (pk - 1) * g.h[2]);
+        if (pk + 2 <= g.nc - 1) D = fmin(D, (pk + 2) * g.h[2] - z);
+        D = D * kRoundDown - g.tol;
+        double lo = fmax(0.0, __dsub_rd(b.y, near));
+        if (!(D - gmax >= lo)) lo = fmax(0.0, __dsub_rd(b.y, gmax));
         double up = __dadd_ru(b.x, shift[old]);
         if (!(up * kBoundMargin < lo)) up = __dmul_ru(__dsqrt_ru(best), kRoundUp);
         if (up * kBoundMargin < lo) {
@@ -330,9 +365,6 @@ __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
     if (!settled) {
       double second = inf;  // second-best squared distance seen
       double floor2 = inf;  // lower bound (squared) on every centroid not seen
-      const int pi = min(g.nc - 1, max(0, (int)floor(x / g.h[0])));
-      const int pj = min(g.nc - 1, max(0, (int)floor(y / g.h[1])));
-      const int pk = min(g.nc - 1, max(0, (int)floor(z / g.h[2])));
       const double hmin = fmin(g.h[0], fmin(g.h[1], g.h[2]));
       const double shrink = 1.0 - 2e-14;
       for (int r = 0; r <= g.nc; ++r) {
@@ -388,10 +420,15 @@ __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
     }
     if (count && old != bj) ++changed;
     label[p] = bj;
+    searched = settled ? 0 : 1;
   }
-  if (count) {
-    for (int o = 16; o > 0; o >>= 1) changed += __shfl_xor_sync(0xffffffffu, changed, o);
-    if ((threadIdx.x & 31) == 0 && changed) atomicAdd(&st->changed, changed);
+  for (int o = 16; o > 0; o >>= 1) {
+    changed += __shfl_xor_sync(0xffffffffu, changed, o);
+    searched += __shfl_xor_sync(0xffffffffu, searched, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (count && changed) atomicAdd(&st->changed, changed);
+    if (searched) atomicAdd(&st->searches, (unsigned long long)searched);
   }
 }
 
@@ -668,12 +705,22 @@ __global__ void __launch_bounds__(256) k_segsum(const double4* __restrict__ sort
 
 // New centroids = sums / count; an empty cluster takes the last centroid's
 // sums and rk shrinks (utility.cpp:831-853).
+// The update also records how far every centroid moved (rounded upward), the
+// largest move, and for every cell of the grid the largest move of a centroid
+// that sat in its 3 x 3 x 3 neighbourhood before the update (cell_of still
+// holds the previous positions' cells here).
 __global__ void __launch_bounds__(1024) k_centroids(double4* __restrict__ sums, KmState* st,
                                                     double4* __restrict__ cen,
-                                                    double* __restrict__ shift) {
+                                                    double* __restrict__ shift,
+                                                    const int* __restrict__ cell_of, CellGrid g,
+                                                    float* __restrict__ nbshift) {
   if (st->done) return;
   int rk = st->rk;
   if (!st->any_empty) {
+    __shared__ unsigned cmax[kMaxCells];
+    const int nc = g.nc, ncells = nc * nc * nc;
+    for (int c = threadIdx.x; c < ncells; c += blockDim.x) cmax[c] = 0u;
+    __syncthreads();
     for (int i = threadIdx.x; i < rk; i += blockDim.x) {
       double4 s = sums[i];
       const double4 o = cen[i];
@@ -685,6 +732,17 @@ __global__ void __launch_bounds__(1024) k_centroids(double4* __restrict__ sums, 
       const double sh = __dmul_ru(__dsqrt_ru(d2), 1.0 + 1e-13);
       shift[i] = sh;
       atomicMax(&st->maxshift_bits, (unsigned long long)__double_as_longlong(sh));
+      atomicMax(&cmax[cell_of[i]], __float_as_uint(__double2float_ru(sh)));
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < ncells; c += blockDim.x) {
+      const int ci = c % nc, cj = (c / nc) % nc, ck = c / (nc * nc);
+      unsigned m = 0u;
+      for (int dk = max(0, ck - 1); dk <= min(nc - 1, ck + 1); ++dk)
+        for (int dj = max(0, cj - 1); dj <= min(nc - 1, cj + 1); ++dj)
+          for (int di = max(0, ci - 1); di <= min(nc - 1, ci + 1); ++di)
+            m = max(m, cmax[di + nc * (dj + nc * dk)]);
+      nbshift[c] = __uint_as_float(m);
     }
     return;
   }
@@ -803,6 +861,8 @@ struct KmBuffers {
   double4* sums;
   double2* bnd;    // per point (upper, lower) distance bounds
   double* shift;   // per centroid: distance moved in the last update
+  int* g2p;        // grid index -> kept-point index
+  float* nbshift;  // per cell: largest move of a centroid in its 27-cell neighbourhood
   double* part_d;
   int* part_i;
   int* sel;
@@ -832,6 +892,8 @@ KmBuffers carve(Arena& a, int n, int mu) {
   b.sums = a.take<double4>(mu);
   b.bnd = a.take<double2>(n);
   b.shift = a.take<double>(mu);
+  b.g2p = a.take<int>(n);
+  b.nbshift = a.take<float>((size_t)kMaxCells);
   b.part_d = a.take<double>((size_t)nchunks * mu);
   b.part_i = a.take<int>((size_t)nchunks * mu);
   b.sel = a.take<int>(mu);
@@ -955,15 +1017,23 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
   am.nz = args.num_grid[2];
   am.nbx = (am.nx + 3) / 4;
   am.nby = (am.ny + 3) / 4;
-  const long long nbricks = (long long)am.nbx * am.nby * ((am.nz + 1) / 2);
-  am.brick = (npt == n && (long long)am.nx * am.ny * am.nz == n && nbricks * 32 < 0x7fffffffLL);
-  const unsigned pgrid = am.brick ? grid_for(nbricks * 32, kAssignThreads)
+  am.nbt = (long long)am.nbx * am.nby * ((am.nz + 1) / 2) * 32;
+  am.npt = npt;
+  am.n = n;
+  am.brick = ((long long)am.nx * am.ny * am.nz == n && am.nbt + n < 0x7fffffffLL);
+  am.g2p = nullptr;
+  if (am.brick && npt < n) {
+    ISDF_CUDA(cudaMemsetAsync(b.g2p, 0xff, sizeof(int) * (size_t)n, stream));
+    k_grid_to_point<<<grid_for(npt, 256), 256, 0, stream>>>(b.pidx, npt, b.g2p);
+    am.g2p = b.g2p;
+  }
+  const unsigned pgrid = am.brick ? grid_for(am.nbt + (n - npt), kAssignThreads)
                                   : grid_for(n, kAssignThreads);
   k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
                                                 b.cell_of);
   k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.cell_start,
                                                       b.cell_cen, cg, am, b.st, b.label, 0,
-                                                      b.bnd, b.shift);
+                                                      b.bnd, b.shift, b.nbshift);
   ISDF_CHECK_LAUNCH();
 
   const double max_f = 1e-5 * n;  // KmeansTolerance * n (utility.cpp:812)
@@ -987,12 +1057,13 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
                                                        b.py, b.pz, b.pw, b.sorted);
       k_segsum<<<grid_for(mu, 8), 256, 0, stream>>>(b.sorted, b.start, b.members, b.px, b.py,
                                                     b.pz, b.pw, b.label, n, b.st, b.sums);
-      k_centroids<<<1, 1024, 0, stream>>>(b.sums, b.st, b.cen, b.shift);
+      k_centroids<<<1, 1024, 0, stream>>>(b.sums, b.st, b.cen, b.shift, b.cell_of, cg,
+                                          b.nbshift);
       k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
                                                     b.cell_of);
       k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen,
                                                           b.cell_start, b.cell_cen, cg, am, b.st,
-                                                          b.label, 1, b.bnd, b.shift);
+                                                          b.label, 1, b.bnd, b.shift, b.nbshift);
       k_iter_end<<<1, 1, 0, stream>>>(b.st);
     }
   };
@@ -1024,6 +1095,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     if (++chunks > max_chunks) return record_error(ISDF_ERR_CUDA, "kmeans: loop did not stop");
   }
   res->iters = hst.s;
+  res->search_frac = (double)hst.searches / ((double)n * (hst.s + 1));
   res->launches = 4 + 3 + (chunks + 1) * kIterChunk * 10 + 2;
   const int rk = hst.rk;
 

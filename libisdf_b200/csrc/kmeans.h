@@ -26,6 +26,7 @@ struct KmeansResult {
   int iters = 0;
   int npt = 0;
   int launches = 0;
+  double search_frac = 0;  // share of point assignments that ran the cell search
 };
 
 size_t kmeans_workspace_bytes(long long ng, int mu);
