@@ -272,9 +272,10 @@ def run_ours(args, shape):
                         qrcp_oversample=args.qrcp_factor, qrcp_seed=args.qrcp_seed)
     s1 = "QRCP" if args.selector == "qrcp" else "Kmeans"
 
-    def solve():
+    def solve(theta=None):
         return isdf.ISDF(d_psi, dom, shape.nocc, shape.nstate, shape.nv1, shape.nc1, shape.nv2,
-                         shape.nc2, mu, d_theta, piv, shape.kmeans_iters, s1=s1, options=opts)
+                         shape.nc2, mu, d_theta if theta is None else theta, piv,
+                         shape.kmeans_iters, s1=s1, options=opts)
 
     fp64_peak = _fp64_peak_tflops(torch)
     int8_peak = _int8_peak_tops(torch) if args.precision == "mixed" else None
@@ -309,22 +310,50 @@ def run_ours(args, shape):
         if dist:
             dist.barrier()
 
-        # end to end from host buffers: H2D psi, solve, D2H theta
+        # End to end from host buffers, as a caller that consumes theta on the
+        # host runs it: every step copies psi in (pinned host -> HBM), solves,
+        # and copies theta out (HBM -> pinned host). The D2H copy of step i
+        # runs on a copy stream while step i+1 solves into the other theta
+        # buffer (two device theta buffers when HBM allows, else one and no
+        # overlap).
         h_theta = torch.empty((mu, ng), dtype=torch.float64).pin_memory()
-        e2e_steps = max(1, min(args.steps, 3))
+        e2e_steps = max(3, args.steps)
+        free_b, _ = torch.cuda.mem_get_info()
+        thetas = [d_theta]
+        if free_b > d_theta.numel() * 8 + (8 << 30):
+            thetas.append(torch.empty_like(d_theta))
+        copy_stream = torch.cuda.Stream()
+        done = [None] * len(thetas)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(e2e_steps):
+        for i in range(e2e_steps):
+            buf = i % len(thetas)
+            if done[buf] is not None:
+                stream.wait_event(done[buf])
             d_psi.copy_(h_psi, non_blocking=True)
-            rep = solve()
-            h_theta.copy_(d_theta, non_blocking=True)
+            rep = solve(thetas[buf])
+            solved = torch.cuda.Event()
+            solved.record(stream)
+            copy_stream.wait_event(solved)
+            with torch.cuda.stream(copy_stream):
+                # in 256 MB pieces, so that the library's small state reads
+                # of the next solve are not queued behind one long copy
+                src, dst = thetas[buf].view(-1), h_theta.view(-1)
+                piece = 1 << 25
+                for o in range(0, src.numel(), piece):
+                    dst[o:o + piece].copy_(src[o:o + piece], non_blocking=True)
+            done[buf] = torch.cuda.Event()
+            done[buf].record(copy_stream)
+        stream.wait_stream(copy_stream)
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+        e2e_bufs = len(thetas)
+        del thetas
 
     if dist:
         dist.destroy_process_group()
@@ -408,7 +437,8 @@ def run_ours(args, shape):
         "roofline": roofline,
         "e2e": {"value": replica_value(world, e2e_steps, e2e_ms), "unit": "solves/s",
                 "h2d_bytes_per_step": int(h_psi.numel() * 8),
-                "d2h_bytes_per_step": int(h_theta.numel() * 8 + piv.nbytes)},
+                "d2h_bytes_per_step": int(h_theta.numel() * 8 + piv.nbytes),
+                "steps": e2e_steps, "theta_buffers": e2e_bufs},
         "gpu_launches": int(sum(launches)),
         "mixed_vs_fp64": accuracy,
         "clocks": clk.summary(),
@@ -484,9 +514,16 @@ def run_serve(args):
     shapes = [synth.SI8, synth.SI64, synth.SI216]
     pool_seeds = [4, 2, 1]
     theta_bufs = [8, 4, 1]
+    mix = [0.6, 0.3, 0.1]
+    if args.serve_mix != "standard":
+        # one shape only (the served form's throughput at that size)
+        k1 = {"si8": 0, "si64": 1, "si216": 2}[args.serve_mix]
+        mix = [1.0 if k == k1 else 0.0 for k in range(3)]
+        pool_seeds = [1 if k == k1 else 0 for k in range(3)]
+        theta_bufs = [args.slots if k == k1 else 0 for k in range(3)]
     rng = np.random.default_rng(args.serve_seed)
     n_req = args.requests
-    kinds = rng.choice(3, size=n_req, p=[0.6, 0.3, 0.1])
+    kinds = rng.choice(3, size=n_req, p=mix)
     arrivals = np.cumsum(rng.exponential(1.0 / args.rate, size=n_req))
     prec = isdf.PRECISION_MIXED if args.precision == "mixed" else isdf.PRECISION_FP64
     opts = isdf.Options(precision=prec)
@@ -498,7 +535,12 @@ def run_serve(args):
     doms = [isdf.Domain(length=(sh.length,) * 3, num_grid=(sh.n,) * 3) for sh in shapes]
     torch.cuda.synchronize()
 
-    srv = isdf.Server(slots=args.slots)
+    budget = 0
+    if args.hbm_budget_gb > 0:
+        budget = int(args.hbm_budget_gb * (1 << 30))
+    elif args.hbm_budget_gb < 0:  # all that is free now, less 4 GiB
+        budget = max(0, torch.cuda.mem_get_info()[0] - (4 << 30))
+    srv = isdf.Server(slots=args.slots, hbm_budget_bytes=budget)
     lock = threading.Condition()
     inflight = {}  # ticket -> (kind, theta, arrival index)
     done_at = np.zeros(n_req)
@@ -509,10 +551,11 @@ def run_serve(args):
         return srv.submit(psi[k][i % pool_seeds[k]], doms[k], sh.nocc, sh.nstate, sh.nv1, sh.nc1,
                           sh.nv2, sh.nc2, sh.mu, theta, piv, sh.kmeans_iters, options=opts)
 
-    # warm-up: one request of each shape (workspaces, graphs)
+    # warm-up: one request of each shape served (workspaces, graphs)
     for k in range(3):
-        st, _ = srv.wait(submit(k, 0, free[k][0]))
-        assert st == 0, isdf.lib().isdf_last_error()
+        if pool_seeds[k]:
+            st, _ = srv.wait(submit(k, 0, free[k][0]))
+            assert st == 0, isdf.lib().isdf_last_error()
 
     stop = threading.Event()
 
@@ -563,8 +606,11 @@ def run_serve(args):
     line = {"metric": "served ISDF solves/s (serving mix)", "value": n_req / span,
             "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
             "data": "synthetic", "precision": args.precision,
-            "config": {"workload": "serving mix: 60 % Si8-like, 30 % Si64-like, 10 % Si216-like, "
-                                   "K-means", "requests": n_req, "rate_per_s": args.rate,
+            "config": {"workload": ("serving mix: 60 % Si8-like, 30 % Si64-like, 10 % Si216-like, "
+                                    "K-means" if args.serve_mix == "standard" else
+                                    f"served {args.serve_mix} requests only, K-means"),
+                       "requests": n_req, "rate_per_s": args.rate,
+                       "hbm_budget_bytes": budget,
                        "slots": args.slots, "psi_pool_seeds": pool_seeds,
                        "theta_buffers": theta_bufs,
                        "mix_counts": [int((kinds == k).sum()) for k in range(3)]},
@@ -600,6 +646,10 @@ def main():
     ap.add_argument("--rate", type=float, default=4.0, help="arrivals per second (--serve)")
     ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--serve-seed", type=int, default=7)
+    ap.add_argument("--serve-mix", choices=["standard", "si8", "si64", "si216"], default="standard",
+                    help="standard: 60/30/10 Si8/Si64/Si216; else one shape only")
+    ap.add_argument("--hbm-budget-gb", type=float, default=0.0,
+                    help="server workspace budget (0: the library default, -1: all free less 4 GiB)")
     args = ap.parse_args()
     from libisdf_b200 import synth
 

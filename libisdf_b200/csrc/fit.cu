@@ -646,6 +646,48 @@ MixedBuffers carve_mixed(Arena& a, long long ng, int nstate, int rk, int slices)
   return b;
 }
 
+// A side with contiguous rows (rs = 1): one thread per row and 16-column
+// K chunk. The warp's loads are 256-byte rows of one column, and the
+// thread's digits of one slice form one 16-byte store that lands next to its
+// neighbours' in the tiled layout: no shared memory, one pass over X.
+template <int S>
+__global__ void __launch_bounds__(256) k_slice_rows(const double* __restrict__ X, long long ks,
+                                                    int M, int K, int mp, int kp,
+                                                    const int* __restrict__ e,
+                                                    int8_t* __restrict__ P) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= mp) return;
+  const int k0 = blockIdx.y * 16;
+  double r[16];
+  const double sc = m < M ? ldexp(1.0, -e[m]) : 0.0;
+#pragma unroll
+  for (int j = 0; j < 16; ++j)
+    r[j] = (m < M && k0 + j < K) ? X[m + (long long)(k0 + j) * ks] * sc : 0.0;
+  int8_t* dst = P + ozaki::tiled_offset<S, ozaki::BM, false>(m / ozaki::BM, k0 / ozaki::BKB,
+                                                             kp / ozaki::BKB, 0,
+                                                             (k0 % ozaki::BKB) / 16, m % ozaki::BM);
+#pragma unroll
+  for (int t = 0; t < S; ++t) {
+    unsigned w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      unsigned v = 0;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int j = q * 4 + b;
+        r[j] *= ozaki::kBase;
+        const double d = rint(r[j]);
+        r[j] -= d;
+        v |= ((unsigned)(int)d & 0xffu) << (8 * b);
+      }
+      w[q] = v;
+    }
+    // slice t of the same row and chunk sits BM * BKB bytes further on
+    *reinterpret_cast<uint4*>(dst + (size_t)t * ozaki::BM * ozaki::BKB) =
+        make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
 // A side: R = 128 row blocks; B side: the stacked 64-column blocks.
 // gathered = true: e holds the binade maxima from the producing GEMM's
 // epilogue, and the pass over X that k_row_exponent makes is saved.
@@ -655,8 +697,14 @@ int slice_operand(const double* X, long long rs, long long ks, int M, int K, int
   if (gathered) k_exp_from_max<<<grid_for(M, 256), 256, 0, s>>>(e, M);
   else k_row_exponent<<<grid_for(M, 256), 256, 0, s>>>(X, rs, ks, M, K, e);
   dim3 g((unsigned)(kp / kSliceK), (unsigned)((mp + kSliceTile - 1) / kSliceTile));
-  if (B_SIDE) k_slice<S, ozaki::BN, true><<<g, 256, 0, s>>>(X, rs, ks, M, K, mp, kp, e, P);
-  else k_slice<S, ozaki::BM, false><<<g, 256, 0, s>>>(X, rs, ks, M, K, mp, kp, e, P);
+  if (B_SIDE) {
+    k_slice<S, ozaki::BN, true><<<g, 256, 0, s>>>(X, rs, ks, M, K, mp, kp, e, P);
+  } else if (rs == 1) {
+    dim3 gr((unsigned)((mp + 255) / 256), (unsigned)(kp / 16));
+    k_slice_rows<S><<<gr, 256, 0, s>>>(X, ks, M, K, mp, kp, e, P);
+  } else {
+    k_slice<S, ozaki::BM, false><<<g, 256, 0, s>>>(X, rs, ks, M, K, mp, kp, e, P);
+  }
   ISDF_CHECK_LAUNCH();
   return ISDF_OK;
 }
