@@ -374,19 +374,26 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
       for (int j = 0; j < BN; ++j) out[j] = 0.0;
       if (nk > 0) {
-        double w = 1.0 / (kBase * kBase);  // 254^{-(d+2)}
+        double w[S];  // 254^{-(d+2)}
+        w[0] = 1.0 / (kBase * kBase);
 #pragma unroll
-        for (int d = 0; d < S; ++d) {
-          if (d > 0) w = w / kBase;
+        for (int d = 1; d < S; ++d) w[d] = w[d - 1] / kBase;
+        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+        // two levels per TMEM round trip; per column the levels still
+        // accumulate in order d = 0, 1, ...
 #pragma unroll
-          for (int c0 = 0; c0 < BN; c0 += 32) {
-            uint32_t v[32];
-            const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d * BN + c0);
-            ISDF_TMEM_LD32(v, addr);
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+#pragma unroll
+          for (int d = 0; d < S; d += 2) {
+            uint32_t va[32], vb[32];
+            ISDF_TMEM_LD32(va, lane_base + (uint32_t)(d * BN + c0));
+            if (d + 1 < S) ISDF_TMEM_LD32(vb, lane_base + (uint32_t)((d + 1) * BN + c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-            for (int j = 0; j < 32; ++j)
-              out[c0 + j] = __fma_rn((double)(int)v[j], w, out[c0 + j]);
+            for (int j = 0; j < 32; ++j) {
+              out[c0 + j] = __fma_rn((double)(int)va[j], w[d], out[c0 + j]);
+              if (d + 1 < S) out[c0 + j] = __fma_rn((double)(int)vb[j], w[d + 1], out[c0 + j]);
+            }
           }
         }
       }
