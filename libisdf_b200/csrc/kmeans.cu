@@ -32,7 +32,7 @@ namespace isdf_b200 {
 
 namespace {
 
-constexpr int kTile = 4096;      // points per counting-sort tile
+constexpr int kTile = 2048;      // points per counting-sort tile (one walking warp each)
 constexpr int kFinalChunk = 4096;  // points per partial argmin chunk
 constexpr int kIterChunk = 8;    // Lloyd iterations launched between host checks
 constexpr int kMaxCellsPerDim = 20;  // centroid cell grid of the pruned assignment
@@ -337,23 +337,35 @@ __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
       bj = old;
       if (count && !st->reset_bounds) {
         const double2 b = bnd[p];
-        // Every other centroid moved closer by at most its shift. Those that
-        // sat in the 27 cells around p moved at most nbshift; the others were
-        // at least D away (D: distance from p to the outside of those cells,
-        // no bound across the domain's faces), so when D - (largest shift)
-        // stays above the lowered bound they cannot undercut it either.
+        // Every other centroid moved closer by at most its shift: at most
+        // the 3^3-block maximum inside the 27 cells around p, the 5^3-block
+        // maximum in the ring beyond (which started at least D1 away), the
+        // global maximum further out (at least D2 away); no bound across the
+        // domain's faces.
         const double gmax = __longlong_as_double((long long)st->maxshift_bits);
-        const double near = (double)nbshift[pi + g.nc * (pj + g.nc * pk)];
-        double D = inf;
-        if (pi >= 2) D = fmin(D, x - (pi - 1) * g.h[0]);
-        if (pi + 2 <= g.nc - 1) D = fmin(D, (pi + 2) * g.h[0] - x);
-        if (pj >= 2) D = fmin(D, y - (pj - 1) * g.h[1]);
-        if (pj + 2 <= g.nc - 1) D = fmin(D, (pj + 2) * g.h[1] - y);
-        if (pk >= 2) D = fmin(D, z - (pk - 1) * g.h[2]);
-        if (pk + 2 <= g.nc - 1) D = fmin(D, (pk + 2) * g.h[2] - z);
-        D = D * kRoundDown - g.tol;
-        double lo = fmax(0.0, __dsub_rd(b.y, near));
-        if (!(D - gmax >= lo)) lo = fmax(0.0, __dsub_rd(b.y, gmax));
+        const int cell = pi + g.nc * (pj + g.nc * pk);
+        const double near1 = (double)nbshift[cell], near2 = (double)nbshift[kMaxCells + cell];
+        // distances from p to the outside of the 3^3 and 5^3 cell blocks around it
+        double D1 = inf, D2 = inf;
+        if (pi >= 2) D1 = fmin(D1, x - (pi - 1) * g.h[0]);
+        if (pi + 2 <= g.nc - 1) D1 = fmin(D1, (pi + 2) * g.h[0] - x);
+        if (pj >= 2) D1 = fmin(D1, y - (pj - 1) * g.h[1]);
+        if (pj + 2 <= g.nc - 1) D1 = fmin(D1, (pj + 2) * g.h[1] - y);
+        if (pk >= 2) D1 = fmin(D1, z - (pk - 1) * g.h[2]);
+        if (pk + 2 <= g.nc - 1) D1 = fmin(D1, (pk + 2) * g.h[2] - z);
+        if (pi >= 3) D2 = fmin(D2, x - (pi - 2) * g.h[0]);
+        if (pi + 3 <= g.nc - 1) D2 = fmin(D2, (pi + 3) * g.h[0] - x);
+        if (pj >= 3) D2 = fmin(D2, y - (pj - 2) * g.h[1]);
+        if (pj + 3 <= g.nc - 1) D2 = fmin(D2, (pj + 3) * g.h[1] - y);
+        if (pk >= 3) D2 = fmin(D2, z - (pk - 2) * g.h[2]);
+        if (pk + 3 <= g.nc - 1) D2 = fmin(D2, (pk + 3) * g.h[2] - z);
+        D1 = D1 * kRoundDown - g.tol;
+        D2 = D2 * kRoundDown - g.tol;
+        // every other centroid was at least l away (and D1 / D2 beyond the blocks)
+        double lo = __dsub_rd(b.y, near1);
+        lo = fmin(lo, __dsub_rd(fmax(b.y, D1), near2));
+        lo = fmin(lo, __dsub_rd(fmax(b.y, D2), gmax));
+        lo = fmax(0.0, lo);
         double up = __dadd_ru(b.x, shift[old]);
         if (!(up * kBoundMargin < lo)) up = __dmul_ru(__dsqrt_ru(best), kRoundUp);
         if (up * kBoundMargin < lo) {
@@ -717,8 +729,9 @@ __global__ void __launch_bounds__(1024) k_centroids(double4* __restrict__ sums, 
   if (st->done) return;
   int rk = st->rk;
   if (!st->any_empty) {
-    __shared__ unsigned cmax[kMaxCells];
+    extern __shared__ unsigned cmax[];  // 3 x ncells: the cells' maxima, then two pass buffers
     const int nc = g.nc, ncells = nc * nc * nc;
+    unsigned* tmp = cmax + ncells;
     for (int c = threadIdx.x; c < ncells; c += blockDim.x) cmax[c] = 0u;
     __syncthreads();
     for (int i = threadIdx.x; i < rk; i += blockDim.x) {
@@ -735,14 +748,32 @@ __global__ void __launch_bounds__(1024) k_centroids(double4* __restrict__ sums, 
       atomicMax(&cmax[cell_of[i]], __float_as_uint(__double2float_ru(sh)));
     }
     __syncthreads();
-    for (int c = threadIdx.x; c < ncells; c += blockDim.x) {
-      const int ci = c % nc, cj = (c / nc) % nc, ck = c / (nc * nc);
-      unsigned m = 0u;
-      for (int dk = max(0, ck - 1); dk <= min(nc - 1, ck + 1); ++dk)
-        for (int dj = max(0, cj - 1); dj <= min(nc - 1, cj + 1); ++dj)
-          for (int di = max(0, ci - 1); di <= min(nc - 1, ci + 1); ++di)
-            m = max(m, cmax[di + nc * (dj + nc * dk)]);
-      nbshift[c] = __uint_as_float(m);
+    // 3^3 and 5^3 neighbourhood maxima as separable passes (x, y, z)
+    unsigned* t2 = tmp + ncells;
+    for (int rad = 1; rad <= 2; ++rad) {
+      for (int c = threadIdx.x; c < ncells; c += blockDim.x) {
+        const int ci = c % nc;
+        unsigned m = 0u;
+        for (int d = max(-rad, -ci); d <= min(rad, nc - 1 - ci); ++d) m = max(m, cmax[c + d]);
+        tmp[c] = m;
+      }
+      __syncthreads();
+      for (int c = threadIdx.x; c < ncells; c += blockDim.x) {
+        const int cj = (c / nc) % nc;
+        unsigned m = 0u;
+        for (int d = max(-rad, -cj); d <= min(rad, nc - 1 - cj); ++d) m = max(m, tmp[c + d * nc]);
+        t2[c] = m;
+      }
+      __syncthreads();
+      float* out = rad == 1 ? nbshift : nbshift + kMaxCells;
+      for (int c = threadIdx.x; c < ncells; c += blockDim.x) {
+        const int ck = c / (nc * nc);
+        unsigned m = 0u;
+        for (int d = max(-rad, -ck); d <= min(rad, nc - 1 - ck); ++d)
+          m = max(m, t2[c + d * nc * nc]);
+        out[c] = __uint_as_float(m);
+      }
+      __syncthreads();
     }
     return;
   }
@@ -844,6 +875,8 @@ int set_kmeans_smem_attrs() {
                                  (int)(sizeof(int) * kKmeansMaxMu)));
   ISDF_CUDA(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(sizeof(int) * (kKmeansMaxMu + kTile))));
+  ISDF_CUDA(cudaFuncSetAttribute(k_centroids, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(3 * sizeof(unsigned) * kMaxCells)));
   if (dev >= 0 && dev < 64) done[dev] = true;
   return ISDF_OK;
 }
@@ -893,7 +926,7 @@ KmBuffers carve(Arena& a, int n, int mu) {
   b.bnd = a.take<double2>(n);
   b.shift = a.take<double>(mu);
   b.g2p = a.take<int>(n);
-  b.nbshift = a.take<float>((size_t)kMaxCells);
+  b.nbshift = a.take<float>(2 * (size_t)kMaxCells);  // 3^3 and 5^3 neighbourhoods
   b.part_d = a.take<double>((size_t)nchunks * mu);
   b.part_i = a.take<int>((size_t)nchunks * mu);
   b.sel = a.take<int>(mu);
@@ -1036,6 +1069,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
                                                       b.bnd, b.shift, b.nbshift);
   ISDF_CHECK_LAUNCH();
 
+  const size_t cmax_smem = 3 * sizeof(unsigned) * ((size_t)cg.nc * cg.nc * cg.nc);
   const double max_f = 1e-5 * n;  // KmeansTolerance * n (utility.cpp:812)
   const size_t hist_smem = sizeof(int) * (size_t)mu;
   const size_t scatter_smem = sizeof(int) * ((size_t)mu + kTile);
@@ -1057,8 +1091,8 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
                                                        b.py, b.pz, b.pw, b.sorted);
       k_segsum<<<grid_for(mu, 8), 256, 0, stream>>>(b.sorted, b.start, b.members, b.px, b.py,
                                                     b.pz, b.pw, b.label, n, b.st, b.sums);
-      k_centroids<<<1, 1024, 0, stream>>>(b.sums, b.st, b.cen, b.shift, b.cell_of, cg,
-                                          b.nbshift);
+      k_centroids<<<1, 1024, cmax_smem, stream>>>(b.sums, b.st, b.cen, b.shift, b.cell_of, cg,
+                                                  b.nbshift);
       k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
                                                     b.cell_of);
       k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen,
