@@ -553,6 +553,12 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
 namespace {
 
 constexpr int kSliceTile = 64;  // rows per slicing tile
+
+// Round to the nearest integer (ties to even) on the FP64 add pipe: adding
+// 1.5 * 2^52 leaves the rounded value in the low word of the sum (two's
+// complement, |x| < 2^31); subtracting it back gives rint(x) exactly.
+constexpr double kRoundShift = 6755399441055744.0;
+__device__ __forceinline__ double round_shift(double x) { return __dadd_rn(x, kRoundShift); }
 constexpr int kSliceK = 32;     // K bytes per slicing tile
 
 // Row-scaled slicing of an M x K FP64 operand, element (m, k) at
@@ -598,9 +604,9 @@ __global__ void __launch_bounds__(256) k_slice(const double* __restrict__ X, lon
 #pragma unroll
     for (int t = 0; t < S; ++t) {
       r *= ozaki::kBase;
-      const double q = rint(r);
-      r -= q;
-      qs[t][mi][ki] = (int8_t)q;
+      const double tq = round_shift(r);
+      r -= tq - kRoundShift;
+      qs[t][mi][ki] = (int8_t)__double2loint(tq);
     }
   }
   __syncthreads();
@@ -676,9 +682,9 @@ __global__ void __launch_bounds__(256) k_slice_rows(const double* __restrict__ X
       for (int b = 0; b < 4; ++b) {
         const int j = q * 4 + b;
         r[j] *= ozaki::kBase;
-        const double d = rint(r[j]);
-        r[j] -= d;
-        v |= ((unsigned)(int)d & 0xffu) << (8 * b);
+        const double tq = round_shift(r[j]);
+        r[j] -= tq - kRoundShift;
+        v |= ((unsigned)__double2loint(tq) & 0xffu) << (8 * b);
       }
       w[q] = v;
     }
