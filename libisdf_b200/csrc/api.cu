@@ -257,6 +257,9 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
 
   // (c, d) fit with the selected points (the GPU path fits with the shrunk
   // rk, isdf-gpu.cpp:12,99); columns past rk_eff are zero-filled.
+  std::unique_lock<std::mutex> fit_guard;
+  if (res && res->fit_lock && (double)ng * rk_fit * rk_fit >= kSerialFitWork)
+    fit_guard = std::unique_lock<std::mutex>(*res->fit_lock);
   auto t1 = std::chrono::steady_clock::now();
   arena.off = mark;
   FitArgs fa;
@@ -289,6 +292,7 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
                               sizeof(double) * (size_t)(rk - rk_fit) * ng, s));
   ISDF_CUDA(cudaStreamSynchronize(s));
   rep.t_fit_ms = ms_since(t1);
+  if (fit_guard.owns_lock()) fit_guard.unlock();
   if (check) {
     // (e) the check of src/common/isdf.cpp:193-206 -> checkcode.cpp
     auto t2 = std::chrono::steady_clock::now();

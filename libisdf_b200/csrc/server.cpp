@@ -12,7 +12,10 @@
 // that does not fit yet, but only until the head has been passed over
 // `max_skips` times, after which nothing new starts until it fits. Latency
 // is measured from submit to completion; p50 / p99 and solves/s are
-// reported by isdf_server_stats().
+// reported by isdf_server_stats(). The fits of large systems (Ng rk^2 >=
+// 1e13) run one at a time: two of them on the tensor cores at once only
+// share the units and the power cap, while another request's K-means
+// selection (FP64 CUDA cores) overlaps a running fit.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -62,6 +65,7 @@ struct Server {
   Clock::time_point first_submit, last_finish;
   bool any_submit = false;
   long long completed = 0, failed = 0, cancelled = 0;
+  std::mutex fit_mutex;  // large fits one at a time (SolveResources::fit_lock)
 };
 
 int set_err(int code, const char* msg);
@@ -121,7 +125,7 @@ void worker(Server* s, int slot) {
       (void)cudaGetLastError();
       rc = set_err(ISDF_ERR_NOMEM, "server: workspace allocation failed");
     } else {
-      SolveResources res{static_cast<char*>(ws), jp->footprint, stream};
+      SolveResources res{static_cast<char*>(ws), jp->footprint, stream, &s->fit_mutex};
       rc = solve(&req.dom, req.d_psi, req.nocc, req.nstate, req.nv1, req.nc1, req.nv2, req.nc2,
                  req.mu_points, req.d_theta, req.piv, req.kmeans_max_iter, req.selector, req.check,
                  &req.opt, &rep, &res);

@@ -26,11 +26,16 @@ int record_error(int code, const char* msg);
 std::mutex& attr_mutex();
 
 // A caller-owned workspace and stream for one solve (the serving loop's slots).
+// fit_lock (optional): held around the fit of a large system (Ng rk^2 at
+// least kSerialFitWork), so that large fits run one at a time while other
+// requests' selections and small fits overlap them.
 struct SolveResources {
   char* base;
   size_t cap;
   cudaStream_t stream;
+  std::mutex* fit_lock = nullptr;
 };
+constexpr double kSerialFitWork = 1e13;
 
 // Device workspace one solve with these parameters needs.
 size_t request_footprint(const isdf_domain_t* dom, int nstate, int nv1, int nc1, int nv2, int nc2,
