@@ -312,6 +312,82 @@ constexpr double kBoundMargin = 1.0 + 1e-12;
 constexpr double kRoundUp = 1.0 + 1e-13;
 constexpr double kRoundDown = 1.0 - 1e-13;
 
+// Exact ring search for the nearest centroid of (x, y, z) (first minimum of
+// the reference's rounded distances), seeded with centroid `old` when it is
+// valid; writes the point's distance bounds and returns the label.
+__device__ __forceinline__ int ring_search(double x, double y, double z, int old, int rk,
+                                           const double4* __restrict__ cen,
+                                           const int* __restrict__ cell_start,
+                                           const double4* __restrict__ cell_cen,
+                                           const CellGrid& g, double2* bnd_p) {
+  const double inf = __longlong_as_double(0x7ff0000000000000LL);
+  double best = inf;
+  int bj = 0x7fffffff;
+  if (old >= 0 && old < rk) {  // any centroid is a valid start
+    best = ref_dist2(x, y, z, cen[old]);
+    bj = old;
+  }
+  const int pi = min(g.nc - 1, max(0, (int)floor(x / g.h[0])));
+  const int pj = min(g.nc - 1, max(0, (int)floor(y / g.h[1])));
+  const int pk = min(g.nc - 1, max(0, (int)floor(z / g.h[2])));
+  double second = inf;  // second-best squared distance seen
+  double floor2 = inf;  // lower bound (squared) on every centroid not seen
+  const double hmin = fmin(g.h[0], fmin(g.h[1], g.h[2]));
+  const double shrink = 1.0 - 2e-14;
+  for (int r = 0; r <= g.nc; ++r) {
+    if (r >= 2) {
+      const double lb = (r - 1) * hmin - g.tol;
+      if (lb > 0.0 && lb * lb * shrink > best) {
+        floor2 = fmin(floor2, lb * lb * shrink);
+        break;
+      }
+    }
+    for (int dk = -r; dk <= r; ++dk) {
+      const int ck = pk + dk;
+      if (ck < 0 || ck >= g.nc) continue;
+      for (int dj = -r; dj <= r; ++dj) {
+        const int cj = pj + dj;
+        if (cj < 0 || cj >= g.nc) continue;
+        for (int di = -r; di <= r; ++di) {
+          if (max(abs(di), max(abs(dj), abs(dk))) != r) continue;
+          const int ci = pi + di;
+          if (ci < 0 || ci >= g.nc) continue;
+          // box lower bound (box widened by tol)
+          const double bx = fmax(0.0, fmax(ci * g.h[0] - g.tol - x, x - (ci + 1) * g.h[0] - g.tol));
+          const double by = fmax(0.0, fmax(cj * g.h[1] - g.tol - y, y - (cj + 1) * g.h[1] - g.tol));
+          const double bz = fmax(0.0, fmax(ck * g.h[2] - g.tol - z, z - (ck + 1) * g.h[2] - g.tol));
+          const double lb = bx * bx + by * by + bz * bz;
+          if (lb * shrink > best) {
+            floor2 = fmin(floor2, lb * shrink);
+            continue;
+          }
+          const int id = ci + g.nc * (cj + g.nc * ck);
+          const int e = cell_start[id + 1];
+          for (int q = cell_start[id]; q < e; ++q) {
+            const double4 c = cell_cen[q];
+            const double d = ref_dist2(x, y, z, c);
+            const int j = (int)c.w;
+            if (d < best || (d == best && j < bj)) {
+              if (j != bj) second = best;
+              best = d;
+              bj = j;
+            } else if (j != bj) {
+              second = fmin(second, d);
+            }
+          }
+        }
+      }
+    }
+  }
+  *bnd_p = make_double2(__dmul_ru(__dsqrt_ru(best), kRoundUp),
+                        __dmul_rd(__dsqrt_rd(fmin(second, floor2)), kRoundDown));
+  return bj;
+}
+
+// Two phases per block: every thread tests its point against its distance
+// bounds; the points that fail are appended (warp order kept) to a block
+// list, which the block's threads then search together, so the divergent
+// ring search runs on full warps.
 __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
     const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
     int n, const double4* __restrict__ cen, const int* __restrict__ cell_start,
@@ -319,129 +395,85 @@ __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
     int* __restrict__ label, int count, double2* __restrict__ bnd,
     const double* __restrict__ shift, const float* __restrict__ nbshift) {
   if (st->done) return;
+  __shared__ int list_p[kAssignThreads], list_old[kAssignThreads];
+  __shared__ int list_n;
+  if (threadIdx.x == 0) list_n = 0;
+  __syncthreads();
   const int rk = st->rk;
+  const int lane = threadIdx.x & 31;
   const int p = assign_point((long long)blockIdx.x * blockDim.x + threadIdx.x, am);
-  int changed = 0, searched = 0;
+  bool need = false;
+  int old = -1;
   if (p >= 0 && p < n) {
-    const double x = px[p], y = py[p], z = pz[p];
-    const double inf = __longlong_as_double(0x7ff0000000000000LL);
-    double best = inf;
-    int bj = 0x7fffffff;
-    const int old = count ? label[p] : -1;
-    bool settled = false;
-    const int pi = min(g.nc - 1, max(0, (int)floor(x / g.h[0])));
-    const int pj = min(g.nc - 1, max(0, (int)floor(y / g.h[1])));
-    const int pk = min(g.nc - 1, max(0, (int)floor(z / g.h[2])));
-    if (old >= 0 && old < rk) {  // seed with the previous centroid (any centroid is a valid start)
-      best = ref_dist2(x, y, z, cen[old]);
-      bj = old;
-      if (count && !st->reset_bounds) {
-        const double2 b = bnd[p];
-        // Every other centroid moved closer by at most its shift: at most
-        // the 3^3-block maximum inside the 27 cells around p, the 5^3-block
-        // maximum in the ring beyond (which started at least D1 away), the
-        // global maximum further out (at least D2 away); no bound across the
-        // domain's faces.
-        const double gmax = __longlong_as_double((long long)st->maxshift_bits);
-        const int cell = pi + g.nc * (pj + g.nc * pk);
-        const double near1 = (double)nbshift[cell], near2 = (double)nbshift[kMaxCells + cell];
-        // distances from p to the outside of the 3^3 and 5^3 cell blocks around it
-        double D1 = inf, D2 = inf;
-        if (pi >= 2) D1 = fmin(D1, x - (pi - 1) * g.h[0]);
-        if (pi + 2 <= g.nc - 1) D1 = fmin(D1, (pi + 2) * g.h[0] - x);
-        if (pj >= 2) D1 = fmin(D1, y - (pj - 1) * g.h[1]);
-        if (pj + 2 <= g.nc - 1) D1 = fmin(D1, (pj + 2) * g.h[1] - y);
-        if (pk >= 2) D1 = fmin(D1, z - (pk - 1) * g.h[2]);
-        if (pk + 2 <= g.nc - 1) D1 = fmin(D1, (pk + 2) * g.h[2] - z);
-        if (pi >= 3) D2 = fmin(D2, x - (pi - 2) * g.h[0]);
-        if (pi + 3 <= g.nc - 1) D2 = fmin(D2, (pi + 3) * g.h[0] - x);
-        if (pj >= 3) D2 = fmin(D2, y - (pj - 2) * g.h[1]);
-        if (pj + 3 <= g.nc - 1) D2 = fmin(D2, (pj + 3) * g.h[1] - y);
-        if (pk >= 3) D2 = fmin(D2, z - (pk - 2) * g.h[2]);
-        if (pk + 3 <= g.nc - 1) D2 = fmin(D2, (pk + 3) * g.h[2] - z);
-        D1 = D1 * kRoundDown - g.tol;
-        D2 = D2 * kRoundDown - g.tol;
-        // every other centroid was at least l away (and D1 / D2 beyond the blocks)
-        double lo = __dsub_rd(b.y, near1);
-        lo = fmin(lo, __dsub_rd(fmax(b.y, D1), near2));
-        lo = fmin(lo, __dsub_rd(fmax(b.y, D2), gmax));
-        lo = fmax(0.0, lo);
-        double up = __dadd_ru(b.x, shift[old]);
-        if (!(up * kBoundMargin < lo)) up = __dmul_ru(__dsqrt_ru(best), kRoundUp);
-        if (up * kBoundMargin < lo) {
-          bnd[p] = make_double2(up, lo);
-          settled = true;
-        }
+    old = count ? label[p] : -1;
+    need = true;
+    if (old >= 0 && old < rk && count && !st->reset_bounds) {
+      const double x = px[p], y = py[p], z = pz[p];
+      const double inf = __longlong_as_double(0x7ff0000000000000LL);
+      const int pi = min(g.nc - 1, max(0, (int)floor(x / g.h[0])));
+      const int pj = min(g.nc - 1, max(0, (int)floor(y / g.h[1])));
+      const int pk = min(g.nc - 1, max(0, (int)floor(z / g.h[2])));
+      const double2 b = bnd[p];
+      // Every other centroid moved closer by at most its shift: at most
+      // the 3^3-block maximum inside the 27 cells around p, the 5^3-block
+      // maximum in the ring beyond (which started at least D1 away), the
+      // global maximum further out (at least D2 away); no bound across the
+      // domain's faces.
+      const double gmax = __longlong_as_double((long long)st->maxshift_bits);
+      const int cell = pi + g.nc * (pj + g.nc * pk);
+      const double near1 = (double)nbshift[cell], near2 = (double)nbshift[kMaxCells + cell];
+      // distances from p to the outside of the 3^3 and 5^3 cell blocks around it
+      double D1 = inf, D2 = inf;
+      if (pi >= 2) D1 = fmin(D1, x - (pi - 1) * g.h[0]);
+      if (pi + 2 <= g.nc - 1) D1 = fmin(D1, (pi + 2) * g.h[0] - x);
+      if (pj >= 2) D1 = fmin(D1, y - (pj - 1) * g.h[1]);
+      if (pj + 2 <= g.nc - 1) D1 = fmin(D1, (pj + 2) * g.h[1] - y);
+      if (pk >= 2) D1 = fmin(D1, z - (pk - 1) * g.h[2]);
+      if (pk + 2 <= g.nc - 1) D1 = fmin(D1, (pk + 2) * g.h[2] - z);
+      if (pi >= 3) D2 = fmin(D2, x - (pi - 2) * g.h[0]);
+      if (pi + 3 <= g.nc - 1) D2 = fmin(D2, (pi + 3) * g.h[0] - x);
+      if (pj >= 3) D2 = fmin(D2, y - (pj - 2) * g.h[1]);
+      if (pj + 3 <= g.nc - 1) D2 = fmin(D2, (pj + 3) * g.h[1] - y);
+      if (pk >= 3) D2 = fmin(D2, z - (pk - 2) * g.h[2]);
+      if (pk + 3 <= g.nc - 1) D2 = fmin(D2, (pk + 3) * g.h[2] - z);
+      D1 = D1 * kRoundDown - g.tol;
+      D2 = D2 * kRoundDown - g.tol;
+      // every other centroid was at least l away (and D1 / D2 beyond the blocks)
+      double lo = __dsub_rd(b.y, near1);
+      lo = fmin(lo, __dsub_rd(fmax(b.y, D1), near2));
+      lo = fmin(lo, __dsub_rd(fmax(b.y, D2), gmax));
+      lo = fmax(0.0, lo);
+      double up = __dadd_ru(b.x, shift[old]);
+      if (!(up * kBoundMargin < lo))
+        up = __dmul_ru(__dsqrt_ru(ref_dist2(x, y, z, cen[old])), kRoundUp);
+      if (up * kBoundMargin < lo) {  // the label stays
+        bnd[p] = make_double2(up, lo);
+        need = false;
       }
     }
-    if (!settled) {
-      double second = inf;  // second-best squared distance seen
-      double floor2 = inf;  // lower bound (squared) on every centroid not seen
-      const double hmin = fmin(g.h[0], fmin(g.h[1], g.h[2]));
-      const double shrink = 1.0 - 2e-14;
-      for (int r = 0; r <= g.nc; ++r) {
-        if (r >= 2) {
-          const double lb = (r - 1) * hmin - g.tol;
-          if (lb > 0.0 && lb * lb * shrink > best) {
-            floor2 = fmin(floor2, lb * lb * shrink);
-            break;
-          }
-        }
-        for (int dk = -r; dk <= r; ++dk) {
-          const int ck = pk + dk;
-          if (ck < 0 || ck >= g.nc) continue;
-          for (int dj = -r; dj <= r; ++dj) {
-            const int cj = pj + dj;
-            if (cj < 0 || cj >= g.nc) continue;
-            for (int di = -r; di <= r; ++di) {
-              if (max(abs(di), max(abs(dj), abs(dk))) != r) continue;
-              const int ci = pi + di;
-              if (ci < 0 || ci >= g.nc) continue;
-              // box lower bound (box widened by tol)
-              const double bx =
-                  fmax(0.0, fmax(ci * g.h[0] - g.tol - x, x - (ci + 1) * g.h[0] - g.tol));
-              const double by =
-                  fmax(0.0, fmax(cj * g.h[1] - g.tol - y, y - (cj + 1) * g.h[1] - g.tol));
-              const double bz =
-                  fmax(0.0, fmax(ck * g.h[2] - g.tol - z, z - (ck + 1) * g.h[2] - g.tol));
-              const double lb = bx * bx + by * by + bz * bz;
-              if (lb * shrink > best) {
-                floor2 = fmin(floor2, lb * shrink);
-                continue;
-              }
-              const int id = ci + g.nc * (cj + g.nc * ck);
-              const int e = cell_start[id + 1];
-              for (int q = cell_start[id]; q < e; ++q) {
-                const double4 c = cell_cen[q];
-                const double d = ref_dist2(x, y, z, c);
-                const int j = (int)c.w;
-                if (d < best || (d == best && j < bj)) {
-                  if (j != bj) second = best;
-                  best = d;
-                  bj = j;
-                } else if (j != bj) {
-                  second = fmin(second, d);
-                }
-              }
-            }
-          }
-        }
-      }
-      bnd[p] = make_double2(__dmul_ru(__dsqrt_ru(best), kRoundUp),
-                            __dmul_rd(__dsqrt_rd(fmin(second, floor2)), kRoundDown));
-    }
-    if (count && old != bj) ++changed;
-    label[p] = bj;
-    searched = settled ? 0 : 1;
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    changed += __shfl_xor_sync(0xffffffffu, changed, o);
-    searched += __shfl_xor_sync(0xffffffffu, searched, o);
+  // append the points that need a search, warp by warp in lane order
+  const unsigned mask = __ballot_sync(0xffffffffu, need);
+  int wbase = 0;
+  if (lane == 0 && mask) wbase = atomicAdd(&list_n, __popc(mask));
+  wbase = __shfl_sync(0xffffffffu, wbase, 0);
+  if (need) {
+    const int slot = wbase + __popc(mask & ((1u << lane) - 1u));
+    list_p[slot] = p;
+    list_old[slot] = old;
   }
-  if ((threadIdx.x & 31) == 0) {
-    if (count && changed) atomicAdd(&st->changed, changed);
-    if (searched) atomicAdd(&st->searches, (unsigned long long)searched);
+  __syncthreads();
+  const int ln = list_n;
+  int changed = 0;
+  for (int i = threadIdx.x; i < ln; i += blockDim.x) {
+    const int q = list_p[i], o = list_old[i];
+    const int bj = ring_search(px[q], py[q], pz[q], o, rk, cen, cell_start, cell_cen, g, &bnd[q]);
+    if (count && o != bj) ++changed;
+    label[q] = bj;
   }
+  for (int o = 16; o > 0; o >>= 1) changed += __shfl_xor_sync(0xffffffffu, changed, o);
+  if (lane == 0 && count && changed) atomicAdd(&st->changed, changed);
+  if (threadIdx.x == 0 && ln) atomicAdd(&st->searches, (unsigned long long)ln);
 }
 
 // ---------------------------------------------------------------- control
