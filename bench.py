@@ -393,18 +393,18 @@ def run_ours(args, shape):
                                              (t_gemm_ms * 1e-3) / 1e12) if t_gemm_ms > 0 else None,
                     "traffic": None}
     else:
-        # Dominant kernel: k_trsm_gemm, the two triangular sweeps as in-place
-        # FP64 tensor-core GEMMs. Algorithmic flops per solve: 2*Ng*rk^2
+        # Dominant kernel: k_trsm_ws, the two triangular sweeps as in-place
+        # FP64 tensor-core GEMMs (warp-specialised bulk-copy tile). Algorithmic flops per solve: 2*Ng*rk^2
         # (Ng*rk^2 per sweep). Its time is the triangular-solve stage on the
         # solve stream (CUDA events in the library around the stage: the
-        # k_trsm_gemm launches plus the small k_build_w launches between
+        # k_trsm_ws launches plus the small k_build_w launches between
         # them), so the rate is a slight underestimate of the kernel's own.
         achieved = 2.0 * ng * rk * rk / (t_solve_ms * 1e-3) / 1e12 if t_solve_ms > 0 else None
         # DRAM traffic of one launch: 8.37 B per grid row and solved column
         # (dram__bytes_read.sum + dram__bytes_write.sum of ncu on the 40^3-grid
         # case), times the mean solved width of a launch over both sweeps
         # (rk/2 + 32 columns).
-        roofline = {"kernel": "k_trsm_gemm (both sweeps of the triangular solve)",
+        roofline = {"kernel": "k_trsm_ws (both sweeps of the triangular solve)",
                     "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
                     "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved else None,
                     "peak_source": ("cuBLAS DGEMM 8192^3 measured in this run: the FP64 "

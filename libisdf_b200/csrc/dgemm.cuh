@@ -14,6 +14,8 @@
 
 #include <cuda_runtime.h>
 
+#include "mbarrier.cuh"
+
 namespace isdf_b200 {
 
 namespace dmma {
@@ -159,6 +161,168 @@ struct Core {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, t = lane & 3;
     const int wm0 = (warp >> 2) * WM, wn0 = (warp & 3) * WN;
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const int r = wm0 + i * 16 + g, c = wn0 + j * 8 + 2 * t;
+        f(r, c, acc[i][j][0]);
+        f(r, c + 1, acc[i][j][1]);
+        f(r + 8, c, acc[i][j][2]);
+        f(r + 8, c + 1, acc[i][j][3]);
+      }
+  }
+};
+
+// A row of zeros: the source of the warp-specialised tile's copies for the
+// columns and rows outside the operands.
+static __device__ double g_zero_row[256];
+
+// Warp-specialised FP64 tensor-core tile. WGM x WGN consumer warps compute
+// the BM x BN tile with mma.sync f64 (warp tile (BM/WGM) x (BN/WGN)); one
+// producer warp fills an ST-deep ring of BK-deep stages with bulk copies:
+// per stage BK columns of A (BM contiguous doubles each) and BK rows of B (BN
+// contiguous doubles each), each into a padded shared-memory row (same
+// fragment layout as Core), all completing on the stage's "full" mbarrier by
+// transaction count. A column or row past K, and the rows / columns past
+// m_rem / n_rem, are copied from a zero row, so every stage carries the same
+// byte count and the fragments never read stale shared memory. Each consumer
+// warp releases a stage through its "empty" mbarrier, so nothing in the K
+// loop synchronises the whole CTA.
+// Requirements (host-checked): A and B 16-byte aligned; lda, ldb, m_rem and
+// n_rem even.
+template <int BM_, int BN_, int WGM, int WGN, int BK_, int ST_>
+struct WsTile {
+  static constexpr int BM = BM_, BN = BN_, BK = BK_, ST = ST_;
+  static constexpr int NW = WGM * WGN, THREADS = NW * 32 + 32;
+  static constexpr int WM = BM / WGM, WN = BN / WGN;
+  static constexpr int MT = WM / 16, NT = WN / 8;
+  static constexpr int LDA_S = BM + PAD, LDB_S = BN + PAD;
+  static constexpr int A_STAGE = BK * LDA_S, B_STAGE = BK * LDB_S;
+  static constexpr size_t BAR_OFF = sizeof(double) * ST * (A_STAGE + B_STAGE);
+  static constexpr size_t SMEM_BYTES = BAR_OFF + 16 * ST + 16;
+  static constexpr uint32_t STAGE_TX = (uint32_t)(BK * (BM + BN) * sizeof(double));
+  static_assert(BM <= 256 && BN <= 256, "zero row");
+  static_assert(WM % 16 == 0 && WN % 8 == 0 && BK % 8 == 0, "tile shape");
+
+  double acc[MT][NT][4];
+
+  __device__ static bool producer() { return (threadIdx.x >> 5) == NW; }
+
+  // acc = A[0:m_rem, 0:K] * B[0:K, 0:n_rem] (zero outside), with
+  // A(m, k) = A[m + k*lda] and B(k, n) = B[k*ldb + n]. Every thread of the
+  // CTA calls it. Returns false (and sets *err) when a wait ran out; the
+  // producer warp returns with acc unset.
+  __device__ bool run(void* smem, const double* A, long long lda, int m_rem, const double* B,
+                      long long ldb, int n_rem, int K, int* err) {
+    uint8_t* base = static_cast<uint8_t*>(smem);
+    double* As = reinterpret_cast<double*>(base);
+    double* Bs = As + ST * A_STAGE;
+    const uint32_t fb = smem_u32(base + BAR_OFF), eb = fb + 8u * ST;
+    volatile int* abortp = reinterpret_cast<volatile int*>(base + BAR_OFF + 16 * ST);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+      for (int i = 0; i < ST; ++i) {
+        mbar_init(fb + 8u * i, 1);
+        mbar_init(eb + 8u * i, NW);
+      }
+      *abortp = 0;
+      asm volatile("fence.mbarrier_init.release.cluster;\n");
+    }
+    __syncthreads();
+    const int nk = K > 0 ? (K + BK - 1) / BK : 0;
+    bool ok = true;
+    if (warp == NW) {
+      // ------------------------------------------------------------ copies
+      int issued = 0;
+      for (int kt = 0; kt < nk; ++kt) {
+        const int s = kt % ST;
+        bool w = true;
+        if (kt >= ST) w = mbar_wait(eb + 8u * s, (uint32_t)((kt / ST) - 1) & 1u, abortp);
+        if (!__all_sync(0xffffffffu, w)) {
+          ok = false;
+          break;
+        }
+        if (lane == 0) mbar_expect_tx(fb + 8u * s, STAGE_TX);
+        __syncwarp();
+        const uint32_t as = smem_u32(As + s * A_STAGE), bs = smem_u32(Bs + s * B_STAGE);
+        const int k0 = kt * BK;
+        for (int c = lane; c < 2 * BK; c += 32) {
+          const bool is_a = c < BK;
+          const int k = k0 + (is_a ? c : c - BK);
+          const int rows = is_a ? BM : BN;
+          const int valid = k < K ? min(rows, is_a ? m_rem : n_rem) : 0;
+          const uint32_t dst = is_a ? as + (uint32_t)(c * LDA_S * 8)
+                                    : bs + (uint32_t)((c - BK) * LDB_S * 8);
+          if (valid > 0)
+            bulk_copy(dst, is_a ? A + (long long)k * lda : B + (long long)k * ldb,
+                      (uint32_t)valid * 8u, fb + 8u * s);
+          if (valid < rows)
+            bulk_copy(dst + (uint32_t)valid * 8u, g_zero_row, (uint32_t)(rows - valid) * 8u,
+                      fb + 8u * s);
+        }
+        ++issued;
+      }
+      // no copy may still be landing when the CTA exits
+      if (lane == 0)
+        for (int t = issued > ST ? issued - ST : 0; t < issued; ++t)
+          if (!mbar_wait_all(fb + 8u * (t % ST), (uint32_t)(t / ST) & 1u)) ok = false;
+      if (lane == 0 && (!ok || *abortp)) *err = 1;
+      __syncwarp();
+      return ok;
+    }
+    // -------------------------------------------------------------- DMMA
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NT; ++j)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm0 = (warp / WGN) * WM, wn0 = (warp % WGN) * WN;
+    for (int kt = 0; kt < nk; ++kt) {
+      const int s = kt % ST;
+      if (!__all_sync(0xffffffffu, mbar_wait(fb + 8u * s, (uint32_t)(kt / ST) & 1u, abortp))) {
+        ok = false;
+        break;
+      }
+      const double* as = As + s * A_STAGE;
+      const double* bs = Bs + s * B_STAGE;
+#pragma unroll
+      for (int kk = 0; kk < BK; kk += 8) {
+        double a[MT][4], b[NT][2];
+#pragma unroll
+        for (int i = 0; i < MT; ++i) {
+          const double* p = as + (kk + t) * LDA_S + wm0 + i * 16 + g;
+          a[i][0] = p[0];
+          a[i][1] = p[8];
+          a[i][2] = p[4 * LDA_S];
+          a[i][3] = p[4 * LDA_S + 8];
+        }
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          const double* p = bs + (kk + t) * LDB_S + wn0 + j * 8 + g;
+          b[j][0] = p[0];
+          b[j][1] = p[4 * LDB_S];
+        }
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int j = 0; j < NT; ++j) mma_16x8x8(acc[i][j], a[i], b[j]);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(eb + 8u * s);
+    }
+    if (!ok && lane == 0) *err = 1;
+    return ok;
+  }
+
+  // Calls f(row, col, value) for every accumulator element (consumer warps).
+  template <class F>
+  __device__ void for_each(F f) const {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm0 = (warp / WGN) * WM, wn0 = (warp % WGN) * WN;
 #pragma unroll
     for (int i = 0; i < MT; ++i)
 #pragma unroll

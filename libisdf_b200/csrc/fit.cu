@@ -11,10 +11,11 @@
 //   4. eps = 1e-10 * (trace / rk) added to the diagonal         (:346-349)
 //   5. lower Cholesky L                                          (:365)
 //   6. theta L^T = Z C^T, then theta L = (that), in place        (:372-382)
-// Kernels: one FP64 tensor-core GEMM core (dgemm.cuh: mma.sync m16n8k8 f64,
-// 3-stage cp.async pipeline) used by the Z GEMM, the Cholesky panel and
-// trailing updates and the triangular-solve steps; a single-CTA 64 x 64
-// diagonal-block factor + inverse.
+// Kernels: FP64 tensor-core GEMM tiles (dgemm.cuh: mma.sync m16n8k8 f64),
+// the 3-stage cp.async Core for the Z GEMM and the Cholesky panel and
+// trailing updates, the warp-specialised bulk-copy WsTile for the
+// triangular-solve steps (Core when theta's columns are not 16-byte
+// aligned); a single-CTA 64 x 64 diagonal-block factor + inverse.
 //
 // Triangular solve. For a 64-column block K = [c0, c0+bs) with diagonal block
 // L_KK and D = L_KK^{-1}, the forward step of theta L^T = Z is
@@ -46,6 +47,7 @@ constexpr int kNB = 64;  // Cholesky / triangular-solve block size
 
 using CoreZ = dmma::Core<128, 128>;  // Z GEMM, Cholesky trailing update
 using CoreN = dmma::Core<128, 64>;   // panel and triangular-solve steps
+using WsN = dmma::WsTile<64, 64, 2, 2, 16, 4>;  // triangular-solve steps, 3 CTAs per SM
 
 // 16-byte cp.async needs 16-byte aligned rows: base aligned, even leading dimension.
 __host__ __device__ inline bool vec2_ok(const void* a, long long lda, const void* b,
@@ -265,6 +267,23 @@ __global__ void __launch_bounds__(256) k_trsm_gemm(double* theta, long long ng, 
   });
 }
 
+// The same step on the warp-specialised tile (theta 16-byte aligned, Ng even).
+__global__ void __launch_bounds__(WsN::THREADS, 3)
+    k_trsm_ws(double* theta, long long ng, int c0, int bs, int kb, int ke,
+              const double* __restrict__ W, int* err) {
+  extern __shared__ __align__(128) double smem[];
+  const long long m0 = (long long)blockIdx.x * WsN::BM;
+  const int m_rem = (int)(ng - m0 < WsN::BM ? ng - m0 : WsN::BM);
+  WsN tile;
+  if (!tile.run(smem, theta + m0 + (long long)kb * ng, ng, m_rem, W + (long long)kb * kNB, kNB,
+                kNB, ke - kb, err))
+    return;
+  if (WsN::producer()) return;
+  tile.for_each([&](int r, int c, double v) {
+    if (r < m_rem && c < bs) theta[(m0 + r) + (long long)(c0 + c) * ng] = v;
+  });
+}
+
 // ---- L^{-1} by blocked doubling (the mixed form's triangular factors).
 // X = L^{-1} is kept twice: Xr row-major (X(i, j) = Xr[i*n + j], which is
 // L^{-T} column-major) and Xc column-major. Level s joins the inverted
@@ -356,7 +375,7 @@ int set_smem_attrs() {
   ISDF_TRY(set_attr(k_chol_panel<1>, CoreN::SMEM_BYTES));
   ISDF_TRY(set_attr(k_chol_panel<2>, CoreN::SMEM_BYTES));
   ISDF_TRY(set_attr(k_trsm_gemm<1>, CoreN::SMEM_BYTES));
-  ISDF_TRY(set_attr(k_trsm_gemm<2>, CoreN::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_trsm_ws, WsN::SMEM_BYTES));
   ISDF_TRY(set_attr(k_trinv_t<1>, CoreN::SMEM_BYTES));
   ISDF_TRY(set_attr(k_trinv_t<2>, CoreN::SMEM_BYTES));
   ISDF_TRY(set_attr(k_trinv_x<1>, CoreN::SMEM_BYTES));
@@ -373,7 +392,8 @@ struct FitBuffers {
   double* dinvT;
   double* dinv;
   double* eps;
-  int* info;
+  int* info;  // [0]: Cholesky (first failing column + 1), [1]: pipeline timeout
+  int* err;
 };
 
 FitBuffers carve(Arena& a, int nstate, int rk) {
@@ -386,7 +406,8 @@ FitBuffers carve(Arena& a, int nstate, int rk) {
   b.dinvT = a.take<double>((size_t)nblk * kNB * kNB);
   b.dinv = a.take<double>((size_t)nblk * kNB * kNB);
   b.eps = a.take<double>(1);
-  b.info = a.take<int>(1);
+  b.info = a.take<int>(2);
+  b.err = b.info ? b.info + 1 : nullptr;
   return b;
 }
 
@@ -469,7 +490,7 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
   res->launches = 1 + (same_ ? 1 : 2) + 2 + (nblk_ + 2 * (nblk_ - 1) + 1) + 4 * nblk_;
 
   ISDF_CUDA(cudaMemcpyAsync(b.piv, args.piv, sizeof(int) * rk, cudaMemcpyHostToDevice, s));
-  ISDF_CUDA(cudaMemsetAsync(b.info, 0, sizeof(int), s));
+  ISDF_CUDA(cudaMemsetAsync(b.info, 0, 2 * sizeof(int), s));
   k_gather_psimu<<<grid_for((long long)args.nstate * rk, 256), 256, 0, s>>>(
       args.d_psi, ng, args.nstate, b.piv, rk, b.Bm);
 
@@ -512,10 +533,12 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
   // theta L^T = Z C^T (forward over column blocks), then theta L = Y (backward)
   const int nblk = (rk + kNB - 1) / kNB;
   const unsigned tg = (unsigned)((ng + CoreN::BM - 1) / CoreN::BM);
+  const unsigned wg = (unsigned)((ng + WsN::BM - 1) / WsN::BM);
   const bool tv2 = vec2_ok(args.d_theta, ng, b.W, kNB);
   auto step = [&](int c0, int bs, int kb, int ke) {
-    if (tv2)
-      k_trsm_gemm<2><<<tg, 256, CoreN::SMEM_BYTES, s>>>(args.d_theta, ng, c0, bs, kb, ke, b.W);
+    if (tv2)  // 16-byte aligned columns: bulk copies
+      k_trsm_ws<<<wg, WsN::THREADS, WsN::SMEM_BYTES, s>>>(args.d_theta, ng, c0, bs, kb, ke, b.W,
+                                                           b.err);
     else
       k_trsm_gemm<1><<<tg, 256, CoreN::SMEM_BYTES, s>>>(args.d_theta, ng, c0, bs, kb, ke, b.W);
   };
@@ -533,8 +556,11 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
   }
   ISDF_CHECK_LAUNCH();
   ISDF_CUDA(mark(3));
+  int err = 0;
+  ISDF_CUDA(cudaMemcpyAsync(&err, b.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ISDF_CUDA(cudaStreamSynchronize(s));
+  if (err) return record_error(ISDF_ERR_TIMEOUT, "fit: a triangular-solve pipeline wait timed out");
   if (!timed) return ISDF_OK;
-  ISDF_CUDA(cudaEventSynchronize(ev.e[3]));
   ISDF_CUDA(cudaEventElapsedTime(&res->t_zct_ms, ev.e[0], ev.e[1]));
   ISDF_CUDA(cudaEventElapsedTime(&res->t_chol_ms, ev.e[1], ev.e[2]));
   ISDF_CUDA(cudaEventElapsedTime(&res->t_solve_ms, ev.e[2], ev.e[3]));
@@ -757,7 +783,7 @@ int fit_mixed_s(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* re
   const int mp = round_up(ng, ozaki::BM);
   const int np = round_up(rk, 128);
   ISDF_CUDA(cudaMemcpyAsync(b.piv, args.piv, sizeof(int) * rk, cudaMemcpyHostToDevice, s));
-  ISDF_CUDA(cudaMemsetAsync(b.info, 0, sizeof(int), s));
+  ISDF_CUDA(cudaMemsetAsync(b.info, 0, 2 * sizeof(int), s));
   ISDF_CUDA(cudaMemsetAsync(mb.err, 0, sizeof(int), s));
   k_gather_psimu<<<grid_for((long long)args.nstate * rk, 256), 256, 0, s>>>(
       args.d_psi, ng, args.nstate, b.piv, rk, b.Bm);
