@@ -176,7 +176,7 @@ struct Core {
 
 // A row of zeros: the source of the warp-specialised tile's copies for the
 // columns and rows outside the operands.
-static __device__ double g_zero_row[256];
+static __device__ __align__(128) double g_zero_row[256];
 
 // Warp-specialised FP64 tensor-core tile. WGM x WGN consumer warps compute
 // the BM x BN tile with mma.sync f64 (warp tile (BM/WGM) x (BN/WGN)); one
@@ -187,8 +187,11 @@ static __device__ double g_zero_row[256];
 // transaction count. A column or row past K, and the rows / columns past
 // m_rem / n_rem, are copied from a zero row, so every stage carries the same
 // byte count and the fragments never read stale shared memory. Each consumer
-// warp releases a stage through its "empty" mbarrier, so nothing in the K
-// loop synchronises the whole CTA.
+// warp releases a stage through its "empty" mbarrier after a proxy fence (its
+// shared-memory reads are generic-proxy accesses, the refill an async-proxy
+// write: without the fence, served solves running side by side saw stages
+// overwritten under the readers), so nothing in the K loop synchronises the
+// whole CTA.
 // Requirements (host-checked): A and B 16-byte aligned; lda, ldb, m_rem and
 // n_rem even.
 template <int BM_, int BN_, int WGM, int WGN, int BK_, int ST_>
@@ -310,6 +313,9 @@ struct WsTile {
 #pragma unroll
           for (int j = 0; j < NT; ++j) mma_16x8x8(acc[i][j], a[i], b[j]);
       }
+      // the stage's fragment loads (generic proxy) must be ordered before the
+      // producer's next bulk copy into the slot (async proxy)
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(eb + 8u * s);
     }

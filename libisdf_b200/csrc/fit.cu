@@ -81,6 +81,33 @@ __global__ void __launch_bounds__(256) k_gemm_z(int M, int N, int K, const doubl
   });
 }
 
+// The same product on the warp-specialised tile (16-byte aligned operands,
+// even sizes and leading dimensions).
+template <int MODE>
+__global__ void __launch_bounds__(WsN::THREADS, 3)
+    k_gemm_zws(int M, int N, int K, const double* __restrict__ A, long long lda,
+               const double* __restrict__ B, long long ldb, double* __restrict__ C, long long ldc,
+               int* err) {
+  extern __shared__ __align__(128) double smem[];
+  // one-dimensional grid, column tiles fastest: the CTAs in flight share their A rows in L2
+  const int ncol = (N + WsN::BN - 1) / WsN::BN;
+  const int n0 = (int)(blockIdx.x % ncol) * WsN::BN;
+  const long long m0 = (long long)(blockIdx.x / ncol) * WsN::BM;
+  const int m_rem = (int)(M - m0 < WsN::BM ? M - m0 : WsN::BM);
+  const int n_rem = N - n0 < WsN::BN ? N - n0 : WsN::BN;
+  WsN tile;
+  if (!tile.run(smem, A + m0, lda, m_rem, B + n0, ldb, n_rem, K, err)) return;
+  if (WsN::producer()) return;
+  tile.for_each([&](int r, int c, double v) {
+    if (r < m_rem && c < n_rem) {
+      double* p = C + (m0 + r) + (long long)(n0 + c) * ldc;
+      if (MODE == 0) *p = v * v;
+      else if (MODE == 1) *p = v;
+      else *p = *p * v;
+    }
+  });
+}
+
 // ----------------------------------------------------------- gathers
 // Bm[k*rk + j] = psi[piv_j + (k0 + k)*ng]  (depth-major B operand)
 __global__ void k_gather_psimu(const double* __restrict__ psi, long long ng, int nstate,
@@ -376,6 +403,9 @@ int set_smem_attrs() {
   ISDF_TRY(set_attr(k_chol_panel<2>, CoreN::SMEM_BYTES));
   ISDF_TRY(set_attr(k_trsm_gemm<1>, CoreN::SMEM_BYTES));
   ISDF_TRY(set_attr(k_trsm_ws, WsN::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_gemm_zws<0>, WsN::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_gemm_zws<1>, WsN::SMEM_BYTES));
+  ISDF_TRY(set_attr(k_gemm_zws<2>, WsN::SMEM_BYTES));
   ISDF_TRY(set_attr(k_trinv_t<1>, CoreN::SMEM_BYTES));
   ISDF_TRY(set_attr(k_trinv_t<2>, CoreN::SMEM_BYTES));
   ISDF_TRY(set_attr(k_trinv_x<1>, CoreN::SMEM_BYTES));
@@ -506,12 +536,17 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
   const double* B2 = b.Bm + (size_t)lo2 * rk;
   const bool zv2 = vec2_ok(A1, ng, B1, rk) && vec2_ok(A2, ng, B2, rk);
   const size_t zs = CoreZ::SMEM_BYTES;
+  // warp-specialised tile: 16-byte aligned operands, Ng and rk even (vec2_ok)
+  const unsigned zw = (unsigned)(((rk + WsN::BN - 1) / WsN::BN) * ((ng + WsN::BM - 1) / WsN::BM));
+  const int wt = WsN::THREADS;
+  const size_t ws = WsN::SMEM_BYTES;
+  double* th = args.d_theta;
   if (same) {
-    if (zv2) k_gemm_z<0, 2><<<zg, 256, zs, s>>>((int)ng, rk, K1, A1, ng, B1, rk, args.d_theta, ng);
+    if (zv2) k_gemm_zws<0><<<zw, wt, ws, s>>>((int)ng, rk, K1, A1, ng, B1, rk, th, ng, b.err);
     else k_gemm_z<0, 1><<<zg, 256, zs, s>>>((int)ng, rk, K1, A1, ng, B1, rk, args.d_theta, ng);
   } else if (zv2) {
-    k_gemm_z<1, 2><<<zg, 256, zs, s>>>((int)ng, rk, K1, A1, ng, B1, rk, args.d_theta, ng);
-    k_gemm_z<2, 2><<<zg, 256, zs, s>>>((int)ng, rk, K2, A2, ng, B2, rk, args.d_theta, ng);
+    k_gemm_zws<1><<<zw, wt, ws, s>>>((int)ng, rk, K1, A1, ng, B1, rk, th, ng, b.err);
+    k_gemm_zws<2><<<zw, wt, ws, s>>>((int)ng, rk, K2, A2, ng, B2, rk, th, ng, b.err);
   } else {
     k_gemm_z<1, 1><<<zg, 256, zs, s>>>((int)ng, rk, K1, A1, ng, B1, rk, args.d_theta, ng);
     k_gemm_z<2, 1><<<zg, 256, zs, s>>>((int)ng, rk, K2, A2, ng, B2, rk, args.d_theta, ng);
