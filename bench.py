@@ -400,7 +400,7 @@ def run_ours(args, shape):
         # k_trsm_ws launches plus the small k_build_w launches between
         # them), so the rate is a slight underestimate of the kernel's own.
         achieved = 2.0 * ng * rk * rk / (t_solve_ms * 1e-3) / 1e12 if t_solve_ms > 0 else None
-        # DRAM traffic of one launch: 8.37 B per grid row and solved column
+        # DRAM traffic of one launch: 8.40 B per grid row and solved column
         # (dram__bytes_read.sum + dram__bytes_write.sum of ncu on the 40^3-grid
         # case), times the mean solved width of a launch over both sweeps
         # (rk/2 + 32 columns).
@@ -411,7 +411,7 @@ def run_ours(args, shape):
                                     "denominator (the measured-peaks file holds HBM and BF16 "
                                     f"figures only; HBM {peaks.get('hbm_gbs')} GB/s from "
                                     f"{peak_src})"),
-                    "traffic": 8.37 * ng * (rk / 2 + 32),
+                    "traffic": 8.40 * ng * (rk / 2 + 32),
                     "traffic_note": "bytes per launch (mean over the sweep), scaled from the "
                                     "ncu capture at Ng = 64000 by rows x solved columns"}
     line = {
