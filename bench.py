@@ -272,10 +272,11 @@ def run_ours(args, shape):
                         qrcp_oversample=args.qrcp_factor, qrcp_seed=args.qrcp_seed)
     s1 = "QRCP" if args.selector == "qrcp" else "Kmeans"
 
-    def solve(theta=None):
-        return isdf.ISDF(d_psi, dom, shape.nocc, shape.nstate, shape.nv1, shape.nc1, shape.nv2,
-                         shape.nc2, mu, d_theta if theta is None else theta, piv,
-                         shape.kmeans_iters, s1=s1, options=opts)
+    def solve(theta=None, psi_d=None):
+        return isdf.ISDF(d_psi if psi_d is None else psi_d, dom, shape.nocc, shape.nstate,
+                         shape.nv1, shape.nc1, shape.nv2, shape.nc2, mu,
+                         d_theta if theta is None else theta, piv, shape.kmeans_iters, s1=s1,
+                         options=opts)
 
     fp64_peak = _fp64_peak_tflops(torch)
     int8_peak = _int8_peak_tops(torch) if args.precision == "mixed" else None
@@ -311,49 +312,76 @@ def run_ours(args, shape):
             dist.barrier()
 
         # End to end from host buffers, as a caller that consumes theta on the
-        # host runs it: every step copies psi in (pinned host -> HBM), solves,
-        # and copies theta out (HBM -> pinned host). The D2H copy of step i
-        # runs on a copy stream while step i+1 solves into the other theta
-        # buffer (two device theta buffers when HBM allows, else one and no
-        # overlap).
+        # host runs it: every step copies its psi in (pinned host -> HBM),
+        # solves, and copies theta out (HBM -> pinned host), in a steady
+        # pipeline: the psi of step i+1 is copied in on an H2D stream and the
+        # theta of step i copied out on a D2H stream while step i+1 solves
+        # (two device psi and theta buffers when HBM allows, else one of each
+        # and those copies do not overlap). At least 8 steps, so that the
+        # pipeline's fill and drain are a small part of the timed region.
         h_theta = torch.empty((mu, ng), dtype=torch.float64).pin_memory()
-        e2e_steps = max(3, args.steps)
+        e2e_steps = max(8, args.steps)
         free_b, _ = torch.cuda.mem_get_info()
         thetas = [d_theta]
         if free_b > d_theta.numel() * 8 + (8 << 30):
             thetas.append(torch.empty_like(d_theta))
+            free_b -= d_theta.numel() * 8
+        psis = [d_psi]
+        if free_b > d_psi.numel() * 8 + (8 << 30):
+            psis.append(torch.empty_like(d_psi))
         copy_stream = torch.cuda.Stream()
-        done = [None] * len(thetas)
+        h2d_stream = torch.cuda.Stream()
+        done = [None] * len(thetas)      # theta buffer copied out
+        used = [None] * len(psis)        # psi buffer no longer read by a solve
+        ready = [None] * len(psis)       # psi buffer holds its step's input
+
+        def fetch(k):
+            b = k % len(psis)
+            if used[b] is not None:
+                h2d_stream.wait_event(used[b])
+            with torch.cuda.stream(h2d_stream):
+                psis[b].copy_(h_psi, non_blocking=True)
+            ready[b] = torch.cuda.Event()
+            ready[b].record(h2d_stream)
+
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
+        h2d_stream.wait_event(e0)
+        fetch(0)
         for i in range(e2e_steps):
-            buf = i % len(thetas)
-            if done[buf] is not None:
-                stream.wait_event(done[buf])
-            d_psi.copy_(h_psi, non_blocking=True)
-            rep = solve(thetas[buf])
+            pb, tb = i % len(psis), i % len(thetas)
+            stream.wait_event(ready[pb])
+            if done[tb] is not None:
+                stream.wait_event(done[tb])
+            if len(psis) > 1 and i + 1 < e2e_steps:
+                fetch(i + 1)  # into the other buffer, beside this solve
+            rep = solve(thetas[tb], psis[pb])
             solved = torch.cuda.Event()
             solved.record(stream)
+            used[pb] = solved
+            if len(psis) == 1 and i + 1 < e2e_steps:
+                fetch(i + 1)
             copy_stream.wait_event(solved)
             with torch.cuda.stream(copy_stream):
                 # in 256 MB pieces, so that the library's small state reads
                 # of the next solve are not queued behind one long copy
-                src, dst = thetas[buf].view(-1), h_theta.view(-1)
+                src, dst = thetas[tb].view(-1), h_theta.view(-1)
                 piece = 1 << 25
                 for o in range(0, src.numel(), piece):
                     dst[o:o + piece].copy_(src[o:o + piece], non_blocking=True)
-            done[buf] = torch.cuda.Event()
-            done[buf].record(copy_stream)
+            done[tb] = torch.cuda.Event()
+            done[tb].record(copy_stream)
         stream.wait_stream(copy_stream)
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
         e2e_bufs = len(thetas)
-        del thetas
+        e2e_psi_bufs = len(psis)
+        del thetas, psis
 
     if dist:
         dist.destroy_process_group()
@@ -438,7 +466,7 @@ def run_ours(args, shape):
         "e2e": {"value": replica_value(world, e2e_steps, e2e_ms), "unit": "solves/s",
                 "h2d_bytes_per_step": int(h_psi.numel() * 8),
                 "d2h_bytes_per_step": int(h_theta.numel() * 8 + piv.nbytes),
-                "steps": e2e_steps, "theta_buffers": e2e_bufs},
+                "steps": e2e_steps, "theta_buffers": e2e_bufs, "psi_buffers": e2e_psi_bufs},
         "gpu_launches": int(sum(launches)),
         "mixed_vs_fp64": accuracy,
         "clocks": clk.summary(),

@@ -24,6 +24,7 @@
 #include "check.h"
 #include "common.cuh"
 #include "dgemm.cuh"
+#include "readback.h"
 #include "fit.h"
 #include "solve.h"
 
@@ -248,8 +249,7 @@ int check_run(const CheckArgs& args, Arena& arena, cudaStream_t s, double* fit_e
                                                 lo2, n2, b.part);
     ISDF_CHECK_LAUNCH();
     std::vector<double2> h(ftiles);
-    ISDF_CUDA(cudaMemcpyAsync(h.data(), b.part, sizeof(double2) * ftiles, cudaMemcpyDeviceToHost, s));
-    ISDF_CUDA(cudaStreamSynchronize(s));
+    ISDF_TRY(read_back(h.data(), b.part, sizeof(double2) * ftiles, s));
     double e2 = 0, r2 = 0;
     for (auto& v : h) {
       e2 += v.x;
@@ -306,8 +306,7 @@ int check_run(const CheckArgs& args, Arena& arena, cudaStream_t s, double* fit_e
   k_diff_norms<<<kDiffBlocks, 256, 0, s>>>(b.ijkl, b.cac, (long long)npair * npair, b.part);
   ISDF_CHECK_LAUNCH();
   std::vector<double2> h(kDiffBlocks);
-  ISDF_CUDA(cudaMemcpyAsync(h.data(), b.part, sizeof(double2) * kDiffBlocks, cudaMemcpyDeviceToHost, s));
-  ISDF_CUDA(cudaStreamSynchronize(s));
+  ISDF_TRY(read_back(h.data(), b.part, sizeof(double2) * kDiffBlocks, s));
   double e2 = 0, x2 = 0;
   for (auto& v : h) {
     e2 += v.x;

@@ -38,6 +38,7 @@
 #include "dgemm.cuh"
 #include "fit.h"
 #include "ozaki.cuh"
+#include "readback.h"
 
 namespace isdf_b200 {
 
@@ -517,7 +518,8 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
   auto mark = [&](int i) { return timed ? cudaEventRecord(ev.e[i], s) : cudaSuccess; };
   const int nblk_ = (rk + kNB - 1) / kNB;
   const bool same_ = (args.nv1 == args.nv2 && args.nc1 == args.nc2);
-  res->launches = 1 + (same_ ? 1 : 2) + 2 + (nblk_ + 2 * (nblk_ - 1) + 1) + 4 * nblk_;
+  res->launches = 1 + (same_ ? 1 : 2) + 2 + (nblk_ + 2 * (nblk_ - 1) + 1) + 4 * nblk_ +
+                  (readback_mailbox() ? 2 : 0);
 
   ISDF_CUDA(cudaMemcpyAsync(b.piv, args.piv, sizeof(int) * rk, cudaMemcpyHostToDevice, s));
   ISDF_CUDA(cudaMemsetAsync(b.info, 0, 2 * sizeof(int), s));
@@ -560,8 +562,7 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
   ISDF_TRY(cholesky(b, rk, s));
   ISDF_CUDA(mark(2));
   int info = 0;
-  ISDF_CUDA(cudaMemcpyAsync(&info, b.info, sizeof(int), cudaMemcpyDeviceToHost, s));
-  ISDF_CUDA(cudaStreamSynchronize(s));
+  ISDF_TRY(read_back(&info, b.info, sizeof(int), s));
   res->chol_info = info;
   if (info != 0) return record_error(ISDF_ERR_NOT_SPD, "fit: C C^T + eps I is not positive definite");
 
@@ -592,8 +593,7 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
   ISDF_CHECK_LAUNCH();
   ISDF_CUDA(mark(3));
   int err = 0;
-  ISDF_CUDA(cudaMemcpyAsync(&err, b.err, sizeof(int), cudaMemcpyDeviceToHost, s));
-  ISDF_CUDA(cudaStreamSynchronize(s));
+  ISDF_TRY(read_back(&err, b.err, sizeof(int), s));
   if (err) return record_error(ISDF_ERR_TIMEOUT, "fit: a triangular-solve pipeline wait timed out");
   if (!timed) return ISDF_OK;
   ISDF_CUDA(cudaEventElapsedTime(&res->t_zct_ms, ev.e[0], ev.e[1]));
@@ -864,8 +864,7 @@ int fit_mixed_s(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* re
   k_regularise<<<1, 256, 0, s>>>(b.P, rk, b.eps);
   ISDF_TRY(cholesky(b, rk, s));
   int info = 0;
-  ISDF_CUDA(cudaMemcpyAsync(&info, b.info, sizeof(int), cudaMemcpyDeviceToHost, s));
-  ISDF_CUDA(cudaStreamSynchronize(s));
+  ISDF_TRY(read_back(&info, b.info, sizeof(int), s));
   res->chol_info = info;
   if (info != 0) return record_error(ISDF_ERR_NOT_SPD, "fit: C C^T + eps I is not positive definite");
   // L^{-T} (= L^{-1} row-major) by blocked doubling from the diagonal-block inverses
@@ -906,9 +905,7 @@ int fit_mixed_s(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* re
   ISDF_CUDA(cudaEventRecord(ev.e[7], s));
   ISDF_CUDA(cudaEventRecord(ev.e[3], s));
   int err = 0;
-  ISDF_CUDA(cudaMemcpyAsync(&err, mb.err, sizeof(int), cudaMemcpyDeviceToHost, s));
-  ISDF_CUDA(cudaEventSynchronize(ev.e[3]));
-  ISDF_CUDA(cudaStreamSynchronize(s));
+  ISDF_TRY(read_back(&err, mb.err, sizeof(int), s));
   if (err) return record_error(ISDF_ERR_TIMEOUT, "mixed fit: a tensor-core pipeline wait timed out");
   ISDF_CUDA(cudaEventElapsedTime(&res->t_zct_ms, ev.e[0], ev.e[1]));
   ISDF_CUDA(cudaEventElapsedTime(&res->t_chol_ms, ev.e[1], ev.e[2]));
@@ -920,7 +917,8 @@ int fit_mixed_s(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* re
   const int nblk = (rk + kNB - 1) / kNB;
   int levels = 0;
   for (int lv = kNB; lv < rk; lv *= 2) ++levels;
-  res->launches = 1 + (same ? 3 : 6) * 2 + 2 + (nblk + 2 * (nblk - 1) + 1) + 1 + 2 * levels + 10;
+  res->launches = 1 + (same ? 3 : 6) * 2 + 2 + (nblk + 2 * (nblk - 1) + 1) + 1 + 2 * levels + 10 +
+                  (readback_mailbox() ? 2 : 0);
   return ISDF_OK;
 }
 

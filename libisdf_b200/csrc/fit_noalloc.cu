@@ -26,6 +26,7 @@
 #include "arena.h"
 #include "common.cuh"
 #include "fit.h"
+#include "readback.h"
 
 namespace isdf_b200 {
 
@@ -102,7 +103,11 @@ extern "C" int isdf_fit_noalloc(const double* d_psi, long long ng, int nstate, i
   fa.d_theta = d_theta;
   FitResult fr;
   cudaStream_t s = (cudaStream_t)stream;  // NULL: the legacy default stream
+  // no pinned mailbox either: the small status reads go by cudaMemcpyAsync
+  const bool mailbox = readback_mailbox();
+  set_readback_mailbox(false);
   int rc = fit_fp64(fa, arena, s, &fr, /*timed=*/false);
+  set_readback_mailbox(mailbox);
   if (chol_info) *chol_info = fr.chol_info;
   if (rc == ISDF_OK) ISDF_CUDA(cudaStreamSynchronize(s));
   return rc;

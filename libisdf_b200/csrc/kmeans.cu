@@ -27,6 +27,7 @@
 #include "common.cuh"
 #include "solve.h"
 #include "kmeans.h"
+#include "readback.h"
 
 namespace isdf_b200 {
 
@@ -1020,8 +1021,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
   k_filter_scatter<<<nfilter, 256, 0, stream>>>(args.d_w, n, b.st, b.tile_cnt, b.pidx);
   ISDF_CHECK_LAUNCH();
   KmState hst;
-  ISDF_CUDA(cudaMemcpyAsync(&hst, b.st, sizeof(KmState), cudaMemcpyDeviceToHost, stream));
-  ISDF_CUDA(cudaStreamSynchronize(stream));
+  ISDF_TRY(read_back(&hst, b.st, sizeof(KmState), stream));
   const int npt = hst.npt;
   res->npt = npt;
   std::memset(args.piv, 0, sizeof(int) * (size_t)n);
@@ -1029,9 +1029,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
   if (npt < mu) {
     // utility.cpp:667-681: piv from the kept list, then a shuffled tail.
     std::vector<int> index(n, 0);
-    ISDF_CUDA(cudaMemcpyAsync(index.data(), b.pidx, sizeof(int) * (size_t)npt,
-                              cudaMemcpyDeviceToHost, stream));
-    ISDF_CUDA(cudaStreamSynchronize(stream));
+    ISDF_TRY(read_back(index.data(), b.pidx, sizeof(int) * (size_t)npt, stream));
     int k0 = 0, k1 = 0;
     for (int i = 0; i < npt; i++) {
       if (i == index[k0]) {
@@ -1045,7 +1043,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     shuffle_like_libstdcxx(args.piv + npt, args.piv + n);
     res->rk_eff = mu;
     res->iters = -1;
-    res->launches = 4;
+    res->launches = 4 + (readback_mailbox() ? 2 : 0);
     return ISDF_OK;
   }
 
@@ -1155,14 +1153,15 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     if (exec) ISDF_CUDA(cudaGraphLaunch(exec, stream));
     else launch_chunk();
     ISDF_CHECK_LAUNCH();
-    ISDF_CUDA(cudaMemcpyAsync(&hst, b.st, sizeof(KmState), cudaMemcpyDeviceToHost, stream));
-    ISDF_CUDA(cudaStreamSynchronize(stream));
+    ISDF_TRY(read_back(&hst, b.st, sizeof(KmState), stream));
     if (hst.done) break;
     if (++chunks > max_chunks) return record_error(ISDF_ERR_CUDA, "kmeans: loop did not stop");
   }
   res->iters = hst.s;
   res->search_frac = (double)hst.searches / ((double)n * (hst.s + 1));
-  res->launches = 4 + 3 + (chunks + 1) * kIterChunk * 10 + 2;
+  // + the state, per-chunk and selection reads through the mapped mailbox
+  res->launches =
+      4 + 3 + (chunks + 1) * kIterChunk * 10 + 2 + (readback_mailbox() ? chunks + 3 : 0);
   const int rk = hst.rk;
 
   dim3 fgrid((unsigned)((rk + 127) / 128), (unsigned)nchunks);
@@ -1172,9 +1171,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
                                                         b.pidx, b.sel);
   ISDF_CHECK_LAUNCH();
   std::vector<int> sel(rk);
-  ISDF_CUDA(cudaMemcpyAsync(sel.data(), b.sel, sizeof(int) * (size_t)rk, cudaMemcpyDeviceToHost,
-                            stream));
-  ISDF_CUDA(cudaStreamSynchronize(stream));
+  ISDF_TRY(read_back(sel.data(), b.sel, sizeof(int) * (size_t)rk, stream));
   // unique (utility.cpp:617-629) and piv (utility.cpp:973-983)
   std::sort(sel.begin(), sel.end());
   sel.erase(std::unique(sel.begin(), sel.end()), sel.end());

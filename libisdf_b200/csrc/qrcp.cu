@@ -36,6 +36,7 @@
 #include "common.cuh"
 #include "dgemm.cuh"
 #include "fit.h"
+#include "readback.h"
 #include "qrcp.h"
 #include "solve.h"
 
@@ -513,8 +514,7 @@ int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* 
   launches += 6;
   ISDF_CHECK_LAUNCH();
   QrState hst;
-  ISDF_CUDA(cudaMemcpyAsync(&hst, b.st, sizeof(QrState), cudaMemcpyDeviceToHost, s));
-  ISDF_CUDA(cudaStreamSynchronize(s));
+  ISDF_TRY(read_back(&hst, b.st, sizeof(QrState), s));
   const int ntot = hst.ntot;
   const int kmax = std::min(kmax_cap, ntot);
   res->ntot_mg = ntot;
@@ -549,19 +549,17 @@ int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* 
 
   // piv = MGIdx[pivots], then the remaining kept columns in pivoted order, then 0
   std::vector<int> idx(ntot), perm(ntot), sel(kmax);
-  ISDF_CUDA(cudaMemcpyAsync(&hst, b.st, sizeof(QrState), cudaMemcpyDeviceToHost, s));
-  ISDF_CUDA(cudaMemcpyAsync(idx.data(), b.idx, sizeof(int) * ntot, cudaMemcpyDeviceToHost, s));
-  ISDF_CUDA(cudaMemcpyAsync(perm.data(), b.perm, sizeof(int) * ntot, cudaMemcpyDeviceToHost, s));
-  if (kmax > 0)
-    ISDF_CUDA(cudaMemcpyAsync(sel.data(), b.sel, sizeof(int) * kmax, cudaMemcpyDeviceToHost, s));
-  ISDF_CUDA(cudaStreamSynchronize(s));
+  ISDF_TRY(read_back(&hst, b.st, sizeof(QrState), s));
+  ISDF_TRY(read_back(idx.data(), b.idx, sizeof(int) * ntot, s));
+  ISDF_TRY(read_back(perm.data(), b.perm, sizeof(int) * ntot, s));
+  if (kmax > 0) ISDF_TRY(read_back(sel.data(), b.sel, sizeof(int) * kmax, s));
   std::memset(args.piv, 0, sizeof(int) * (size_t)n);
   for (int j = 0; j < ntot; ++j) args.piv[j] = idx[perm[j]];
   res->steps = kmax;
   res->num_pre = p;
   res->nflag = hst.nflag;
   res->done_early = hst.done;
-  res->launches = launches;
+  res->launches = launches + (readback_mailbox() ? (kmax > 0 ? 5 : 4) : 0);
   return ISDF_OK;
 }
 
