@@ -269,7 +269,8 @@ def run_ours(args, shape):
     stream = torch.cuda.Stream()
     prec = isdf.PRECISION_MIXED if args.precision == "mixed" else isdf.PRECISION_FP64
     opts = isdf.Options(stream=stream.cuda_stream, precision=prec,
-                        qrcp_oversample=args.qrcp_factor, qrcp_seed=args.qrcp_seed)
+                        qrcp_oversample=args.qrcp_factor, qrcp_seed=args.qrcp_seed,
+                        mixed_slices=args.mixed_slices)
     s1 = "QRCP" if args.selector == "qrcp" else "Kmeans"
 
     def solve(theta=None, psi_d=None):
@@ -410,7 +411,7 @@ def run_ours(args, shape):
         # ops per solve: 2 GEMMs x 2 x Ng x rk x (rk/2 + 32) x S(S+1)/2 (each
         # tile runs the K range its triangular factor leaves nonzero). Time:
         # CUDA events around the two launches on the solve stream.
-        S = isdf.Options().mixed_slices
+        S = args.mixed_slices
         ops = 2 * 2.0 * ng * rk * (rk / 2 + 32) * S * (S + 1) / 2
         achieved = ops / (t_gemm_ms * 1e-3) / 1e12 if t_gemm_ms > 0 else None
         roofline = {"kernel": "k_ozaki_gemm (Y = Z L^-T and theta = Y L^-1, INT8 digit pairs)",
@@ -452,7 +453,9 @@ def run_ours(args, shape):
                    "kmeans_search_frac": round(float(rep.kmeans_search_frac), 4), "selector": s1,
                    **({"qrcp_oversample": args.qrcp_factor, "qrcp_seed": args.qrcp_seed}
                       if s1 == "QRCP" else {}),
-                   "precision": args.precision, "parallelism": f"replicas x{world}",
+                   "precision": args.precision,
+                   **({"mixed_slices": args.mixed_slices} if args.precision == "mixed" else {}),
+                   "parallelism": f"replicas x{world}",
                    "l2": (f"inputs larger than L2 (psi {ng * shape.nstate * 8 / 1e9:.2f} GB, "
                           f"theta {ng * mu * 8 / 1e9:.2f} GB; L2 126 MB)")},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
@@ -661,6 +664,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=["si8", "si64", "si216", "si64c"], default="si64")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--mixed-slices", type=int, choices=[5, 6, 7], default=6,
+                    help="INT8 digits per operand in the mixed form (Options.mixed_slices)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--selector", choices=["kmeans", "qrcp"], default="kmeans")
     ap.add_argument("--qrcp-factor", type=float, default=1.5,
