@@ -87,3 +87,32 @@ def test_fit_not_spd_reports_info(torch_cuda):
     with pytest.raises(isdf.IsdfError) as e:
         isdf.fit(d_psi, 512, 4, 2, 2, 2, 2, 2, 8, np.arange(8, dtype=np.int32), d_theta)
     assert e.value.code == isdf.ISDF_ERR_NOT_SPD
+
+
+@pytest.mark.parametrize("name", ["small_s1s2", "small_mu0", "small_iters0", "si8_example"])
+def test_fit_warp_specialised_tiles_equal_cp_async_tiles(torch_cuda, name):
+    """The Z C^T product and the triangular sweeps run on the warp-specialised
+    bulk-copy tile when psi and theta are 16-byte aligned, else on the
+    cp.async tile. Both accumulate the same k-ordered tensor-core products, so
+    theta must be bit-identical; the shapes are ragged (Ng not a multiple of
+    the 64-row tile, rk not a multiple of 64, K not a multiple of the 16-deep
+    stage), and the S1 != S2 case runs the two-factor epilogue."""
+    torch = torch_cuda
+    g = load_golden(name)
+    psi = g["psi"]
+    ng, nstate = psi.shape
+    a = (int(g["nocc"]), int(g["nv1"]), int(g["nc1"]), int(g["nv2"]), int(g["nc2"]))
+    rk = int(g["rk_eff"])
+    flat = np.ascontiguousarray(np.asfortranarray(psi).T).ravel()
+    outs = []
+    for shift in (0, 1):  # one double in: 8-byte, not 16-byte, aligned
+        buf_psi = torch.zeros(flat.size + 1, dtype=torch.float64, device="cuda")
+        buf_psi[shift:shift + flat.size] = torch.from_numpy(flat).cuda()
+        buf_th = torch.full((rk * ng + 1,), float("nan"), dtype=torch.float64, device="cuda")
+        d_psi = buf_psi[shift:shift + flat.size]
+        d_theta = buf_th[shift:shift + rk * ng]
+        assert (d_psi.data_ptr() % 16 == 0) == (shift == 0)
+        assert isdf.fit(d_psi, ng, nstate, *a, rk, g["piv"], d_theta) == 0
+        outs.append(d_theta.cpu().numpy())
+    assert np.isfinite(outs[0]).all()
+    assert np.array_equal(outs[0], outs[1])
