@@ -228,30 +228,48 @@ __global__ void k_pick(int k, int p, int ntot, const double* __restrict__ Ac,
   }
 }
 
-// cdot[l] = Q[:, l] . x for l < k (one warp per l).
-__global__ void k_qt_x(const double* __restrict__ Q, int m, int k, const double* __restrict__ x,
-                       const QrState* st, double* __restrict__ cdot) {
+// cdot[l] = Q[:, l] . x for l < k: one block per l (a strided partial per
+// thread, then a fixed-order tree), so the sums do not depend on scheduling.
+__global__ void __launch_bounds__(256) k_qt_x(const double* __restrict__ Q, int m, int k,
+                                              const double* __restrict__ x, const QrState* st,
+                                              double* __restrict__ cdot) {
   if (st->done) return;
-  const int l = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
+  const int l = blockIdx.x;
   if (l >= k) return;
+  __shared__ double red[8];
   const double* q = Q + (long long)l * m;
   double s = 0.0;
-  for (int i = lane; i < m; i += 32) s = fma(q[i], x[i], s);
+  for (int i = threadIdx.x; i < m; i += 256) s = fma(q[i], x[i], s);
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) cdot[l] = s;
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = red[0];
+    for (int w = 1; w < 8; ++w) v += red[w];
+    cdot[l] = v;
+  }
 }
 
-// x -= Q[:, 0:k] cdot
-__global__ void k_x_minus_qc(const double* __restrict__ Q, int m, int k,
-                             const double* __restrict__ cdot, const QrState* st,
-                             double* __restrict__ x) {
+// x -= Q[:, 0:k] cdot: a block takes 32 consecutive rows (one per lane), its
+// eight warps the columns l = w (mod 8), and the eight partials are added in
+// warp order.
+__global__ void __launch_bounds__(256) k_x_minus_qc(const double* __restrict__ Q, int m, int k,
+                                                    const double* __restrict__ cdot,
+                                                    const QrState* st, double* __restrict__ x) {
   if (st->done) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
+  __shared__ double red[8][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + lane;
   double s = 0.0;
-  for (int l = 0; l < k; ++l) s = fma(Q[i + (long long)l * m], cdot[l], s);
-  x[i] -= s;
+  if (i < m)
+    for (int l = w; l < k; l += 8) s = fma(Q[i + (long long)l * m], cdot[l], s);
+  red[w][lane] = s;
+  __syncthreads();
+  if (w == 0 && i < m) {
+    double v = red[0][lane];
+    for (int u = 1; u < 8; ++u) v += red[u][lane];
+    x[i] -= v;
+  }
 }
 
 // q_k = x / |x| into Q[:, k] and into Qm (depth-major: Qm[i*p + j] = q[i + j*p]).
@@ -352,6 +370,67 @@ __global__ void __launch_bounds__(256) k_update(const double* __restrict__ Ac,
     atomicMax(&st->maxbits, (unsigned long long)__double_as_longlong(mx));
 }
 
+// The same downdate on the warp-specialised tile (16-byte aligned Bc and Qm,
+// ntot and p even): 64 rows x BN columns (BN >= p, a multiple of 8, the
+// columns past p copied as zeros), four DMMA warps of 16 full rows each, so
+// the row dot with A closes inside a quad of lanes. BN tracks p instead of a
+// fixed 128-wide tile, so no tensor-core work is spent on padding beyond the
+// next multiple of 16.
+template <int BN>
+using UpdTile = dmma::WsTile<64, BN, 4, 1, 16, 3>;
+
+template <int BN, int MINB>
+__global__ void __launch_bounds__(UpdTile<BN>::THREADS, MINB)
+    k_update_ws(const double* __restrict__ Ac, const double* __restrict__ Bc, int ntot, int p,
+                const double* __restrict__ Qm, const unsigned char* __restrict__ active,
+                double* __restrict__ nu, double* __restrict__ nu0, QrState* st, int* err) {
+  using T = UpdTile<BN>;
+  if (st->done) return;
+  extern __shared__ __align__(128) double smem[];
+  const int m0 = blockIdx.x * T::BM;
+  const int m_rem = min(T::BM, ntot - m0);
+  T tile;
+  if (!tile.run(smem, Bc + m0, ntot, m_rem, Qm, p, p, p, err)) return;
+  if (T::producer()) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  double mx = 0.0;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int r = warp * 16 + g + 8 * h;
+    double s = 0.0;
+    if (r < m_rem) {
+#pragma unroll
+      for (int j = 0; j < T::NT; ++j) {
+        const int c = j * 8 + 2 * t;
+        if (c < p) s = fma(Ac[(m0 + r) + (long long)c * ntot], tile.acc[0][j][2 * h], s);
+        if (c + 1 < p) s = fma(Ac[(m0 + r) + (long long)(c + 1) * ntot], tile.acc[0][j][2 * h + 1], s);
+      }
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    if (t == 0 && r < m_rem) {
+      const int c = m0 + r;
+      if (active[c]) {
+        double v = nu[c];
+        if (v != 0.0) {
+          const double ratio = fabs(s) / v;
+          const double temp = fmax(1.0 - ratio * ratio, 0.0);
+          const double rel = v / nu0[c];
+          const double temp2 = 1.0 + 0.05 * temp * rel * rel;
+          if (temp2 == 1.0) atomicAdd(&st->nflag, 1);
+          v = v * sqrt(temp);
+          nu[c] = v;
+        }
+        mx = fmax(mx, v);
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0 && mx > 0.0)
+    atomicMax(&st->maxbits, (unsigned long long)__double_as_longlong(mx));
+}
+
 // Householder QR of the K x p draws (host, FP64): returns p orthonormal columns
 // spanning the same space, row-major (K x p) for the depth-major GEMM operand.
 std::vector<double> orthonormal_rows(const std::vector<double>& g_colmajor, int K, int p) {
@@ -410,6 +489,7 @@ struct QrBuffers {
   int *idx, *pos, *perm, *sel, *tile_cnt;
   unsigned char* active;
   QrState* st;
+  int* err;  // a bounded pipeline wait of the update ran out
 };
 
 QrBuffers carve(Arena& a, long long n, int p, int k1, int k2, int kmax) {
@@ -436,6 +516,7 @@ QrBuffers carve(Arena& a, long long n, int p, int k1, int k2, int kmax) {
   b.tile_cnt = a.take<int>((size_t)ntiles);
   b.active = a.take<unsigned char>((size_t)n);
   b.st = a.take<QrState>(1);
+  b.err = a.take<int>(1);
   return b;
 }
 
@@ -449,8 +530,39 @@ int set_update_attrs() {
                                  (int)CoreU::SMEM_BYTES));
   ISDF_CUDA(cudaFuncSetAttribute(k_update<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)CoreU::SMEM_BYTES));
+#define ISDF_UPD_ATTR(BN, MINB)                                                              \
+  ISDF_CUDA(cudaFuncSetAttribute(k_update_ws<BN, MINB>,                                      \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,                \
+                                 (int)UpdTile<BN>::SMEM_BYTES))
+  ISDF_UPD_ATTR(32, 3);
+  ISDF_UPD_ATTR(48, 3);
+  ISDF_UPD_ATTR(64, 3);
+  ISDF_UPD_ATTR(80, 3);
+  ISDF_UPD_ATTR(96, 3);
+  ISDF_UPD_ATTR(112, 2);
+  ISDF_UPD_ATTR(128, 2);
+#undef ISDF_UPD_ATTR
   if (dev >= 0 && dev < 64) done[dev] = true;
   return ISDF_OK;
+}
+
+template <int BN, int MINB>
+void launch_update_bn(const QrBuffers& b, int ntot, int p, cudaStream_t s) {
+  using T = UpdTile<BN>;
+  const unsigned grid = (unsigned)((ntot + T::BM - 1) / T::BM);
+  k_update_ws<BN, MINB><<<grid, T::THREADS, T::SMEM_BYTES, s>>>(b.Ac, b.Bc, ntot, p, b.Qm,
+                                                               b.active, b.nu, b.nu0, b.st, b.err);
+}
+
+// The downdate on the narrowest warp-specialised tile that holds p columns.
+void launch_update_ws(const QrBuffers& b, int ntot, int p, cudaStream_t s) {
+  if (p <= 32) launch_update_bn<32, 3>(b, ntot, p, s);
+  else if (p <= 48) launch_update_bn<48, 3>(b, ntot, p, s);
+  else if (p <= 64) launch_update_bn<64, 3>(b, ntot, p, s);
+  else if (p <= 80) launch_update_bn<80, 3>(b, ntot, p, s);
+  else if (p <= 96) launch_update_bn<96, 3>(b, ntot, p, s);
+  else if (p <= 112) launch_update_bn<112, 2>(b, ntot, p, s);
+  else launch_update_bn<128, 2>(b, ntot, p, s);
 }
 
 }  // namespace
@@ -494,6 +606,7 @@ int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* 
   ISDF_CUDA(cudaMemcpyAsync(b.G1, q1.data(), sizeof(double) * q1.size(), cudaMemcpyHostToDevice, s));
   ISDF_CUDA(cudaMemcpyAsync(b.G2, q2.data(), sizeof(double) * q2.size(), cudaMemcpyHostToDevice, s));
   ISDF_CUDA(cudaMemsetAsync(b.st, 0, sizeof(QrState), s));
+  ISDF_CUDA(cudaMemsetAsync(b.err, 0, sizeof(int), s));
 
   // A = psi_S1 G1, B = psi_S2 G2
   ISDF_TRY(dgemm_store((int)n, p, k1, args.d_psi + (long long)(args.nocc - args.nv1) * n, n, b.G1,
@@ -530,15 +643,14 @@ int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* 
     launches += 2;
     if (k > 0) {
       for (int pass = 0; pass < 2; ++pass) {
-        k_qt_x<<<(k + 7) / 8, 256, 0, s>>>(b.Q, m, k, b.x, b.st, b.cdot);
-        k_x_minus_qc<<<(m + 255) / 256, 256, 0, s>>>(b.Q, m, k, b.cdot, b.st, b.x);
+        k_qt_x<<<k, 256, 0, s>>>(b.Q, m, k, b.x, b.st, b.cdot);
+        k_x_minus_qc<<<(m + 31) / 32, 256, 0, s>>>(b.Q, m, k, b.cdot, b.st, b.x);
         launches += 2;
       }
     }
     k_normalise<<<1, 1024, 0, s>>>(k, p, b.x, b.st, b.Q, b.Qm);
-    if (uv2)
-      k_update<2><<<ugrid, 256, CoreU::SMEM_BYTES, s>>>(b.Ac, b.Bc, ntot, p, b.Qm, b.active, b.nu,
-                                                        b.nu0, b.st);
+    if (uv2)  // 16-byte aligned rows: the warp-specialised tile
+      launch_update_ws(b, ntot, p, s);
     else
       k_update<1><<<ugrid, 256, CoreU::SMEM_BYTES, s>>>(b.Ac, b.Bc, ntot, p, b.Qm, b.active, b.nu,
                                                         b.nu0, b.st);
@@ -550,6 +662,9 @@ int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* 
   // piv = MGIdx[pivots], then the remaining kept columns in pivoted order, then 0
   std::vector<int> idx(ntot), perm(ntot), sel(kmax);
   ISDF_TRY(read_back(&hst, b.st, sizeof(QrState), s));
+  int err = 0;
+  ISDF_TRY(read_back(&err, b.err, sizeof(int), s));
+  if (err) return record_error(ISDF_ERR_TIMEOUT, "QRCP: an update pipeline wait timed out");
   ISDF_TRY(read_back(idx.data(), b.idx, sizeof(int) * ntot, s));
   ISDF_TRY(read_back(perm.data(), b.perm, sizeof(int) * ntot, s));
   if (kmax > 0) ISDF_TRY(read_back(sel.data(), b.sel, sizeof(int) * kmax, s));
@@ -559,7 +674,7 @@ int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* 
   res->num_pre = p;
   res->nflag = hst.nflag;
   res->done_early = hst.done;
-  res->launches = launches + (readback_mailbox() ? (kmax > 0 ? 5 : 4) : 0);
+  res->launches = launches + (readback_mailbox() ? (kmax > 0 ? 6 : 5) : 0);
   return ISDF_OK;
 }
 
