@@ -146,19 +146,24 @@ __global__ void __launch_bounds__(256) k_keep_scatter(const double* __restrict__
   }
 }
 
-// Compacted operands Ac, Bc (ntot x p, column-major), residual norms, order.
+// Compacted operands Ac, Bc (ntot x p, column-major with an even leading
+// dimension ld = ntot rounded up, the padding row zero, so that every column
+// starts on a 16-byte boundary), residual norms, order.
 __global__ void k_compact(const double* __restrict__ A, const double* __restrict__ B, long long n,
                           int p, const int* __restrict__ idx, const double* __restrict__ norm2,
                           QrState* st, double* __restrict__ Ac, double* __restrict__ Bc,
                           double* __restrict__ nu, double* __restrict__ nu0, int* __restrict__ pos,
                           int* __restrict__ perm, unsigned char* __restrict__ active) {
   const int ntot = st->ntot;
+  const long long ld = ntot + (ntot & 1);
+  if ((ntot & 1) && blockIdx.x == 0 && threadIdx.x == 0)
+    for (int j = 0; j < p; ++j) Ac[ntot + j * ld] = Bc[ntot + j * ld] = 0.0;
   double mx = 0.0;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ntot; c += gridDim.x * blockDim.x) {
     const long long r = idx[c];
     for (int j = 0; j < p; ++j) {
-      Ac[c + (long long)j * ntot] = A[r + (long long)j * n];
-      Bc[c + (long long)j * ntot] = B[r + (long long)j * n];
+      Ac[c + j * ld] = A[r + (long long)j * n];
+      Bc[c + j * ld] = B[r + (long long)j * n];
     }
     const double v = sqrt(norm2[r]);
     nu[c] = v;
@@ -194,7 +199,7 @@ __global__ void k_argpos(const double* __restrict__ nu, const int* __restrict__ 
 
 // Pivot bookkeeping (one thread) and the pivot's feature vector
 // x[i + j*p] = B(c, i) * A(c, j).
-__global__ void k_pick(int k, int p, int ntot, const double* __restrict__ Ac,
+__global__ void k_pick(int k, int p, int ld, const double* __restrict__ Ac,
                        const double* __restrict__ Bc, int* __restrict__ pos,
                        int* __restrict__ perm, unsigned char* __restrict__ active,
                        int* __restrict__ sel, QrState* st, double* __restrict__ x) {
@@ -224,7 +229,7 @@ __global__ void k_pick(int k, int p, int ntot, const double* __restrict__ Ac,
   const int m = p * p;
   for (int e = threadIdx.x; e < m; e += blockDim.x) {
     const int i = e % p, j = e / p;
-    x[e] = Bc[col + (long long)i * ntot] * Ac[col + (long long)j * ntot];
+    x[e] = Bc[col + (long long)i * ld] * Ac[col + (long long)j * ld];
   }
 }
 
@@ -309,7 +314,8 @@ __global__ void __launch_bounds__(1024) k_normalise(int k, int p, const double* 
 using CoreU = dmma::Core<128, 128>;
 template <int VEC>
 __global__ void __launch_bounds__(256) k_update(const double* __restrict__ Ac,
-                                                const double* __restrict__ Bc, int ntot, int p,
+                                                const double* __restrict__ Bc, int ntot, int ld,
+                                                int p,
                                                 const double* __restrict__ Qm,
                                                 const unsigned char* __restrict__ active,
                                                 double* __restrict__ nu,
@@ -320,7 +326,7 @@ __global__ void __launch_bounds__(256) k_update(const double* __restrict__ Ac,
   const int m_rem = min(CoreU::BM, ntot - m0);
   CoreU core;
   core.zero();
-  core.run<VEC>(smem, Bc + m0, ntot, Qm, p, m_rem, p, 0, p);
+  core.run<VEC>(smem, Bc + m0, ld, Qm, p, m_rem, p, 0, p);
   // row dot with A, reduced over the 4 lanes of a quad and the 4 column warps
   double* red = smem;  // [4][128], the pipeline buffers are free again
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -336,8 +342,8 @@ __global__ void __launch_bounds__(256) k_update(const double* __restrict__ Ac,
 #pragma unroll
         for (int j = 0; j < CoreU::NT; ++j) {
           const int c = wn0 + j * 8 + 2 * t;
-          if (c < p) s = fma(Ac[(m0 + r) + (long long)c * ntot], core.acc[i][j][2 * h], s);
-          if (c + 1 < p) s = fma(Ac[(m0 + r) + (long long)(c + 1) * ntot], core.acc[i][j][2 * h + 1], s);
+          if (c < p) s = fma(Ac[(m0 + r) + (long long)c * ld], core.acc[i][j][2 * h], s);
+          if (c + 1 < p) s = fma(Ac[(m0 + r) + (long long)(c + 1) * ld], core.acc[i][j][2 * h + 1], s);
         }
       }
       s += __shfl_xor_sync(0xffffffffu, s, 1);
@@ -371,7 +377,8 @@ __global__ void __launch_bounds__(256) k_update(const double* __restrict__ Ac,
 }
 
 // The same downdate on the warp-specialised tile (16-byte aligned Bc and Qm,
-// ntot and p even): 64 rows x BN columns (BN >= p, a multiple of 8, the
+// p even; the even leading dimension lets the last odd row copy its zero
+// padding partner): 64 rows x BN columns (BN >= p, a multiple of 8, the
 // columns past p copied as zeros), four DMMA warps of 16 full rows each, so
 // the row dot with A closes inside a quad of lanes. BN tracks p instead of a
 // fixed 128-wide tile, so no tensor-core work is spent on padding beyond the
@@ -381,7 +388,8 @@ using UpdTile = dmma::WsTile<64, BN, 4, 1, 16, 3>;
 
 template <int BN, int MINB>
 __global__ void __launch_bounds__(UpdTile<BN>::THREADS, MINB)
-    k_update_ws(const double* __restrict__ Ac, const double* __restrict__ Bc, int ntot, int p,
+    k_update_ws(const double* __restrict__ Ac, const double* __restrict__ Bc, int ntot, int ld,
+                int p,
                 const double* __restrict__ Qm, const unsigned char* __restrict__ active,
                 double* __restrict__ nu, double* __restrict__ nu0, QrState* st, int* err) {
   using T = UpdTile<BN>;
@@ -390,7 +398,7 @@ __global__ void __launch_bounds__(UpdTile<BN>::THREADS, MINB)
   const int m0 = blockIdx.x * T::BM;
   const int m_rem = min(T::BM, ntot - m0);
   T tile;
-  if (!tile.run(smem, Bc + m0, ntot, m_rem, Qm, p, p, p, err)) return;
+  if (!tile.run(smem, Bc + m0, ld, (m_rem + 1) & ~1, Qm, p, p, p, err)) return;
   if (T::producer()) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
@@ -403,8 +411,8 @@ __global__ void __launch_bounds__(UpdTile<BN>::THREADS, MINB)
 #pragma unroll
       for (int j = 0; j < T::NT; ++j) {
         const int c = j * 8 + 2 * t;
-        if (c < p) s = fma(Ac[(m0 + r) + (long long)c * ntot], tile.acc[0][j][2 * h], s);
-        if (c + 1 < p) s = fma(Ac[(m0 + r) + (long long)(c + 1) * ntot], tile.acc[0][j][2 * h + 1], s);
+        if (c < p) s = fma(Ac[(m0 + r) + (long long)c * ld], tile.acc[0][j][2 * h], s);
+        if (c + 1 < p) s = fma(Ac[(m0 + r) + (long long)(c + 1) * ld], tile.acc[0][j][2 * h + 1], s);
       }
     }
     s += __shfl_xor_sync(0xffffffffu, s, 1);
@@ -499,8 +507,8 @@ QrBuffers carve(Arena& a, long long n, int p, int k1, int k2, int kmax) {
   b.A = a.take<double>((size_t)n * p);
   b.B = a.take<double>((size_t)n * p);
   b.norm2 = a.take<double>((size_t)n);
-  b.Ac = a.take<double>((size_t)n * p);
-  b.Bc = a.take<double>((size_t)n * p);
+  b.Ac = a.take<double>((size_t)(n + 1) * p);  // leading dimension up to n + 1 (even)
+  b.Bc = a.take<double>((size_t)(n + 1) * p);
   b.nu = a.take<double>((size_t)n);
   b.nu0 = a.take<double>((size_t)n);
   b.Q = a.take<double>((size_t)m * kmax);
@@ -547,22 +555,22 @@ int set_update_attrs() {
 }
 
 template <int BN, int MINB>
-void launch_update_bn(const QrBuffers& b, int ntot, int p, cudaStream_t s) {
+void launch_update_bn(const QrBuffers& b, int ntot, int ld, int p, cudaStream_t s) {
   using T = UpdTile<BN>;
   const unsigned grid = (unsigned)((ntot + T::BM - 1) / T::BM);
-  k_update_ws<BN, MINB><<<grid, T::THREADS, T::SMEM_BYTES, s>>>(b.Ac, b.Bc, ntot, p, b.Qm,
-                                                               b.active, b.nu, b.nu0, b.st, b.err);
+  k_update_ws<BN, MINB><<<grid, T::THREADS, T::SMEM_BYTES, s>>>(
+      b.Ac, b.Bc, ntot, ld, p, b.Qm, b.active, b.nu, b.nu0, b.st, b.err);
 }
 
 // The downdate on the narrowest warp-specialised tile that holds p columns.
-void launch_update_ws(const QrBuffers& b, int ntot, int p, cudaStream_t s) {
-  if (p <= 32) launch_update_bn<32, 3>(b, ntot, p, s);
-  else if (p <= 48) launch_update_bn<48, 3>(b, ntot, p, s);
-  else if (p <= 64) launch_update_bn<64, 3>(b, ntot, p, s);
-  else if (p <= 80) launch_update_bn<80, 3>(b, ntot, p, s);
-  else if (p <= 96) launch_update_bn<96, 3>(b, ntot, p, s);
-  else if (p <= 112) launch_update_bn<112, 2>(b, ntot, p, s);
-  else launch_update_bn<128, 2>(b, ntot, p, s);
+void launch_update_ws(const QrBuffers& b, int ntot, int ld, int p, cudaStream_t s) {
+  if (p <= 32) launch_update_bn<32, 3>(b, ntot, ld, p, s);
+  else if (p <= 48) launch_update_bn<48, 3>(b, ntot, ld, p, s);
+  else if (p <= 64) launch_update_bn<64, 3>(b, ntot, ld, p, s);
+  else if (p <= 80) launch_update_bn<80, 3>(b, ntot, ld, p, s);
+  else if (p <= 96) launch_update_bn<96, 3>(b, ntot, ld, p, s);
+  else if (p <= 112) launch_update_bn<112, 2>(b, ntot, ld, p, s);
+  else launch_update_bn<128, 2>(b, ntot, ld, p, s);
 }
 
 }  // namespace
@@ -633,13 +641,14 @@ int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* 
   res->ntot_mg = ntot;
 
   // pivoted Gram-Schmidt over the kept columns
+  const int ld = ntot + (ntot & 1);  // Ac / Bc leading dimension (k_compact)
   const unsigned ugrid = (unsigned)((ntot + CoreU::BM - 1) / CoreU::BM);
   const bool uv2 = ((reinterpret_cast<size_t>(b.Bc) | reinterpret_cast<size_t>(b.Qm)) & 15) == 0 &&
-                   ntot % 2 == 0 && p % 2 == 0;
+                   p % 2 == 0;
   const unsigned agrid = (unsigned)std::min(kNumSMs * 8, (ntot + 255) / 256);
   for (int k = 0; k < kmax; ++k) {
     k_argpos<<<agrid, 256, 0, s>>>(b.nu, b.pos, b.active, ntot, b.st);
-    k_pick<<<1, 1024, 0, s>>>(k, p, ntot, b.Ac, b.Bc, b.pos, b.perm, b.active, b.sel, b.st, b.x);
+    k_pick<<<1, 1024, 0, s>>>(k, p, ld, b.Ac, b.Bc, b.pos, b.perm, b.active, b.sel, b.st, b.x);
     launches += 2;
     if (k > 0) {
       for (int pass = 0; pass < 2; ++pass) {
@@ -650,9 +659,9 @@ int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* 
     }
     k_normalise<<<1, 1024, 0, s>>>(k, p, b.x, b.st, b.Q, b.Qm);
     if (uv2)  // 16-byte aligned rows: the warp-specialised tile
-      launch_update_ws(b, ntot, p, s);
+      launch_update_ws(b, ntot, ld, p, s);
     else
-      k_update<1><<<ugrid, 256, CoreU::SMEM_BYTES, s>>>(b.Ac, b.Bc, ntot, p, b.Qm, b.active, b.nu,
+      k_update<1><<<ugrid, 256, CoreU::SMEM_BYTES, s>>>(b.Ac, b.Bc, ntot, ld, p, b.Qm, b.active, b.nu,
                                                         b.nu0, b.st);
     launches += 2;
     if ((k & 255) == 255) ISDF_CHECK_LAUNCH();
