@@ -244,6 +244,7 @@ __global__ void __launch_bounds__(256) k_qt_x(const double* __restrict__ Q, int 
   __shared__ double red[8];
   const double* q = Q + (long long)l * m;
   double s = 0.0;
+#pragma unroll 4
   for (int i = threadIdx.x; i < m; i += 256) s = fma(q[i], x[i], s);
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -266,8 +267,10 @@ __global__ void __launch_bounds__(256) k_x_minus_qc(const double* __restrict__ Q
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = blockIdx.x * 32 + lane;
   double s = 0.0;
-  if (i < m)
+  if (i < m) {
+#pragma unroll 8
     for (int l = w; l < k; l += 8) s = fma(Q[i + (long long)l * m], cdot[l], s);
+  }
   red[w][lane] = s;
   __syncthreads();
   if (w == 0 && i < m) {
@@ -378,13 +381,18 @@ __global__ void __launch_bounds__(256) k_update(const double* __restrict__ Ac,
 
 // The same downdate on the warp-specialised tile (16-byte aligned Bc and Qm,
 // p even; the even leading dimension lets the last odd row copy its zero
-// padding partner): 64 rows x BN columns (BN >= p, a multiple of 8, the
-// columns past p copied as zeros), four DMMA warps of 16 full rows each, so
-// the row dot with A closes inside a quad of lanes. BN tracks p instead of a
-// fixed 128-wide tile, so no tensor-core work is spent on padding beyond the
-// next multiple of 16.
+// padding partner): 64 rows x BN columns, BN = p rounded up to a multiple of
+// 8 (the columns past p copied as zeros), four DMMA warps of 16 full rows
+// each, so the row dot with A closes inside a quad of lanes. BN tracks p
+// instead of a fixed 128-wide tile: at most 7 padding columns take
+// tensor-core work.
 template <int BN>
 using UpdTile = dmma::WsTile<64, BN, 4, 1, 16, 3>;
+// three CTAs per SM while the accumulators leave room (136 registers)
+template <int BN>
+struct UpdMinBlocks {
+  static constexpr int value = BN <= 96 ? 3 : 2;
+};
 
 template <int BN, int MINB>
 __global__ void __launch_bounds__(UpdTile<BN>::THREADS, MINB)
@@ -538,39 +546,58 @@ int set_update_attrs() {
                                  (int)CoreU::SMEM_BYTES));
   ISDF_CUDA(cudaFuncSetAttribute(k_update<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)CoreU::SMEM_BYTES));
-#define ISDF_UPD_ATTR(BN, MINB)                                                              \
-  ISDF_CUDA(cudaFuncSetAttribute(k_update_ws<BN, MINB>,                                      \
+#define ISDF_UPD_ATTR(BN)                                                                  \
+  ISDF_CUDA(cudaFuncSetAttribute(k_update_ws<BN, UpdMinBlocks<BN>::value>,                   \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                \
                                  (int)UpdTile<BN>::SMEM_BYTES))
-  ISDF_UPD_ATTR(32, 3);
-  ISDF_UPD_ATTR(48, 3);
-  ISDF_UPD_ATTR(64, 3);
-  ISDF_UPD_ATTR(80, 3);
-  ISDF_UPD_ATTR(96, 3);
-  ISDF_UPD_ATTR(112, 2);
-  ISDF_UPD_ATTR(128, 2);
+  ISDF_UPD_ATTR(16);
+  ISDF_UPD_ATTR(24);
+  ISDF_UPD_ATTR(32);
+  ISDF_UPD_ATTR(40);
+  ISDF_UPD_ATTR(48);
+  ISDF_UPD_ATTR(56);
+  ISDF_UPD_ATTR(64);
+  ISDF_UPD_ATTR(72);
+  ISDF_UPD_ATTR(80);
+  ISDF_UPD_ATTR(88);
+  ISDF_UPD_ATTR(96);
+  ISDF_UPD_ATTR(104);
+  ISDF_UPD_ATTR(112);
+  ISDF_UPD_ATTR(120);
+  ISDF_UPD_ATTR(128);
 #undef ISDF_UPD_ATTR
   if (dev >= 0 && dev < 64) done[dev] = true;
   return ISDF_OK;
 }
 
-template <int BN, int MINB>
+template <int BN>
 void launch_update_bn(const QrBuffers& b, int ntot, int ld, int p, cudaStream_t s) {
   using T = UpdTile<BN>;
   const unsigned grid = (unsigned)((ntot + T::BM - 1) / T::BM);
-  k_update_ws<BN, MINB><<<grid, T::THREADS, T::SMEM_BYTES, s>>>(
+  k_update_ws<BN, UpdMinBlocks<BN>::value><<<grid, T::THREADS, T::SMEM_BYTES, s>>>(
       b.Ac, b.Bc, ntot, ld, p, b.Qm, b.active, b.nu, b.nu0, b.st, b.err);
 }
 
-// The downdate on the narrowest warp-specialised tile that holds p columns.
+// The downdate on the narrowest warp-specialised tile that holds p columns
+// (p rounded up to a multiple of 8).
 void launch_update_ws(const QrBuffers& b, int ntot, int ld, int p, cudaStream_t s) {
-  if (p <= 32) launch_update_bn<32, 3>(b, ntot, ld, p, s);
-  else if (p <= 48) launch_update_bn<48, 3>(b, ntot, ld, p, s);
-  else if (p <= 64) launch_update_bn<64, 3>(b, ntot, ld, p, s);
-  else if (p <= 80) launch_update_bn<80, 3>(b, ntot, ld, p, s);
-  else if (p <= 96) launch_update_bn<96, 3>(b, ntot, ld, p, s);
-  else if (p <= 112) launch_update_bn<112, 2>(b, ntot, ld, p, s);
-  else launch_update_bn<128, 2>(b, ntot, ld, p, s);
+  switch ((p + 7) / 8) {
+    case 0: case 1: case 2: launch_update_bn<16>(b, ntot, ld, p, s); break;
+    case 3: launch_update_bn<24>(b, ntot, ld, p, s); break;
+    case 4: launch_update_bn<32>(b, ntot, ld, p, s); break;
+    case 5: launch_update_bn<40>(b, ntot, ld, p, s); break;
+    case 6: launch_update_bn<48>(b, ntot, ld, p, s); break;
+    case 7: launch_update_bn<56>(b, ntot, ld, p, s); break;
+    case 8: launch_update_bn<64>(b, ntot, ld, p, s); break;
+    case 9: launch_update_bn<72>(b, ntot, ld, p, s); break;
+    case 10: launch_update_bn<80>(b, ntot, ld, p, s); break;
+    case 11: launch_update_bn<88>(b, ntot, ld, p, s); break;
+    case 12: launch_update_bn<96>(b, ntot, ld, p, s); break;
+    case 13: launch_update_bn<104>(b, ntot, ld, p, s); break;
+    case 14: launch_update_bn<112>(b, ntot, ld, p, s); break;
+    case 15: launch_update_bn<120>(b, ntot, ld, p, s); break;
+    default: launch_update_bn<128>(b, ntot, ld, p, s); break;
+  }
 }
 
 }  // namespace
