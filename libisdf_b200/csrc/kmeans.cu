@@ -291,15 +291,12 @@ __device__ void block_inclusive_scan(int* a, int n, int* warp_tot) {
   __syncthreads();
 }
 
-// Centroids into the cell grid (cell_start, cell_cen), then the starts of
-// the per-cell neighbourhood lists (nb_start: for every cell, the number of
-// centroids in the up to 27 cells around it, scanned) that k_nb_fill fills.
+// Centroids into the cell grid (cell_start, cell_cen).
 __global__ void __launch_bounds__(1024) k_build_cells(const double4* __restrict__ cen,
                                                       const KmState* st, CellGrid g,
                                                       int* __restrict__ cell_start,
                                                       double4* __restrict__ cell_cen,
-                                                      int* __restrict__ cell_of,
-                                                      int* __restrict__ nb_start) {
+                                                      int* __restrict__ cell_of) {
   if (st->done) return;
   extern __shared__ int sc[];  // ncells + 1 counters
   __shared__ int warp_tot[32];
@@ -320,68 +317,12 @@ __global__ void __launch_bounds__(1024) k_build_cells(const double4* __restrict_
   block_inclusive_scan(sc + 1, ncells, warp_tot);
   for (int c = threadIdx.x; c <= ncells; c += blockDim.x) cell_start[c] = sc[c];
   __syncthreads();
-  // neighbourhood sizes from the cell starts (before the placement below
-  // turns sc into running offsets)
-  if (nb_start) {
-    for (int c = threadIdx.x; c < ncells; c += blockDim.x) {
-      const int ci = c % nc, cj = (c / nc) % nc, ck = c / (nc * nc);
-      int cnt = 0;
-      for (int dk = -1; dk <= 1; ++dk)
-        for (int dj = -1; dj <= 1; ++dj)
-          for (int di = -1; di <= 1; ++di) {
-            const int ni = ci + di, nj = cj + dj, nk = ck + dk;
-            if (ni < 0 || ni >= nc || nj < 0 || nj >= nc || nk < 0 || nk >= nc) continue;
-            const int id = ni + nc * (nj + nc * nk);
-            cnt += sc[id + 1] - sc[id];
-          }
-      nb_start[c + 1] = cnt;
-    }
-    if (threadIdx.x == 0) nb_start[0] = 0;
-  }
-  __syncthreads();
   // placement inside a cell is arbitrary: the search compares (d, index) pairs
   for (int j = threadIdx.x; j < rk; j += blockDim.x) {
     const int slot = atomicAdd(&sc[cell_of[j]], 1);
     const double4 c = cen[j];
     cell_cen[slot] = make_double4(c.x, c.y, c.z, (double)j);
   }
-  if (nb_start) {
-    __syncthreads();
-    for (int c = threadIdx.x; c < ncells; c += blockDim.x) sc[c] = nb_start[c + 1];
-    __syncthreads();
-    block_inclusive_scan(sc, ncells, warp_tot);
-    for (int c = threadIdx.x; c < ncells; c += blockDim.x) nb_start[c + 1] = sc[c];
-  }
-}
-
-// nb_cen[nb_start[c] ..) = the centroids (x, y, z, index) of the up to 27
-// cells around cell c: one warp per cell, one lane per neighbouring cell.
-__global__ void __launch_bounds__(256) k_nb_fill(const KmState* st, CellGrid g,
-                                                 const int* __restrict__ cell_start,
-                                                 const double4* __restrict__ cell_cen,
-                                                 const int* __restrict__ nb_start,
-                                                 double4* __restrict__ nb_cen) {
-  if (st->done) return;
-  const int nc = g.nc, ncells = nc * nc * nc;
-  const int c = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (c >= ncells) return;
-  const int ci = c % nc, cj = (c / nc) % nc, ck = c / (nc * nc);
-  int s0 = 0, cnt = 0;
-  if (lane < 27) {
-    const int ni = ci + lane % 3 - 1, nj = cj + (lane / 3) % 3 - 1, nk = ck + lane / 9 - 1;
-    if (ni >= 0 && ni < nc && nj >= 0 && nj < nc && nk >= 0 && nk < nc) {
-      const int id = ni + nc * (nj + nc * nk);
-      s0 = cell_start[id];
-      cnt = cell_start[id + 1] - s0;
-    }
-  }
-  int incl = cnt;
-  for (int o = 1; o < 32; o <<= 1) {
-    const int u = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += u;
-  }
-  double4* dst = nb_cen + nb_start[c] + (incl - cnt);
-  for (int q = 0; q < cnt; ++q) dst[q] = cell_cen[s0 + q];
 }
 
 // Squared distance in the reference's rounding (pdist2, utility.cpp:598-615).
@@ -479,9 +420,8 @@ __device__ __forceinline__ int ring_search(double x, double y, double z, int old
 // Per point, once per selection (the points do not move): its cell and the
 // distances from it to the outside of the 3^3 and 5^3 cell blocks around it
 // (rounded down, less the binning tolerance; infinite where a block reaches
-// the domain's faces), which the distance-bound test and the neighbourhood
-// search read instead of recomputing three divisions and twelve face
-// distances every iteration.
+// the domain's faces), which the distance-bound test reads instead of
+// recomputing three divisions and twelve face distances every iteration.
 __global__ void k_point_cells(const double* __restrict__ px, const double* __restrict__ py,
                               const double* __restrict__ pz, int n, CellGrid g,
                               int* __restrict__ pcell, double2* __restrict__ pd12) {
@@ -509,49 +449,6 @@ __global__ void k_point_cells(const double* __restrict__ px, const double* __res
   pd12[p] = make_double2(D1 * kRoundDown - g.tol, D2 * kRoundDown - g.tol);
 }
 
-// The search over the point's cell neighbourhood list (the centroids of the
-// up to 27 cells around it, one contiguous run, so the lanes of a warp,
-// which mostly share a cell, loop in step): every centroid outside those
-// cells lies beyond the block's inner faces, at least D1 away (k_point_cells;
-// tol covers the binning of centroids near a face). When the best distance is
-// below D1 the result is certified as the ring search's is; otherwise the
-// ring search runs.
-__device__ __forceinline__ int nb_search(double x, double y, double z, int cell, double D1,
-                                         int old, int rk, const double4* __restrict__ cen,
-                                         const int* __restrict__ nb_start,
-                                         const double4* __restrict__ nb_cen,
-                                         const int* __restrict__ cell_start,
-                                         const double4* __restrict__ cell_cen,
-                                         const CellGrid& g, double2* bnd_p) {
-  const double inf = __longlong_as_double(0x7ff0000000000000LL);
-  double best = inf;
-  int bj = 0x7fffffff;
-  if (old >= 0 && old < rk) {
-    best = ref_dist2(x, y, z, cen[old]);
-    bj = old;
-  }
-  double second = inf;
-  const int e = nb_start[cell + 1];
-  for (int q = nb_start[cell]; q < e; ++q) {
-    const double4 c = nb_cen[q];
-    const double d = ref_dist2(x, y, z, c);
-    const int j = (int)c.w;
-    if (d < best || (d == best && j < bj)) {
-      if (j != bj) second = best;
-      best = d;
-      bj = j;
-    } else if (j != bj) {
-      second = fmin(second, d);
-    }
-  }
-  const double floor2 = D1 * D1 * (1.0 - 2e-14);
-  if (!(D1 > 0.0 && floor2 > best))
-    return ring_search(x, y, z, old, rk, cen, cell_start, cell_cen, g, bnd_p);
-  *bnd_p = make_double2(__dmul_ru(__dsqrt_ru(best), kRoundUp),
-                        __dmul_rd(__dsqrt_rd(fmin(second, floor2)), kRoundDown));
-  return bj;
-}
-
 // Two phases per block: every thread tests its point against its distance
 // bounds; the points that fail are appended (warp order kept) to a block
 // list, which the block's threads then search together, so the divergent
@@ -562,7 +459,6 @@ __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
     const double4* __restrict__ cell_cen, CellGrid g, AssignMap am, KmState* st,
     int* __restrict__ label, int count, double2* __restrict__ bnd,
     const double* __restrict__ shift, const float* __restrict__ nbshift,
-    const int* __restrict__ nb_start, const double4* __restrict__ nb_cen,
     const int* __restrict__ pcell, const double2* __restrict__ pd12) {
   if (st->done) return;
   __shared__ int list_p[kAssignThreads], list_old[kAssignThreads];
@@ -618,10 +514,7 @@ __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
   int changed = 0;
   for (int i = threadIdx.x; i < ln; i += blockDim.x) {
     const int q = list_p[i], o = list_old[i];
-    const int bj = nb_start ? nb_search(px[q], py[q], pz[q], pcell[q], pd12[q].x, o, rk, cen,
-                                        nb_start, nb_cen, cell_start, cell_cen, g, &bnd[q])
-                            : ring_search(px[q], py[q], pz[q], o, rk, cen, cell_start, cell_cen,
-                                          g, &bnd[q]);
+    const int bj = ring_search(px[q], py[q], pz[q], o, rk, cen, cell_start, cell_cen, g, &bnd[q]);
     if (count && o != bj) ++changed;
     label[q] = bj;
   }
@@ -1088,8 +981,6 @@ struct KmBuffers {
   KmState* st;
   int* cell_start;
   double4* cell_cen;
-  int* nb_start;     // per cell: start of its neighbourhood list in nb_cen
-  double4* nb_cen;   // the centroids of the up to 27 cells around each cell
   int* pcell;        // per point: its cell
   double2* pd12;     // per point: distances to the outside of its 3^3 / 5^3 cell blocks
   int* cell_of;
@@ -1124,8 +1015,6 @@ KmBuffers carve(Arena& a, int n, int mu) {
   b.cell_start = a.take<int>((size_t)kMaxCells + 1);
   b.cell_cen = a.take<double4>(mu);
   b.cell_of = a.take<int>(mu);
-  b.nb_start = a.take<int>((size_t)kMaxCells + 1);
-  b.nb_cen = a.take<double4>((size_t)27 * mu);  // every centroid in at most 27 lists
   b.pcell = a.take<int>(n);
   b.pd12 = a.take<double2>(n);
   return b;
@@ -1235,7 +1124,6 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     cg.tol = 1e-9 * lmax;
   }
   const size_t cell_smem = sizeof(int) * ((size_t)cg.nc * cg.nc * cg.nc + 1);
-  const unsigned nb_blocks = (unsigned)((cg.nc * cg.nc * cg.nc + 7) / 8);
   AssignMap am{};
   am.nx = args.num_grid[0];
   am.ny = args.num_grid[1];
@@ -1256,11 +1144,11 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
                                   : grid_for(n, kAssignThreads);
   k_point_cells<<<grid_for(n, 256), 256, 0, stream>>>(b.px, b.py, b.pz, n, cg, b.pcell, b.pd12);
   k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
-                                                b.cell_of, nullptr);
+                                                b.cell_of);
   k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.cell_start,
                                                       b.cell_cen, cg, am, b.st, b.label, 0,
-                                                      b.bnd, b.shift, b.nbshift, nullptr,
-                                                      nullptr, b.pcell, b.pd12);
+                                                      b.bnd, b.shift, b.nbshift, b.pcell,
+                                                      b.pd12);
   ISDF_CHECK_LAUNCH();
 
   const size_t cmax_smem = 3 * sizeof(unsigned) * ((size_t)cg.nc * cg.nc * cg.nc);
@@ -1270,7 +1158,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
   ISDF_TRY(set_kmeans_smem_attrs());
   int chunks = 0;
   const int max_chunks = args.max_iter / kIterChunk + 2;
-  // One chunk = kIterChunk Lloyd iterations (11 launches each; every kernel
+  // One chunk = kIterChunk Lloyd iterations (10 launches each; every kernel
   // returns at once when the loop has stopped). The chunk is captured once
   // into a CUDA graph and replayed, which removes the per-launch host cost
   // that dominates small solves; direct launches are the fallback when the
@@ -1288,13 +1176,11 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
       k_centroids<<<1, 1024, cmax_smem, stream>>>(b.sums, b.st, b.cen, b.shift, b.cell_of, cg,
                                                   b.nbshift);
       k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
-                                                    b.cell_of, b.nb_start);
-      k_nb_fill<<<nb_blocks, 256, 0, stream>>>(b.st, cg, b.cell_start, b.cell_cen, b.nb_start,
-                                               b.nb_cen);
+                                                    b.cell_of);
       k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen,
                                                           b.cell_start, b.cell_cen, cg, am, b.st,
                                                           b.label, 1, b.bnd, b.shift, b.nbshift,
-                                                          b.nb_start, b.nb_cen, b.pcell, b.pd12);
+                                                          b.pcell, b.pd12);
       k_iter_end<<<1, 1, 0, stream>>>(b.st);
     }
   };
@@ -1328,7 +1214,8 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
   res->search_frac = (double)hst.searches / ((double)n * (hst.s + 1));
   // + the state, per-chunk and selection reads through the mapped mailbox
   res->launches =
-      4 + 4 + (chunks + 1) * kIterChunk * 11 + 2 + (readback_mailbox() ? chunks + 3 : 0);
+      4 + 4 + (am.g2p ? 1 : 0) + (chunks + 1) * kIterChunk * 10 + 2 +
+      (readback_mailbox() ? chunks + 3 : 0);
   const int rk = hst.rk;
 
   dim3 fgrid((unsigned)((rk + 127) / 128), (unsigned)nchunks);
