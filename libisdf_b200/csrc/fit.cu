@@ -395,9 +395,7 @@ int set_smem_attrs() {
   ISDF_TRY(set_attr(k_gemm_z<0, 1>, CoreZ::SMEM_BYTES));
   ISDF_TRY(set_attr(k_gemm_z<1, 1>, CoreZ::SMEM_BYTES));
   ISDF_TRY(set_attr(k_gemm_z<2, 1>, CoreZ::SMEM_BYTES));
-  ISDF_TRY(set_attr(k_gemm_z<0, 2>, CoreZ::SMEM_BYTES));
   ISDF_TRY(set_attr(k_gemm_z<1, 2>, CoreZ::SMEM_BYTES));
-  ISDF_TRY(set_attr(k_gemm_z<2, 2>, CoreZ::SMEM_BYTES));
   ISDF_TRY(set_attr(k_chol_update<1>, CoreZ::SMEM_BYTES));
   ISDF_TRY(set_attr(k_chol_update<2>, CoreZ::SMEM_BYTES));
   ISDF_TRY(set_attr(k_chol_panel<1>, CoreN::SMEM_BYTES));

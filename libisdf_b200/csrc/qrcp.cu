@@ -544,8 +544,6 @@ int set_update_attrs() {
   if (dev >= 0 && dev < 64 && done[dev]) return ISDF_OK;
   ISDF_CUDA(cudaFuncSetAttribute(k_update<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)CoreU::SMEM_BYTES));
-  ISDF_CUDA(cudaFuncSetAttribute(k_update<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)CoreU::SMEM_BYTES));
 #define ISDF_UPD_ATTR(BN)                                                                  \
   ISDF_CUDA(cudaFuncSetAttribute(k_update_ws<BN, UpdMinBlocks<BN>::value>,                   \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                \
