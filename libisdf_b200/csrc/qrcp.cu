@@ -257,25 +257,25 @@ __global__ void __launch_bounds__(256) k_qt_x(const double* __restrict__ Q, int 
 }
 
 // x -= Q[:, 0:k] cdot: a block takes 32 consecutive rows (one per lane), its
-// eight warps the columns l = w (mod 8), and the eight partials are added in
-// warp order.
-__global__ void __launch_bounds__(256) k_x_minus_qc(const double* __restrict__ Q, int m, int k,
-                                                    const double* __restrict__ cdot,
-                                                    const QrState* st, double* __restrict__ x) {
+// 32 warps the columns l = w (mod 32), and the 32 partials are added in warp
+// order (enough loads in flight per SM to stream Q from L2).
+__global__ void __launch_bounds__(1024) k_x_minus_qc(const double* __restrict__ Q, int m, int k,
+                                                     const double* __restrict__ cdot,
+                                                     const QrState* st, double* __restrict__ x) {
   if (st->done) return;
-  __shared__ double red[8][32];
+  __shared__ double red[32][33];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int i = blockIdx.x * 32 + lane;
   double s = 0.0;
   if (i < m) {
-#pragma unroll 8
-    for (int l = w; l < k; l += 8) s = fma(Q[i + (long long)l * m], cdot[l], s);
+#pragma unroll 4
+    for (int l = w; l < k; l += 32) s = fma(Q[i + (long long)l * m], cdot[l], s);
   }
   red[w][lane] = s;
   __syncthreads();
   if (w == 0 && i < m) {
     double v = red[0][lane];
-    for (int u = 1; u < 8; ++u) v += red[u][lane];
+    for (int u = 1; u < 32; ++u) v += red[u][lane];
     x[i] -= v;
   }
 }
@@ -678,7 +678,7 @@ int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* 
     if (k > 0) {
       for (int pass = 0; pass < 2; ++pass) {
         k_qt_x<<<k, 256, 0, s>>>(b.Q, m, k, b.x, b.st, b.cdot);
-        k_x_minus_qc<<<(m + 31) / 32, 256, 0, s>>>(b.Q, m, k, b.cdot, b.st, b.x);
+        k_x_minus_qc<<<(m + 31) / 32, 1024, 0, s>>>(b.Q, m, k, b.cdot, b.st, b.x);
         launches += 2;
       }
     }
