@@ -43,7 +43,7 @@ def test_select_matches_reference(torch_cuda, name):
 
 
 def test_select_si8_synthetic_matches_oracle(torch_cuda):
-    """BASELINE config-0 shape: 40^3 grid, 32 states, mu = 320, 100 iterations."""
+    """Si8-like shape: 40^3 grid, 32 states, mu = 320, 100 iterations."""
     torch = torch_cuda
     s = synth.SI8
     psi = synth.shape_orbitals(s, 0)

@@ -1,6 +1,6 @@
 """Mixed-precision form (INT8-sliced tcgen05 GEMMs, FP64 Cholesky and
 triangular inverse) against the FP64 form and the FP64 oracle. The bar is
-the north star's: fitted pair densities (theta C) within 1e-6 relative of the
+the mixed form's accuracy target: fitted pair densities (theta C) within 1e-6 relative of the
 FP64 result; piv is identical (K-means stays FP64)."""
 import numpy as np
 import pytest

@@ -71,7 +71,7 @@ def test_qrcp_pivots_match_oracle(torch_cuda, name, mu, factor, seed):
 
 
 def test_qrcp_si8_synthetic(torch_cuda):
-    """BASELINE config-0 shape with the QRCP selector (40^3, 32 states, mu = 320)."""
+    """Si8-like shape with the QRCP selector (40^3, 32 states, mu = 320)."""
     s = synth.SI8
     psi = synth.shape_orbitals(s, 2)
     a = (s.nocc, s.nv1, s.nc1, s.nv2, s.nc2)
