@@ -31,8 +31,9 @@ def test_check_reproduces_reference_numbers(torch_cuda, name):
 
 
 def test_check_inside_isdf_si8(torch_cuda):
-    """Si8-like shape (40^3 grid, 32 states, mu = 320), check = true: the report carries both errors,
-    equal to the numpy restatement's on the same theta."""
+    """Si8-like shape (40^3 grid, 32 states, mu = 320), check = true: the
+    report carries both errors, equal to the numpy restatement's on the same
+    theta."""
     torch = torch_cuda
     s = synth.SI8
     psi = synth.shape_orbitals(s, 0)
