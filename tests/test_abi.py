@@ -63,3 +63,34 @@ def test_cxx_header_compiles():
     r = subprocess.run(["g++", "-std=c++14", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
                         "-x", "c++", "-"], input=src.encode(), capture_output=True)
     assert r.returncode == 0, r.stderr.decode()
+
+
+_STRUCTS = [("isdf_domain_t", "_Domain"), ("isdf_options_t", "_Options"),
+            ("isdf_report_t", "_Report"), ("isdf_server_config_t", "_ServerConfig"),
+            ("isdf_request_t", "_Request"), ("isdf_server_stats_t", "_ServerStats")]
+
+
+def test_ctypes_structs_match_the_c_layout(tmp_path):
+    """The Python binding's ctypes structures have the size and field offsets
+    that a C compiler gives the structs of include/isdf_c.h (a mismatch would
+    pass garbage across the boundary without any error)."""
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "isdf_c.h"', 'int main(void) {']
+    for c_name, py_name in _STRUCTS:
+        cls = getattr(isdf, py_name)
+        lines.append(f'  printf("{py_name} size %zu\\n", sizeof({c_name}));')
+        for field, _ in cls._fields_:
+            lines.append(f'  printf("{py_name} {field} %zu\\n", offsetof({c_name}, {field}));')
+    lines += ['  return 0;', '}']
+    src = tmp_path / "layout.c"
+    exe = tmp_path / "layout"
+    src.write_text("\n".join(lines) + "\n")
+    r = subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o",
+                        str(exe)], capture_output=True)
+    assert r.returncode == 0, r.stderr.decode()
+    out = subprocess.run([str(exe)], capture_output=True, check=True).stdout.decode().split("\n")
+    c_layout = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for _, py_name in _STRUCTS:
+        cls = getattr(isdf, py_name)
+        assert c_layout[(py_name, "size")] == ctypes.sizeof(cls), py_name
+        for field, _ in cls._fields_:
+            assert c_layout[(py_name, field)] == getattr(cls, field).offset, (py_name, field)
