@@ -57,3 +57,30 @@ def test_port_and_reference_agree_live():
         assert a[1:3] == b[1:3]
         assert np.array_equal(a[0], b[0])
     assert g["piv"].dtype == np.int32
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_port_and_reference_agree_on_random_shapes(seed):
+    """Random odd and even grids, state windows (S1 != S2 included), mu and
+    iteration caps: the port's weights and pivots equal the reference code's
+    bit for bit."""
+    ref = pytest.importorskip("oracle.ref")
+    if not ref.available():
+        pytest.skip("oracle/_ref not built on this machine")
+    rng = np.random.default_rng(100 + seed)
+    ng = tuple(int(x) for x in rng.integers(5, 13, size=3))
+    n = ng[0] * ng[1] * ng[2]
+    nstate = int(rng.integers(4, 10))
+    nocc = int(rng.integers(2, nstate - 1))
+    nv1, nv2 = int(rng.integers(1, nocc + 1)), int(rng.integers(1, nocc + 1))
+    nc1, nc2 = int(rng.integers(0, nstate - nocc + 1)), int(rng.integers(0, nstate - nocc + 1))
+    length = tuple(float(x) for x in rng.uniform(5.0, 12.0, size=3))
+    mu = int(rng.integers(4, min(64, n // 4)))
+    iters = int(rng.choice([0, 1, 5, 30]))
+    psi = np.asfortranarray(np.linalg.qr(rng.standard_normal((n, nstate)))[0])
+    w_ref = ref.weight(psi, nocc, nv1, nc1, nv2, nc2)
+    a = ref.kmeans_piv(psi, ng, length, nocc, nv1, nc1, nv2, nc2, mu, iters)
+    b = port.kmeans_piv(psi, ng, length, nocc, nv1, nc1, nv2, nc2, mu, iters)
+    assert np.array_equal(b[3], w_ref)
+    assert a[1:3] == b[1:3]
+    assert np.array_equal(a[0], b[0])
