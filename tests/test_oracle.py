@@ -84,3 +84,30 @@ def test_port_and_reference_agree_on_random_shapes(seed):
     assert np.array_equal(b[3], w_ref)
     assert a[1:3] == b[1:3]
     assert np.array_equal(a[0], b[0])
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_fit_restatement_and_reference_agree_on_random_shapes(seed):
+    """The numpy fit (oracle/fit.py) against the reference's getbasis on random
+    shapes, with pivots from the reference's own K-means: fitted pair densities
+    to 1e-8 (theta itself carries cond(C C^T) x eps)."""
+    ref = pytest.importorskip("oracle.ref")
+    if not ref.available():
+        pytest.skip("oracle/_ref not built on this machine")
+    rng = np.random.default_rng(200 + seed)
+    ng = tuple(int(x) for x in rng.integers(6, 12, size=3))
+    n = ng[0] * ng[1] * ng[2]
+    nstate = int(rng.integers(5, 10))
+    nocc = int(rng.integers(2, nstate - 1))
+    nv1, nv2 = int(rng.integers(1, nocc + 1)), int(rng.integers(1, nocc + 1))
+    nc1, nc2 = int(rng.integers(1, nstate - nocc + 1)), int(rng.integers(1, nstate - nocc + 1))
+    length = tuple(float(x) for x in rng.uniform(5.0, 12.0, size=3))
+    mu = int(rng.integers(8, min(48, (nv1 + nc1) * (nv2 + nc2) + 1)))
+    psi = np.asfortranarray(np.linalg.qr(rng.standard_normal((n, nstate)))[0])
+    piv, rk, _, _ = ref.kmeans_piv(psi, ng, length, nocc, nv1, nc1, nv2, nc2, mu, 10)
+    a = (nocc, nv1, nc1, nv2, nc2)
+    th_ref = ref.getbasis(psi, ng, length, *a, rk, piv)
+    th = ofit.getbasis(psi, *a, rk, piv)
+    fd = ofit.fitted_densities(th, psi, *a, rk, piv)
+    fd_ref = ofit.fitted_densities(th_ref, psi, *a, rk, piv)
+    assert ofit.rel(fd, fd_ref) < 1e-8
