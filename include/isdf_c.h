@@ -58,14 +58,26 @@ typedef struct isdf_domain_t {
 
 typedef struct isdf_options_t {
   int precision;          /* ISDF_PRECISION_* (default FP64) */
-  int refine_steps;       /* mixed precision: FP64 refinement steps (default 2) */
+  int refine_steps;       /* must be 0 (the default): FP64 iterative refinement of the
+                             mixed form's theta solve is not built, because each step
+                             would cost a full Ng x mu x mu product while the mixed
+                             form's fitted densities are already within 1e-6 of FP64;
+                             nonzero returns ISDF_ERR_UNSUPPORTED */
   double qrcp_oversample; /* QRCP sketch width = IRound(sqrt(f * mu)); reference 1.5 */
   long long qrcp_seed;    /* srand48 seed of the QRCP sketch; reference 41 */
   long long rand_seed;    /* >= 0: srand() before K-means (only its npt < mu branch
                              draws from rand()); < 0: keep the process state */
   void* stream;           /* cudaStream_t to run on; NULL = library stream */
   int mixed_slices;       /* mixed precision: base-254 INT8 digits per FP64 operand, 5..7 (default 6) */
-  int reserved[7];
+  int kmeans_warm_start;  /* nonzero: K-means starts from the caller's previous pivots,
+                             piv[0..mu), when piv[0] != piv[1] (an SCF loop passes the
+                             piv of its last solve back in): those with a weight above
+                             the filter threshold, topped up with the first kept grid
+                             points not among them, as the reference's KMEAN does
+                             (src/common/utility.cpp:725-749; its ISDF() zeroes piv
+                             first, isdf.cpp:174-175, so there it never happens).
+                             0 (default): piv is ignored on input, as in the reference */
+  int reserved[6];
 } isdf_options_t;
 
 typedef struct isdf_report_t {
@@ -86,7 +98,12 @@ typedef struct isdf_report_t {
   int kernel_launches; /* kernels this library launched for the solve */
   float t_gemm_ms;     /* GEMM launches of the triangular stage alone (FP64: the whole stage) */
   float kmeans_search_frac; /* share of K-means point assignments that ran the cell search */
-  int reserved[4];
+  int qrcp_steps;           /* QRCP: pivots taken */
+  int qrcp_norm_recomputes; /* QRCP: residual norms recomputed exactly because the
+                               downdate lost accuracy (dgeqpf's cancellation test) */
+  int kmeans_warm_pivots;   /* K-means warm start: previous pivots reused as initial
+                               centroids (-1: cold start) */
+  int reserved[1];
 } isdf_report_t;
 
 /* Fills *opt with the reference's defaults. */
@@ -125,6 +142,7 @@ int isdf_kmeans_select(const isdf_domain_t* dom, const double* d_w, int mu, int 
 int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, int nc1, int nv2,
              int nc2, int rk, const int* piv, double* d_theta, int precision, int refine_steps,
              int* chol_info, void* stream);
+/* (refine_steps must be 0; see isdf_options_t.refine_steps.) */
 
 /* The check of the reference (src/common/checkcode.cpp:54-313, called by
  * src/common/isdf.cpp:193-206 when check = true): the pair-density fit error
@@ -152,9 +170,11 @@ int isdf_check(const isdf_domain_t* dom, const double* d_psi, int nocc, int nsta
  * with a message naming the bytes needed. Every process that loads the
  * library holds the array on each GPU it uses until exit. All calls on a
  * device share the array, so calls that overlap on the GPU race; it keeps
- * the last call's contents (each call clears what must start at zero). The
- * first call on a device looks up the array's address once; make it before
- * any stream capture. stream NULL = the legacy default stream. Synchronous. */
+ * the last call's contents (each call clears what must start at zero). Every
+ * call looks up the array's device address on the current device (a cheap
+ * runtime query, so the address stays right after cudaDeviceReset); the first
+ * call on a device also loads the array's module, so make it before any
+ * stream capture. stream NULL = the legacy default stream. Synchronous. */
 int isdf_fit_noalloc(const double* d_psi, long long ng, int nstate, int nocc, int nv1, int nc1,
                      int nv2, int nc2, int rk, const int* piv, double* d_theta, int* chol_info,
                      void* stream);
@@ -216,10 +236,22 @@ int isdf_server_destroy(void* server);
 const char* isdf_last_error(void);
 const char* isdf_status_string(int code);
 
-/* Device memory the solve needs beyond psi and theta, in bytes (the serving
- * loop admits requests by it). */
+/* Device memory the solve needs beyond psi and theta, in bytes, for the
+ * default QRCP oversampling (1.5) and WITHOUT the check's buffers (their size
+ * depends on the grid's shape, which this signature does not carry): the
+ * `check` argument is ignored. isdf_request_workspace_bytes() gives the full
+ * footprint of one request. */
 size_t isdf_workspace_bytes(long long ng, int nstate, int mu, int selector, int precision,
                             int check);
+
+/* The full device footprint of one isdf_solve() call beyond psi and theta, in
+ * bytes: the selector's, the fit's and (check != 0) the check's buffers for
+ * this grid, state window, mu (0 = the default formula) and options (QRCP
+ * oversampling, precision; opt may be NULL). The serving loop admits requests
+ * by this figure. Returns 0 for invalid arguments. */
+size_t isdf_request_workspace_bytes(const isdf_domain_t* dom, int nstate, int nv1, int nc1,
+                                    int nv2, int nc2, int mu_points, int selector, int check,
+                                    const isdf_options_t* opt);
 
 /* Releases the per-device workspace cached by isdf_solve(). */
 void isdf_release_workspace(void);

@@ -60,7 +60,8 @@ class _Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("refine_steps", ctypes.c_int),
                 ("qrcp_oversample", ctypes.c_double), ("qrcp_seed", ctypes.c_longlong),
                 ("rand_seed", ctypes.c_longlong), ("stream", ctypes.c_void_p),
-                ("mixed_slices", ctypes.c_int), ("reserved", ctypes.c_int * 7)]
+                ("mixed_slices", ctypes.c_int), ("kmeans_warm_start", ctypes.c_int),
+                ("reserved", ctypes.c_int * 6)]
 
 
 class _Report(ctypes.Structure):
@@ -72,7 +73,9 @@ class _Report(ctypes.Structure):
                 ("t_solve_ms", ctypes.c_double), ("t_check_ms", ctypes.c_double),
                 ("t_total_ms", ctypes.c_double), ("chol_info", ctypes.c_int),
                 ("kernel_launches", ctypes.c_int), ("t_gemm_ms", ctypes.c_float),
-                ("kmeans_search_frac", ctypes.c_float), ("reserved", ctypes.c_int * 4)]
+                ("kmeans_search_frac", ctypes.c_float), ("qrcp_steps", ctypes.c_int),
+                ("qrcp_norm_recomputes", ctypes.c_int), ("kmeans_warm_pivots", ctypes.c_int),
+                ("reserved", ctypes.c_int * 1)]
 
 
 class _ServerConfig(ctypes.Structure):
@@ -125,12 +128,13 @@ class Domain:
 @dataclass
 class Options:
     precision: int = PRECISION_FP64
-    refine_steps: int = 2
+    refine_steps: int = 0  # FP64 refinement is not built: nonzero is rejected
     qrcp_oversample: float = 1.5
     qrcp_seed: int = 41
     rand_seed: int = -1
     stream: int = 0
     mixed_slices: int = 6
+    kmeans_warm_start: bool = False  # reuse the caller's previous piv (utility.cpp:725-749)
 
     def _c(self) -> _Options:
         o = _Options()
@@ -141,6 +145,7 @@ class Options:
         o.rand_seed = self.rand_seed
         o.stream = self.stream or None
         o.mixed_slices = self.mixed_slices
+        o.kmeans_warm_start = int(bool(self.kmeans_warm_start))
         return o
 
 
@@ -163,6 +168,9 @@ class Report:
     kernel_launches: int
     t_gemm_ms: float = 0.0
     kmeans_search_frac: float = 0.0
+    qrcp_steps: int = 0
+    qrcp_norm_recomputes: int = 0
+    kmeans_warm_pivots: int = -1
 
 
 _lib = None
@@ -193,6 +201,9 @@ def lib() -> ctypes.CDLL:
         L.isdf_status_string.restype = ctypes.c_char_p
         L.isdf_workspace_bytes.argtypes = [LL, I, I, I, I, I]
         L.isdf_workspace_bytes.restype = ctypes.c_size_t
+        L.isdf_request_workspace_bytes.argtypes = [ctypes.POINTER(_Domain), I, I, I, I, I, I, I,
+                                                   I, ctypes.POINTER(_Options)]
+        L.isdf_request_workspace_bytes.restype = ctypes.c_size_t
         L.isdf_default_options.argtypes = [ctypes.POINTER(_Options)]
         _lib = L
     return _lib
@@ -240,10 +251,7 @@ def ISDF(d_psirow, domain: Domain, nocc: int, nstate: int, nv1: int, nc1: int, n
                           mu_points, _dptr(d_thetaCol), piv.ctypes.data, KmeansMaxIter_ISDF, sel,
                           int(bool(check)), ctypes.byref(o), ctypes.byref(r))
     _check(rc)
-    return Report(r.rk_requested, r.rk_eff, r.kmeans_iters, r.npt, r.fit_err, r.coul_err,
-                  r.t_select_ms, r.t_fit_ms, r.t_zct_ms, r.t_chol_ms, r.t_solve_ms, r.t_check_ms,
-                  r.t_total_ms, r.chol_info, r.kernel_launches, r.t_gemm_ms,
-                  r.kmeans_search_frac)
+    return _report(r)
 
 
 def kmeans_weight(d_psi, ng: int, nstate: int, nocc: int, nv1: int, nc1: int, nv2: int, nc2: int,
@@ -267,7 +275,7 @@ def kmeans_select(domain: Domain, d_w, mu: int, max_iter: int, rand_seed: int = 
 
 
 def fit(d_psi, ng: int, nstate: int, nocc: int, nv1: int, nc1: int, nv2: int, nc2: int, rk: int,
-        piv: np.ndarray, d_theta, precision: int = PRECISION_FP64, refine_steps: int = 2,
+        piv: np.ndarray, d_theta, precision: int = PRECISION_FP64, refine_steps: int = 0,
         stream: int = 0) -> int:
     """theta for given pivots; returns the Cholesky info (0 = ok)."""
     piv = np.ascontiguousarray(piv, dtype=np.int32)
@@ -296,7 +304,8 @@ def _report(r: _Report) -> Report:
     return Report(r.rk_requested, r.rk_eff, r.kmeans_iters, r.npt, r.fit_err, r.coul_err,
                   r.t_select_ms, r.t_fit_ms, r.t_zct_ms, r.t_chol_ms, r.t_solve_ms, r.t_check_ms,
                   r.t_total_ms, r.chol_info, r.kernel_launches, r.t_gemm_ms,
-                  r.kmeans_search_frac)
+                  r.kmeans_search_frac, r.qrcp_steps, r.qrcp_norm_recomputes,
+                  r.kmeans_warm_pivots)
 
 
 class Server:
@@ -384,4 +393,17 @@ class Server:
 
 def workspace_bytes(ng: int, nstate: int, mu: int, selector: int = SELECT_KMEANS,
                     precision: int = PRECISION_FP64, check: bool = False) -> int:
+    """Footprint at the default QRCP oversampling, without the check's buffers."""
     return int(lib().isdf_workspace_bytes(ng, nstate, mu, selector, precision, int(check)))
+
+
+def request_workspace_bytes(domain: Domain, nstate: int, nv1: int, nc1: int, nv2: int, nc2: int,
+                            mu_points: int, s1: str = "Kmeans", check: bool = False,
+                            options: Options | None = None) -> int:
+    """The full device footprint of one ISDF() call beyond psi and theta."""
+    d = domain._c()
+    o = (options or Options())._c()
+    sel = {"Kmeans": SELECT_KMEANS, "QRCP": SELECT_QRCP}[s1]
+    return int(lib().isdf_request_workspace_bytes(ctypes.byref(d), nstate, nv1, nc1, nv2, nc2,
+                                                  mu_points, sel, int(bool(check)),
+                                                  ctypes.byref(o)))

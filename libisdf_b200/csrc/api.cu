@@ -174,6 +174,9 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
     return record_error(ISDF_ERR_ARG, "unknown precision");
   if (opt.precision == ISDF_PRECISION_MIXED && (opt.mixed_slices < 5 || opt.mixed_slices > 7))
     return record_error(ISDF_ERR_ARG, "mixed_slices must be 5, 6 or 7");
+  if (opt.refine_steps != 0)
+    return record_error(ISDF_ERR_UNSUPPORTED,
+                        "refine_steps must be 0: FP64 refinement of the theta solve is not built");
   if (check && check_workspace_bytes(dom->num_grid, nstate, rk, (nv1 + nc1) * (nv2 + nc2)) >
                    kCheckMaxBytes)
     return record_error(ISDF_ERR_UNSUPPORTED,
@@ -219,6 +222,7 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
     ka.max_iter = kmeans_max_iter;
     ka.rand_seed = opt.rand_seed;
     ka.piv = piv;
+    ka.warm = opt.kmeans_warm_start;
     ISDF_TRY(kmeans_weight(d_psi, ng, nocc, nv1, nc1, nv2, nc2, d_w, s));
     KmeansResult kr;
     ISDF_TRY(kmeans_select(ka, arena, s, &kr));
@@ -226,6 +230,7 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
     rep.kmeans_iters = kr.iters;
     rep.npt = kr.npt;
     rep.kmeans_search_frac = (float)kr.search_frac;
+    rep.kmeans_warm_pivots = kr.warm_pivots;
     rep.kernel_launches = 1 + kr.launches;
     rk_fit = kr.rk_eff;
   } else {
@@ -250,8 +255,9 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
     rep.kmeans_iters = 0;
     rep.npt = qr.ntot_mg;
     rep.kernel_launches = qr.launches;
-    rep.reserved[0] = qr.steps;
-    rep.reserved[1] = qr.nflag;
+    rep.qrcp_steps = qr.steps;
+    rep.qrcp_norm_recomputes = qr.recomputes;
+    rep.kmeans_warm_pivots = -1;
   }
   rep.t_select_ms = ms_since(t0);
 
@@ -330,7 +336,7 @@ void isdf_default_options(isdf_options_t* opt) {
   if (!opt) return;
   std::memset(opt, 0, sizeof(*opt));
   opt->precision = ISDF_PRECISION_FP64;
-  opt->refine_steps = 2;
+  opt->refine_steps = 0;
   opt->qrcp_oversample = 1.5;
   opt->qrcp_seed = 41;
   opt->rand_seed = -1;
@@ -396,10 +402,12 @@ int isdf_kmeans_select(const isdf_domain_t* dom, const double* d_w, int mu, int 
 int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, int nc1, int nv2,
              int nc2, int rk, const int* piv, double* d_theta, int precision, int refine_steps,
              int* chol_info, void* stream) {
-  (void)refine_steps;
   try {
     if (!d_psi || !d_theta || !piv || ng <= 0 || rk <= 0 || rk > ng)
       return record_error(ISDF_ERR_ARG, "bad fit arguments");
+    if (refine_steps != 0)
+      return record_error(ISDF_ERR_UNSUPPORTED,
+                          "refine_steps must be 0: FP64 refinement of the theta solve is not built");
     ISDF_TRY(check_state_ranges(nocc, nstate, nv1, nc1, nv2, nc2));
     for (int j = 0; j < rk; ++j)
       if (piv[j] < 0 || piv[j] >= ng) return record_error(ISDF_ERR_ARG, "pivot outside the grid");
@@ -494,7 +502,19 @@ const char* isdf_status_string(int code) {
 
 size_t isdf_workspace_bytes(long long ng, int nstate, int mu, int selector, int precision,
                             int check) {
+  (void)check;  // the check's buffers depend on the grid's shape: see the request variant
   return solve_workspace_bytes(ng, nstate, mu, selector, precision, 0, 1.5, nullptr, 0);
+}
+
+size_t isdf_request_workspace_bytes(const isdf_domain_t* dom, int nstate, int nv1, int nc1,
+                                    int nv2, int nc2, int mu_points, int selector, int check,
+                                    const isdf_options_t* opt) {
+  if (!dom || nstate <= 0 || nv1 < 0 || nc1 < 0 || nv2 < 0 || nc2 < 0 || nv1 + nc1 <= 0 ||
+      nv2 + nc2 <= 0 || mu_points < 0)
+    return 0;
+  for (int i = 0; i < 3; ++i)
+    if (dom->num_grid[i] <= 0) return 0;
+  return request_footprint(dom, nstate, nv1, nc1, nv2, nc2, mu_points, selector, check, opt);
 }
 
 void isdf_release_workspace(void) {

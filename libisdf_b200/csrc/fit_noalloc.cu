@@ -17,11 +17,13 @@
 //    (other host threads, or streams that are not ordered) race on it;
 //  * the array keeps the previous call's contents; the one scratch word that
 //    must start at zero (the Cholesky failure index) is cleared by every call;
-//  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress, once per device); make that first call before
-//    any stream capture begins.
+//  * every call looks up the array's device address on the current device
+//    (cudaGetSymbolAddress: a cheap runtime query, so a cudaDeviceReset
+//    between calls leaves no stale address behind); the first call on a
+//    device also loads the module that holds the array, so make that first
+//    call before any stream capture begins.
 #include <cstdio>
-#include <mutex>
+#include <exception>
 
 #include "arena.h"
 #include "common.cuh"
@@ -34,38 +36,21 @@ namespace {
 
 static __device__ __align__(256) char g_fit_scratch[ISDF_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kMaxDev = 64;
-std::mutex g_addr_mu;
-void* g_addr[kMaxDev] = {};
-
-// Device address of g_fit_scratch on the current device. In host code the
-// name g_fit_scratch is only a host-side stand-in: it must never be passed
-// to a kernel, the address below must.
+// Device address of g_fit_scratch on the current device, looked up with that
+// device current. In host code the name g_fit_scratch is only a host-side
+// stand-in: it must never be passed to a kernel, the address below must.
 int scratch_address(void** out) {
-  int dev = 0;
-  ISDF_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDev) return record_error(ISDF_ERR_UNSUPPORTED, "device index");
-  std::lock_guard<std::mutex> lock(g_addr_mu);
-  if (!g_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_fit_scratch);
-    if (e != cudaSuccess)
-      return record_cuda_error(e, "cudaGetSymbolAddress(g_fit_scratch)", __FILE__, __LINE__);
-    g_addr[dev] = p;
-  }
-  *out = g_addr[dev];
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_fit_scratch);
+  if (e != cudaSuccess)
+    return record_cuda_error(e, "cudaGetSymbolAddress(g_fit_scratch)", __FILE__, __LINE__);
+  *out = p;
   return ISDF_OK;
 }
 
-}  // namespace
-
-}  // namespace isdf_b200
-
-using namespace isdf_b200;
-
-extern "C" int isdf_fit_noalloc(const double* d_psi, long long ng, int nstate, int nocc, int nv1,
-                                int nc1, int nv2, int nc2, int rk, const int* piv,
-                                double* d_theta, int* chol_info, void* stream) {
+int fit_noalloc(const double* d_psi, long long ng, int nstate, int nocc, int nv1, int nc1,
+                int nv2, int nc2, int rk, const int* piv, double* d_theta, int* chol_info,
+                void* stream) {
   if (!d_psi || !d_theta || !piv || ng <= 0 || rk <= 0 || rk > ng || nstate <= 0)
     return record_error(ISDF_ERR_ARG, "isdf_fit_noalloc: bad arguments");
   if (nv1 < 0 || nc1 < 0 || nv2 < 0 || nc2 < 0 || nv1 + nc1 <= 0 || nv2 + nc2 <= 0 ||
@@ -106,9 +91,31 @@ extern "C" int isdf_fit_noalloc(const double* d_psi, long long ng, int nstate, i
   // no pinned mailbox either: the small status reads go by cudaMemcpyAsync
   const bool mailbox = readback_mailbox();
   set_readback_mailbox(false);
+  struct MailboxRestore {
+    bool on;
+    ~MailboxRestore() { set_readback_mailbox(on); }
+  } restore{mailbox};
   int rc = fit_fp64(fa, arena, s, &fr, /*timed=*/false);
-  set_readback_mailbox(mailbox);
   if (chol_info) *chol_info = fr.chol_info;
   if (rc == ISDF_OK) ISDF_CUDA(cudaStreamSynchronize(s));
   return rc;
+}
+
+}  // namespace
+
+}  // namespace isdf_b200
+
+using namespace isdf_b200;
+
+extern "C" int isdf_fit_noalloc(const double* d_psi, long long ng, int nstate, int nocc, int nv1,
+                                int nc1, int nv2, int nc2, int rk, const int* piv,
+                                double* d_theta, int* chol_info, void* stream) {
+  try {
+    return fit_noalloc(d_psi, ng, nstate, nocc, nv1, nc1, nv2, nc2, rk, piv, d_theta, chol_info,
+                       stream);
+  } catch (const std::exception& e) {
+    return record_error(ISDF_ERR_CUDA, e.what());
+  } catch (...) {
+    return record_error(ISDF_ERR_CUDA, "isdf_fit_noalloc: unknown exception");
+  }
 }

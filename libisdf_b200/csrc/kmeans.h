@@ -18,7 +18,8 @@ struct KmeansArgs {
   int mu;
   int max_iter;
   long long rand_seed;  // >= 0: srand() first
-  int* piv;             // host int[ng]
+  int* piv;             // host int[ng]; read first when warm != 0
+  int warm = 0;         // start from the previous pivots in piv (utility.cpp:725-749)
 };
 
 struct KmeansResult {
@@ -27,6 +28,7 @@ struct KmeansResult {
   int npt = 0;
   int launches = 0;
   double search_frac = 0;  // share of point assignments that ran the cell search
+  int warm_pivots = -1;    // warm start: previous pivots kept as initial centroids
 };
 
 size_t kmeans_workspace_bytes(long long ng, int mu);

@@ -706,7 +706,7 @@ int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* 
   for (int j = 0; j < ntot; ++j) args.piv[j] = idx[perm[j]];
   res->steps = kmax;
   res->num_pre = p;
-  res->nflag = hst.nflag;
+  res->recomputes = hst.nflag;
   res->done_early = hst.done;
   res->launches = launches + (readback_mailbox() ? (kmax > 0 ? 6 : 5) : 0);
   return ISDF_OK;

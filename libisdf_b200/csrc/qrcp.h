@@ -22,7 +22,7 @@ struct QrcpResult {
   int ntot_mg = 0;   // kept columns
   int steps = 0;     // pivots computed (min(mu, numPre^2, ntot_mg))
   int num_pre = 0;
-  int nflag = 0;     // downdates that met LAPACK's norm-recompute criterion
+  int recomputes = 0;  // residual norms recomputed exactly (LAPACK's cancellation test)
   int done_early = 0;
   int launches = 0;
 };

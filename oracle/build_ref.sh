@@ -4,10 +4,13 @@
 # together with the single-rank MPI / FFTW shims and BLAS forwarders in
 # oracle/shims, into oracle/_ref/libisdf_ref.so. The reference's flags are
 # kept (-O2 -std=c++14, no -march, so no FMA contraction: Makefile:102,159).
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]
+# REFERENCE_ROOT: the argument, else $ISDF_REFERENCE_ROOT, else the read-only
+# checkout this recipe was written against (/root/reference). Nothing else in
+# the repository names that location.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${ISDF_REFERENCE_ROOT:-/root/reference}}"
 OUT="$HERE/_ref"
 if [ ! -d "$REF/src" ]; then
   echo "reference sources not found under $REF; skipping oracle/_ref build" >&2

@@ -82,7 +82,11 @@ def localized_orbitals(n, length, nstate, seed, alpha):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference-data", default="/root/reference/examples/si8/data")
+    root = os.environ.get("ISDF_REFERENCE_ROOT", "")
+    ap.add_argument("--reference-data",
+                    default=os.path.join(root, "examples", "si8", "data") if root else None,
+                    required=not root,
+                    help="the reference's examples/si8/data (default: under $ISDF_REFERENCE_ROOT)")
     a = ap.parse_args()
     if not ref.available():
         sys.exit("oracle/_ref/libisdf_ref.so is missing: run oracle/build_ref.sh first")
