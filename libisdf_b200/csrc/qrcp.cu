@@ -20,7 +20,13 @@
 //     t_r = sum_j A(r, j) (B_r Qm)_j, Qm(i, j) = q_k[i + j*numPre]: one
 //     FP64 tensor-core tile GEMM over all columns with the row dot fused into
 //     its epilogue, and the multiplicative downdate of LAPACK's dgeqpf,
-//     nu <- nu sqrt(max(0, 1 - (t/nu)^2)).
+//     nu <- nu sqrt(max(0, 1 - (t/nu)^2));
+//   * where dgeqpf's cancellation test fires (LAPACK Working Note 176:
+//     temp (nu / nu_ref)^2 <= sqrt(eps), eps = 2^-53), the downdated value is
+//     not used: dgeqpf then recomputes the norm of the column's transformed
+//     trailing part, i.e. of its residual after the k+1 projections; here
+//     that residual is formed from the column's features (projected on
+//     q_0..q_k twice) and its norm becomes both nu and the new reference nu_ref.
 // Orthonormalising G by Householder QR instead of the reference's dgesvd
 // changes G1, G2 by orthogonal factors: MG changes by an orthogonal matrix on
 // its left, which leaves the column norms and the pivot sequence unchanged.
@@ -50,9 +56,33 @@ struct QrState {
   unsigned long long maxbits;  // max residual norm of the active columns (bit pattern)
   int minpos;                  // first position holding that maximum
   int done;
-  int nflag;                   // downdates that hit LAPACK's recompute criterion
+  int nrec;                    // columns flagged for a norm recompute in this step
   int ntot;
+  int total_rec;               // norms recomputed over the whole selection
+  int pad;
 };
+
+// dgeqpf's recompute threshold sqrt(eps), eps = dlamch('Epsilon') = 2^-53.
+__device__ __forceinline__ double tol3z() { return sqrt(1.1102230246251565e-16); }
+
+// The downdate of one active column's residual norm with t = q_k . x_c, as
+// dgeqpf does it. Returns false (and lists the column) where the cancellation
+// test fires: that column's norm is recomputed exactly after this kernel.
+__device__ __forceinline__ bool downdate_norm(int c, double t, double* __restrict__ nu,
+                                              const double* __restrict__ nu0, QrState* st,
+                                              int* __restrict__ rec_list) {
+  const double v = nu[c];
+  if (v == 0.0) return true;
+  const double ratio = fabs(t) / v;
+  const double temp = fmax(1.0 - ratio * ratio, 0.0);
+  const double rel = v / nu0[c];
+  if (temp * rel * rel <= tol3z()) {
+    rec_list[atomicAdd(&st->nrec, 1)] = c;
+    return false;
+  }
+  nu[c] = v * sqrt(temp);
+  return true;
+}
 
 // ------------------------------------------------------------- norms, filter
 // Squared MG column norm per grid point, summed j-outer, i-inner with
@@ -223,6 +253,7 @@ __global__ void k_pick(int k, int p, int ld, const double* __restrict__ Ac,
     }
     st->maxbits = 0ull;
     st->minpos = INT_MAX;
+    st->nrec = 0;
   }
   __syncthreads();
   if (col < 0) return;
@@ -322,7 +353,8 @@ __global__ void __launch_bounds__(256) k_update(const double* __restrict__ Ac,
                                                 const double* __restrict__ Qm,
                                                 const unsigned char* __restrict__ active,
                                                 double* __restrict__ nu,
-                                                double* __restrict__ nu0, QrState* st) {
+                                                double* __restrict__ nu0, QrState* st,
+                                                int* __restrict__ rec_list) {
   if (st->done) return;
   extern __shared__ double smem[];
   const int m0 = blockIdx.x * CoreU::BM;
@@ -361,17 +393,7 @@ __global__ void __launch_bounds__(256) k_update(const double* __restrict__ Ac,
     if (active[c]) {
       const double tdot = red[threadIdx.x] + red[CoreU::BM + threadIdx.x] +
                           red[2 * CoreU::BM + threadIdx.x] + red[3 * CoreU::BM + threadIdx.x];
-      double v = nu[c];
-      if (v != 0.0) {
-        const double ratio = fabs(tdot) / v;
-        const double temp = fmax(1.0 - ratio * ratio, 0.0);
-        const double rel = v / nu0[c];
-        const double temp2 = 1.0 + 0.05 * temp * rel * rel;
-        if (temp2 == 1.0) atomicAdd(&st->nflag, 1);
-        v = v * sqrt(temp);
-        nu[c] = v;
-      }
-      mx = v;
+      if (downdate_norm(c, tdot, nu, nu0, st, rec_list)) mx = nu[c];
     }
   }
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -399,7 +421,8 @@ __global__ void __launch_bounds__(UpdTile<BN>::THREADS, MINB)
     k_update_ws(const double* __restrict__ Ac, const double* __restrict__ Bc, int ntot, int ld,
                 int p,
                 const double* __restrict__ Qm, const unsigned char* __restrict__ active,
-                double* __restrict__ nu, double* __restrict__ nu0, QrState* st, int* err) {
+                double* __restrict__ nu, double* __restrict__ nu0, QrState* st,
+                int* __restrict__ rec_list, int* err) {
   using T = UpdTile<BN>;
   if (st->done) return;
   extern __shared__ __align__(128) double smem[];
@@ -427,24 +450,74 @@ __global__ void __launch_bounds__(UpdTile<BN>::THREADS, MINB)
     s += __shfl_xor_sync(0xffffffffu, s, 2);
     if (t == 0 && r < m_rem) {
       const int c = m0 + r;
-      if (active[c]) {
-        double v = nu[c];
-        if (v != 0.0) {
-          const double ratio = fabs(s) / v;
-          const double temp = fmax(1.0 - ratio * ratio, 0.0);
-          const double rel = v / nu0[c];
-          const double temp2 = 1.0 + 0.05 * temp * rel * rel;
-          if (temp2 == 1.0) atomicAdd(&st->nflag, 1);
-          v = v * sqrt(temp);
-          nu[c] = v;
-        }
-        mx = fmax(mx, v);
-      }
+      if (active[c] && downdate_norm(c, s, nu, nu0, st, rec_list)) mx = fmax(mx, nu[c]);
     }
   }
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if (lane == 0 && mx > 0.0)
     atomicMax(&st->maxbits, (unsigned long long)__double_as_longlong(mx));
+}
+
+// Exact residual norms of the columns the downdate flagged in this step
+// (dgeqpf's recompute). One CTA per flagged column at a time: the column's
+// features x[i + j*p] = B(c, i) A(c, j) go to shared memory, are projected
+// on q_0..q_k twice (classical Gram-Schmidt: all k+1 dots, one warp per q_l
+// with a fixed lane order, then the update, one thread per feature summing
+// over l in order), and the residual's norm becomes nu[c] and the new
+// reference nu0[c]. cbuf: gridDim.x x k1 doubles of scratch for the dots.
+constexpr int kRecomputeGrid = 148;
+__global__ void __launch_bounds__(256) k_recompute(const double* __restrict__ Ac,
+                                                   const double* __restrict__ Bc, int ld, int p,
+                                                   const double* __restrict__ Q, int m, int k1,
+                                                   const int* __restrict__ rec_list,
+                                                   double* __restrict__ nu,
+                                                   double* __restrict__ nu0, QrState* st,
+                                                   double* __restrict__ cbuf) {
+  extern __shared__ double x[];  // m features
+  __shared__ double red[8];
+  if (st->done) return;
+  const int nrec = st->nrec;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* c = cbuf + (size_t)blockIdx.x * k1;
+  for (int f = blockIdx.x; f < nrec; f += gridDim.x) {
+    const int col = rec_list[f];
+    for (int e = threadIdx.x; e < m; e += 256) {
+      const int i = e % p, j = e / p;
+      x[e] = Bc[col + (long long)i * ld] * Ac[col + (long long)j * ld];
+    }
+    __syncthreads();
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int l = warp; l < k1; l += 8) {
+        const double* q = Q + (long long)l * m;
+        double s = 0.0;
+        for (int i = lane; i < m; i += 32) s = fma(q[i], x[i], s);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) c[l] = s;
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < m; i += 256) {
+        double s = 0.0;
+        for (int l = 0; l < k1; ++l) s = fma(Q[(long long)l * m + i], c[l], s);
+        x[i] -= s;
+      }
+      __syncthreads();
+    }
+    double s = 0.0;
+    for (int i = threadIdx.x; i < m; i += 256) s = fma(x[i], x[i], s);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < 8; ++w) t += red[w];
+      const double v = sqrt(t);
+      nu[col] = v;
+      nu0[col] = v;
+      if (v > 0.0) atomicMax(&st->maxbits, (unsigned long long)__double_as_longlong(v));
+      atomicAdd(&st->total_rec, 1);
+    }
+    __syncthreads();
+  }
 }
 
 // Householder QR of the K x p draws (host, FP64): returns p orthonormal columns
@@ -501,8 +574,8 @@ std::vector<double> gaussian_draws(int m, int n) {
 }
 
 struct QrBuffers {
-  double *A, *B, *norm2, *Ac, *Bc, *nu, *nu0, *Q, *Qm, *x, *cdot, *G1, *G2;
-  int *idx, *pos, *perm, *sel, *tile_cnt;
+  double *A, *B, *norm2, *Ac, *Bc, *nu, *nu0, *Q, *Qm, *x, *cdot, *G1, *G2, *rec_dots;
+  int *idx, *pos, *perm, *sel, *tile_cnt, *rec_list;
   unsigned char* active;
   QrState* st;
   int* err;  // a bounded pipeline wait of the update ran out
@@ -530,6 +603,8 @@ QrBuffers carve(Arena& a, long long n, int p, int k1, int k2, int kmax) {
   b.perm = a.take<int>((size_t)n);
   b.sel = a.take<int>((size_t)kmax);
   b.tile_cnt = a.take<int>((size_t)ntiles);
+  b.rec_list = a.take<int>((size_t)n);
+  b.rec_dots = a.take<double>((size_t)kRecomputeGrid * kmax);
   b.active = a.take<unsigned char>((size_t)n);
   b.st = a.take<QrState>(1);
   b.err = a.take<int>(1);
@@ -544,6 +619,8 @@ int set_update_attrs() {
   if (dev >= 0 && dev < 64 && done[dev]) return ISDF_OK;
   ISDF_CUDA(cudaFuncSetAttribute(k_update<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)CoreU::SMEM_BYTES));
+  ISDF_CUDA(cudaFuncSetAttribute(k_recompute, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(double) * kMaxPre * kMaxPre)));
 #define ISDF_UPD_ATTR(BN)                                                                  \
   ISDF_CUDA(cudaFuncSetAttribute(k_update_ws<BN, UpdMinBlocks<BN>::value>,                   \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                \
@@ -573,7 +650,7 @@ void launch_update_bn(const QrBuffers& b, int ntot, int ld, int p, cudaStream_t 
   using T = UpdTile<BN>;
   const unsigned grid = (unsigned)((ntot + T::BM - 1) / T::BM);
   k_update_ws<BN, UpdMinBlocks<BN>::value><<<grid, T::THREADS, T::SMEM_BYTES, s>>>(
-      b.Ac, b.Bc, ntot, ld, p, b.Qm, b.active, b.nu, b.nu0, b.st, b.err);
+      b.Ac, b.Bc, ntot, ld, p, b.Qm, b.active, b.nu, b.nu0, b.st, b.rec_list, b.err);
 }
 
 // The downdate on the narrowest warp-specialised tile that holds p columns
@@ -687,8 +764,11 @@ int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* 
       launch_update_ws(b, ntot, ld, p, s);
     else
       k_update<1><<<ugrid, 256, CoreU::SMEM_BYTES, s>>>(b.Ac, b.Bc, ntot, ld, p, b.Qm, b.active, b.nu,
-                                                        b.nu0, b.st);
-    launches += 2;
+                                                        b.nu0, b.st, b.rec_list);
+    k_recompute<<<kRecomputeGrid, 256, sizeof(double) * m, s>>>(b.Ac, b.Bc, ld, p, b.Q, m, k + 1,
+                                                                b.rec_list, b.nu, b.nu0, b.st,
+                                                                b.rec_dots);
+    launches += 3;
     if ((k & 255) == 255) ISDF_CHECK_LAUNCH();
   }
   ISDF_CHECK_LAUNCH();
@@ -706,7 +786,7 @@ int qrcp_select(const QrcpArgs& args, Arena& arena, cudaStream_t s, QrcpResult* 
   for (int j = 0; j < ntot; ++j) args.piv[j] = idx[perm[j]];
   res->steps = kmax;
   res->num_pre = p;
-  res->recomputes = hst.nflag;
+  res->recomputes = hst.total_rec;
   res->done_early = hst.done;
   res->launches = launches + (readback_mailbox() ? (kmax > 0 ? 6 : 5) : 0);
   return ISDF_OK;

@@ -49,6 +49,34 @@ def getbasis(psi, nocc, nv1, nc1, nv2, nc2, rk, piv):
     return np.asfortranarray(th.T)
 
 
+def getbasis_rows(psi, nocc, nv1, nc1, nv2, nc2, rk, piv, rows):
+    """theta restricted to the grid rows `rows` (len(rows) x rk): the same
+    operations as getbasis, but Z C^T is formed only on those rows and on the
+    rk interpolation rows that C C^T is gathered from (getbasis_MPI.cpp:188-214).
+    Each row of theta depends only on its own row of Z C^T, so this is the
+    full-size fit evaluated where it is compared, at a cost independent of Ng."""
+    psi = np.asarray(psi)
+    p = np.asarray(piv[:rk], dtype=np.int64)
+    rows = np.asarray(rows, dtype=np.int64)
+    s1 = slice(nocc - nv1, nocc + nc1)
+    s2 = slice(nocc - nv2, nocc + nc2)
+
+    def z(r):
+        p1 = psi[r][:, s1] @ psi[p][:, s1].T
+        if nv1 != nv2 or nc1 != nc2:
+            return p1 * (psi[r][:, s2] @ psi[p][:, s2].T)
+        return p1 * p1
+
+    # Z C^T on the interpolation rows: row j is grid row piv[j], so C C^T
+    # gathers cc[mu, nu] = zp[nu, mu]
+    cc, _ = cct(z(p), rk, np.arange(rk))
+    L = np.linalg.cholesky(cc)
+    zr = z(rows)
+    y = sl.solve_triangular(L, zr.T, lower=True)
+    th = sl.solve_triangular(L, y, lower=True, trans="T")
+    return np.asfortranarray(th.T)
+
+
 def pair_densities(psi_rows, nocc, nv1, nc1, nv2, nc2):
     """rho_ij on the given rows, column (k - lo1) * n2 + (j - lo2), as checkcode.cpp:62-73."""
     a = psi_rows[:, nocc - nv1:nocc + nc1]

@@ -14,7 +14,9 @@ Follows src/cpu/getpoints_QRCP.cpp:11-500 at one rank:
   * column-pivoted QR of the kept columns; the reference calls ScaLAPACK
     pdgeqpf (:440, src/cpu/scalapack.cpp:44-54), which is not available here:
     this restatement calls LAPACK dgeqpf (the same unblocked Householder CPQR
-    with norm downdating) from scipy's OpenBLAS;
+    with norm downdating) from scipy's OpenBLAS, or its C restatement
+    (oracle/qrcp_port.cpp: port_dgeqpf), which can stop after a prefix of
+    pivots and follow a forced pivot sequence;
   * piv[j] = MGIdx[pivot_j] for j < ntotMG, 0 after (:454-457).
 Only tests import this module.
 """
@@ -141,3 +143,86 @@ def residual_norms(mg, selected):
     q, _ = np.linalg.qr(mg[:, selected])
     r = mg - q @ (q.T @ mg)
     return np.linalg.norm(r, axis=0)
+
+
+# ----------------------------------------------------------------- C restatement
+def _port():
+    from oracle import port
+
+    L = port.lib()
+    if not getattr(L, "_qrcp_bound", False):
+        P, I, LL = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong
+        L.port_qrcp_mg.argtypes = [P, P, LL, I, P, I, P]
+        L.port_dgeqpf.argtypes = [P, LL, LL, I, P, P, P, P, P]
+        L.port_dgeqpf.restype = LL
+        L._qrcp_bound = True
+    return L
+
+
+def _p(x):
+    return None if x is None else x.ctypes.data_as(ctypes.c_void_p)
+
+
+def mg_matrix(A, B, idx):
+    """MG restricted to the kept columns idx: p^2 x len(idx), F-order."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    idx = np.ascontiguousarray(idx, dtype=np.int32)
+    p = A.shape[1]
+    mg = np.empty((p * p, len(idx)), order="F")
+    _port().port_qrcp_mg(_p(A), _p(B), A.shape[0], p, _p(idx), len(idx), _p(mg))
+    return mg
+
+
+def dgeqpf_port(mg, kmax=None, forced=None):
+    """port_dgeqpf on mg (overwritten). Returns (order, free_choice, max_norm,
+    taken_norm, recomputes): order[i] = the column taken at step i (0-based
+    column of mg); free_choice[i] = the column dgeqpf itself picks at step i
+    given the columns taken before; max_norm / taken_norm their norms."""
+    m, n = mg.shape
+    assert mg.flags.f_contiguous and mg.dtype == np.float64
+    k = min(m, n) if kmax is None else min(kmax, m, n)
+    jpvt = np.zeros(n, dtype=np.int32)
+    free = np.zeros(k, dtype=np.int32)
+    mx = np.zeros(k)
+    tk = np.zeros(k)
+    f = None
+    if forced is not None:
+        f = np.full(k, -1, dtype=np.int32)
+        f[:min(k, len(forced))] = np.asarray(forced[:k], dtype=np.int32)
+    rec = _port().port_dgeqpf(_p(mg), m, n, k, _p(f), _p(jpvt), _p(free), _p(mx), _p(tk))
+    if rec < 0:
+        raise ValueError("a forced pivot names a column taken at an earlier step")
+    return jpvt[:k].astype(np.int64), free.astype(np.int64), mx, tk, int(rec)
+
+
+def sketch_operands(psi, nocc, nv1, nc1, nv2, nc2, mu, seed=41, factor=1.5):
+    """(A, B, kept columns idx, numPre) of the reference's QRCP selector."""
+    psi = np.asarray(psi)
+    p = num_pre(mu, factor)
+    g1, g2 = sketch(nv1 + nc1, nv2 + nc2, p, seed)
+    A = np.asfortranarray(psi[:, nocc - nv1:nocc + nc1] @ g1)
+    B = np.asfortranarray(psi[:, nocc - nv2:nocc + nc2] @ g2)
+    norms = mg_norms(A, B)
+    idx = np.nonzero(norms > norms.max() * 1e-5)[0]
+    return A, B, idx, p
+
+
+def follow_pivots(psi, nocc, nv1, nc1, nv2, nc2, mu, piv_other, seed=41, factor=1.5,
+                  kmax=None):
+    """Runs the dgeqpf restatement on the reference's MG while taking, at every
+    step, the grid point that another implementation picked (piv_other, grid
+    indices in pivot order). Returns per step: the grid point dgeqpf would
+    have picked, the largest remaining norm, the norm of the point taken, the
+    number of steps, the largest column norm and the recompute count."""
+    A, B, idx, p = sketch_operands(psi, nocc, nv1, nc1, nv2, nc2, mu, seed, factor)
+    k = min(mu, len(idx), p * p) if kmax is None else min(kmax, mu, len(idx), p * p)
+    col_of = {int(g): c for c, g in enumerate(idx)}
+    forced = np.array([col_of.get(int(g), -2) for g in piv_other[:k]], dtype=np.int64)
+    if (forced < 0).any():
+        raise ValueError("a pivot of the other run is not a kept MG column")
+    mg = mg_matrix(A, B, idx)
+    top = float(np.sqrt((mg * mg).sum(axis=0).max()))
+    _, free, mx, tk, rec = dgeqpf_port(mg, k, forced)
+    return idx[free], mx, tk, k, top, rec
+

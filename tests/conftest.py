@@ -27,3 +27,24 @@ def torch_cuda():
     if not torch.cuda.is_available():
         pytest.fail("GPU test collected on a machine without CUDA")
     return torch
+
+
+# Achieved parity figures (differences against the oracle) recorded by the
+# tests and printed in the terminal summary, so that a run's output states
+# what was measured, not only that the bounds held.
+_PARITY = []
+
+
+def record_parity(test: str, quantity: str, value, bound=None):
+    _PARITY.append((test, quantity, value, bound))
+
+
+def pytest_terminal_summary(terminalreporter, exitstatus, config):
+    if not _PARITY:
+        return
+    tr = terminalreporter
+    tr.write_sep("-", "parity figures (achieved vs bound)")
+    for test, q, v, b in _PARITY:
+        vs = f"{v:.3e}" if isinstance(v, float) else str(v)
+        bs = "" if b is None else (f" (bound {b:.1e})" if isinstance(b, float) else f" ({b})")
+        tr.write_line(f"{test}: {q} = {vs}{bs}")

@@ -111,3 +111,15 @@ def test_fit_restatement_and_reference_agree_on_random_shapes(seed):
     fd = ofit.fitted_densities(th, psi, *a, rk, piv)
     fd_ref = ofit.fitted_densities(th_ref, psi, *a, rk, piv)
     assert ofit.rel(fd, fd_ref) < 1e-8
+
+
+def test_sampled_row_fit_equals_full_fit_rows():
+    """oracle.fit.getbasis_rows (the fit evaluated on sampled grid rows, used
+    at the full benchmark sizes) gives exactly the rows of the full fit."""
+    rng = np.random.default_rng(0)
+    psi = np.linalg.qr(rng.standard_normal((3000, 10)))[0]
+    piv = rng.choice(3000, size=40, replace=False).astype(np.int32)
+    rows = np.sort(rng.choice(3000, size=100, replace=False))
+    for a in [(5, 5, 5, 5, 5), (5, 5, 3, 2, 4)]:
+        full = ofit.getbasis(psi, *a, 40, piv)
+        assert np.array_equal(full[rows], ofit.getbasis_rows(psi, *a, 40, piv, rows))
