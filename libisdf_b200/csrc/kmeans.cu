@@ -174,6 +174,22 @@ __global__ void __launch_bounds__(256) k_filter_scatter(const double* __restrict
   }
 }
 
+// Coordinates of grid point t by the formula of utility.cpp:711-713 (and
+// :758-760 for centroids), each operation rounded as the reference's build.
+__device__ __forceinline__ void grid_coords(int t, int nx, int ny, double dx0, double dx1,
+                                            double dx2, double* gx_, double* gy_,
+                                            double* gz_) {
+  const double gx = rmul((double)(t % nx), dx0);
+  const double gy = rmul(rdiv(rsub((double)(t % (nx * ny)), rdiv(gx, dx0)), (double)nx), dx1);
+  const double gz =
+      rmul(rdiv(rsub(rsub((double)t, rdiv(gx, dx0)), rmul(rdiv(gy, dx1), (double)nx)),
+                (double)(nx * ny)),
+           dx2);
+  *gx_ = gx;
+  *gy_ = gy;
+  *gz_ = gz;
+}
+
 // Point coordinates and weights (utility.cpp:707-713); the centroids start
 // at the first rk kept points (utility.cpp:750-762), i.e. points 0..rk-1.
 __global__ void k_points(const int* __restrict__ pidx, const double* __restrict__ w, int n,
@@ -183,16 +199,32 @@ __global__ void k_points(const int* __restrict__ pidx, const double* __restrict_
                          double4* __restrict__ cen) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     int t = pidx[p];
-    double gx = rmul((double)(t % nx), dx0);
-    double gy = rmul(rdiv(rsub((double)(t % (nx * ny)), rdiv(gx, dx0)), (double)nx), dx1);
-    double gz = rmul(rdiv(rsub(rsub((double)t, rdiv(gx, dx0)), rmul(rdiv(gy, dx1), (double)nx)),
-                          (double)(nx * ny)),
-                     dx2);
+    double gx, gy, gz;
+    grid_coords(t, nx, ny, dx0, dx1, dx2, &gx, &gy, &gz);
     px[p] = gx;
     py[p] = gy;
     pz[p] = gz;
     pw[p] = w[t];
     if (p < rk) cen[p] = make_double4(gx, gy, gz, 0.0);
+  }
+}
+
+// Warm start (utility.cpp:725-749): w at the previous pivots, for the
+// filter test the reference applies to them.
+__global__ void k_gather_w(const double* __restrict__ w, const int* __restrict__ idx, int cnt,
+                           double* __restrict__ out) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < cnt; j += gridDim.x * blockDim.x)
+    out[j] = w[idx[j]];
+}
+
+// Warm start: centroid j starts at grid point cinit[j].
+__global__ void k_warm_centroids(const int* __restrict__ cinit, int rk, int nx, int ny,
+                                 double dx0, double dx1, double dx2,
+                                 double4* __restrict__ cen) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < rk; j += gridDim.x * blockDim.x) {
+    double gx, gy, gz;
+    grid_coords(cinit[j], nx, ny, dx0, dx1, dx2, &gx, &gy, &gz);
+    cen[j] = make_double4(gx, gy, gz, 0.0);
   }
 }
 
@@ -1061,6 +1093,14 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
   const int nfilter = (n + 1023) / 1024;
   const int nchunks = (n + kFinalChunk - 1) / kFinalChunk;
   if (args.rand_seed >= 0) std::srand((unsigned)args.rand_seed);
+  // warm start: the caller's previous pivots, read before piv is rewritten
+  std::vector<int> prev;
+  if (args.warm && n > 1 && args.piv[0] != args.piv[1]) {
+    prev.assign(args.piv, args.piv + mu);
+    for (int v : prev)
+      if (v < 0 || v >= n) return record_error(ISDF_ERR_ARG, "kmeans: warm-start pivot outside the grid");
+  }
+  res->warm_pivots = -1;
 
   // filter: maxW, kept-point compaction, zero tail
   ISDF_CUDA(cudaMemsetAsync(b.st, 0, sizeof(KmState), stream));
@@ -1100,9 +1140,41 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
   const double dx0 = args.length[0] / args.num_grid[0];
   const double dx1 = args.length[1] / args.num_grid[1];
   const double dx2 = args.length[2] / args.num_grid[2];
+  std::vector<int> cinit;
+  if (!prev.empty()) {
+    // utility.cpp:725-749: the previous pivots whose weight passes the
+    // filter, in their order, then the first kept points not among them
+    // (at most mu kept points are examined: each one either joins or is
+    // one of the kept previous pivots)
+    ISDF_CUDA(cudaMemcpyAsync(b.sel, prev.data(), sizeof(int) * (size_t)mu,
+                              cudaMemcpyHostToDevice, stream));
+    k_gather_w<<<grid_for(mu, 256), 256, 0, stream>>>(args.d_w, b.sel, mu, b.part_d);
+    ISDF_CHECK_LAUNCH();
+    std::vector<double> wprev(mu);
+    std::vector<int> head(mu);
+    ISDF_TRY(read_back(wprev.data(), b.part_d, sizeof(double) * (size_t)mu, stream));
+    ISDF_TRY(read_back(head.data(), b.pidx, sizeof(int) * (size_t)mu, stream));
+    double maxw;
+    std::memcpy(&maxw, &hst.maxw_bits, sizeof(double));
+    const double thr = 1e-8 * maxw;
+    cinit.reserve(mu);
+    for (int i = 0; i < mu; ++i)
+      if (wprev[i] > thr) cinit.push_back(prev[i]);
+    res->warm_pivots = (int)cinit.size();
+    std::vector<char> in((size_t)n, 0);
+    for (int c : cinit) in[c] = 1;
+    for (int k = 0; (int)cinit.size() < mu && k < mu; ++k)
+      if (!in[head[k]]) cinit.push_back(head[k]);
+    ISDF_CUDA(cudaMemcpyAsync(b.sel, cinit.data(), sizeof(int) * (size_t)mu,
+                              cudaMemcpyHostToDevice, stream));
+  }
   k_points<<<grid_for(n, 256), 256, 0, stream>>>(b.pidx, args.d_w, n, args.num_grid[0],
                                                  args.num_grid[1], dx0, dx1, dx2, b.px, b.py,
                                                  b.pz, b.pw, mu, b.cen);
+  if (!prev.empty())
+    k_warm_centroids<<<grid_for(mu, 256), 256, 0, stream>>>(b.sel, mu, args.num_grid[0],
+                                                            args.num_grid[1], dx0, dx1, dx2,
+                                                            b.cen);
   {
     KmState init{};
     init.flag = n;

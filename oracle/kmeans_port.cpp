@@ -13,7 +13,11 @@
 //      alias grid point 0 with weight w[0] and join every assignment and
 //      update (utility.cpp:648,659,707-713);
 //    - coordinates from the grid index by the formula of utility.cpp:711-713;
-//    - initial centroids = the first rk kept points (utility.cpp:750-762);
+//    - initial centroids = the first rk kept points (utility.cpp:750-762), or
+//      with a warm start (piv[0] != piv[1] on entry, utility.cpp:725-749) the
+//      previous pivots whose weight passes the filter, topped up with the
+//      first kept points not among them (port_kmeans_warm; the reference's
+//      ISDF() zeroes piv first, so only a caller of KMEAN reaches this);
 //    - distances ((dx*dx + dy*dy) + dz*dz), no FMA (utility.cpp:598-615);
 //    - per-point argmin over centroids, first minimum wins (utility.cpp:579-595);
 //    - centroid sums accumulated in point order (utility.cpp:814-822);
@@ -78,10 +82,20 @@ void port_weight(const double* psi, long long ng, int nocc, int nv1, int nc1, in
 // Returns rk_eff (>= 1) or a negative code. iters_out: Lloyd iterations run
 // (-1 on the early-return branch). rand_seed >= 0 reseeds std::rand first
 // (only the early-return branch draws from it); < 0 keeps the process state.
-int port_kmeans(const double* w, int n, const int* nG, const double* len, int rk, int max_iter,
-                long long rand_seed, int* piv, int* iters_out) {
+// warm != 0: piv holds the previous pivots on entry (used when piv[0] !=
+// piv[1]); *warm_used receives how many of them were kept (-1: cold start).
+int port_kmeans_warm(const double* w, int n, const int* nG, const double* len, int rk,
+                     int max_iter, long long rand_seed, int* piv, int* iters_out, int warm,
+                     int* warm_used) {
   if (rand_seed >= 0) std::srand((unsigned)rand_seed);
   const double kmeans_tol = 1e-5, df_tol = 1e-8;
+  std::vector<int> prev;
+  if (warm && n > 1 && piv[0] != piv[1]) {
+    prev.assign(piv, piv + rk);
+    for (int v : prev)
+      if (v < 0 || v >= n) return -2;
+  }
+  if (warm_used) *warm_used = -1;
   std::memset(piv, 0, sizeof(int) * (size_t)n);
   double maxW = 0.0;
   for (int i = 0; i < n; i++)
@@ -114,7 +128,18 @@ int port_kmeans(const double* w, int n, const int* nG, const double* len, int rk
     coords(tmp, nG, dx, &gx[i], &gy[i], &gz[i]);
   }
   std::vector<double> cx(rk), cy(rk), cz(rk), cnt(rk);
-  for (int j = 0; j < rk; j++) coords(index[j], nG, dx, &cx[j], &cy[j], &cz[j]);
+  std::vector<int> cinit(index.begin(), index.begin() + rk);
+  if (!prev.empty()) {
+    cinit.clear();
+    for (int i = 0; i < rk; i++)
+      if (w[prev[i]] > df_tol * maxW) cinit.push_back(prev[i]);
+    if (warm_used) *warm_used = (int)cinit.size();
+    std::vector<char> in(n, 0);
+    for (int c : cinit) in[c] = 1;
+    for (int k = 0; (int)cinit.size() < rk && k < npt; k++)
+      if (!in[index[k]]) cinit.push_back(index[k]);
+  }
+  for (int j = 0; j < rk; j++) coords(cinit[j], nG, dx, &cx[j], &cy[j], &cz[j]);
 
   auto dist = [&](int i, int j) {
     double d1 = gx[i] - cx[j], d2 = gy[i] - cy[j], d3 = gz[i] - cz[j];
@@ -208,6 +233,11 @@ int port_kmeans(const double* w, int n, const int* nG, const double* len, int rk
     }
   }
   return rk;
+}
+
+int port_kmeans(const double* w, int n, const int* nG, const double* len, int rk, int max_iter,
+                long long rand_seed, int* piv, int* iters_out) {
+  return port_kmeans_warm(w, n, nG, len, rk, max_iter, rand_seed, piv, iters_out, 0, nullptr);
 }
 
 int port_num_threads(void) {

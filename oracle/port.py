@@ -24,6 +24,8 @@ def lib():
         _lib.port_weight.argtypes = [P, ctypes.c_longlong, I, I, I, I, I, P]
         _lib.port_kmeans.argtypes = [P, I, P, P, I, I, ctypes.c_longlong, P, P]
         _lib.port_kmeans.restype = I
+        _lib.port_kmeans_warm.argtypes = [P, I, P, P, I, I, ctypes.c_longlong, P, P, I, P]
+        _lib.port_kmeans_warm.restype = I
         _lib.port_num_threads.restype = I
     return _lib
 
@@ -51,6 +53,24 @@ def kmeans(w, ng, length, mu, iters, rand_seed=1):
     if rk <= 0:
         raise RuntimeError(f"port_kmeans failed: {rk}")
     return piv, rk, int(it[0])
+
+
+def kmeans_warm(w, ng, length, mu, iters, prev_piv, rand_seed=1):
+    """K-means started from the previous pivots prev_piv (used when
+    prev_piv[0] != prev_piv[1], utility.cpp:725-749). Returns (piv, rk_eff,
+    iterations run, previous pivots kept as initial centroids or -1)."""
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    g = np.ascontiguousarray(ng, dtype=np.int32)
+    ln = np.ascontiguousarray(length, dtype=np.float64)
+    piv = np.array(prev_piv, dtype=np.int32, copy=True)
+    assert piv.size == w.shape[0]
+    it = np.zeros(1, dtype=np.int32)
+    used = np.zeros(1, dtype=np.int32)
+    rk = lib().port_kmeans_warm(_ptr(w), w.shape[0], _ptr(g), _ptr(ln), mu, iters, rand_seed,
+                                _ptr(piv), _ptr(it), 1, _ptr(used))
+    if rk <= 0:
+        raise RuntimeError(f"port_kmeans_warm failed: {rk}")
+    return piv, rk, int(it[0]), int(used[0])
 
 
 def kmeans_piv(psi, ng, length, nocc, nv1, nc1, nv2, nc2, mu, iters, rand_seed=1):

@@ -37,6 +37,9 @@ def lib():
         _lib.ref_bench_kmeans_step.restype = ctypes.c_double
         _lib.ref_qrcp_sketch.argtypes = [I, I, I, ctypes.c_long, P, P]
         _lib.ref_qrcp_gaussians.argtypes = [I, I, I, ctypes.c_long, P, P]
+        _lib.ref_kmeans_warm.argtypes = [P, P, P, I, I, P, P, P, P, P, I]
+        _lib.ref_bench_kmean.argtypes = [P, P, P, I, I, P]
+        _lib.ref_bench_kmean.restype = ctypes.c_double
         _lib.ref_iround.argtypes = [ctypes.c_double]
         _lib.ref_iround.restype = I
     return _lib
@@ -83,6 +86,24 @@ def kmeans_piv(psi, ng, length, nocc, nv1, nc1, nv2, nc2, mu, iters, rand_seed=1
     return piv, int(rk[0]), int(it[0]), w
 
 
+def kmeans_warm(w, ng, length, mu, iters, prev_piv):
+    """The reference's KMEAN on weight w with piv = prev_piv on entry (its warm
+    start when prev_piv[0] != prev_piv[1]). Returns (piv, rk_eff, iterations,
+    "Reusable pivots" as logged or -1)."""
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    g, ln = _geom(ng, length)
+    piv = np.array(prev_piv, dtype=np.int32, copy=True)
+    rk = np.zeros(1, dtype=np.int32)
+    it = np.zeros(1, dtype=np.int32)
+    used = np.zeros(1, dtype=np.int32)
+    log = ctypes.create_string_buffer(1 << 16)
+    rc = lib().ref_kmeans_warm(_ptr(w), _ptr(g), _ptr(ln), mu, iters, _ptr(piv), _ptr(rk),
+                               _ptr(it), _ptr(used), log, len(log))
+    if rc != 0:
+        raise OracleError(f"ref_kmeans_warm rc={rc}: {log.value.decode(errors='replace')[-400:]}")
+    return piv, int(rk[0]), int(it[0]), int(used[0])
+
+
 def getbasis(psi, ng, length, nocc, nv1, nc1, nv2, nc2, rk, piv):
     """theta (Ng x rk, F-order) from the reference's getbasis_MPI at one rank."""
     psi = np.asfortranarray(psi, dtype=np.float64)
@@ -121,6 +142,14 @@ def iround(a: float) -> int:
 def bench_kmeans_step(npt: int, rk: int, repeats: int = 1) -> float:
     """Seconds of one reference Lloyd step (pdist2 + findMin) at full size."""
     return float(lib().ref_bench_kmeans_step(npt, rk, repeats))
+
+
+def bench_kmean(w, ng, length, mu: int, iters: int) -> float:
+    """Seconds of the reference's whole KMEAN with KmeansMaxIter = iters."""
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    g, ln = _geom(ng, length)
+    piv = np.zeros(w.shape[0], dtype=np.int32)
+    return float(lib().ref_bench_kmean(_ptr(w), _ptr(g), _ptr(ln), mu, iters, _ptr(piv)))
 
 
 def bench_getbasis_rows(psi, shape, fraction: int, repeats: int = 1) -> float:

@@ -76,6 +76,36 @@ void ref_weight(const double* psi, int ng_total, int nocc, int nv1, int nc1, int
   for (int kk = 0; kk < ng_total; kk++) w[kk] = 0.0 + sumI[kk] * sumJ[kk];
 }
 
+// The reference's KMEAN called directly with the caller's piv, as an SCF
+// loop that keeps piv between solves would call it: when piv[0] != piv[1] on
+// entry KMEAN starts from those pivots (src/common/utility.cpp:725-749), the
+// warm start that the reference's ISDF() never reaches because it zeroes piv
+// first (src/common/isdf.cpp:174-175). w: the weight; *reused: the count the
+// reference logs as "Reusable pivots" (-1 when it logged none).
+int ref_kmeans_warm(const double* w, const int* ng, const double* len, int mu, int iters,
+                    int* piv, int* rk_eff, int* n_iter, int* reused, char* log, int loglen) {
+  try {
+    LogCapture cap;
+    Domain dom = make_domain(ng, len);
+    const int n = dom.NumGridTotal();
+    DblNumVec weight(n);
+    std::memcpy(weight.Data(), w, sizeof(double) * n);
+    Int rk = mu;
+    KMEAN(n, weight, rk, 1e-5, iters, 1e-8, dom, piv);
+    *rk_eff = rk;
+    std::string s = cap.str();
+    double v = -1;
+    *n_iter = parse_after(s, "Converged in ", &v) == 0 ? (int)v : -1;
+    v = -1;
+    *reused = parse_after(s, "Reusable pivots: ", &v) == 0 ? (int)v : -1;
+    copy_log(s, log, loglen);
+    return 0;
+  } catch (const std::exception& e) {
+    copy_log(e.what(), log, loglen);
+    return -1;
+  }
+}
+
 // The K-means point selection of the GPU ISDF() path: weight, then KMEAN
 // (src/common/utility.cpp:631-988) with the tolerances of
 // src/cuda/isdf-gpu.cpp:31-32, piv zeroed first as src/common/isdf.cpp:174-175
@@ -200,6 +230,25 @@ double ref_bench_kmeans_step(int npt, int rk, int repeats) {
     if (t < best) best = t;
   }
   return best;
+}
+
+// Seconds for the reference's KMEAN (src/common/utility.cpp:631-988) on the
+// weight w of a grid ng x len with KmeansMaxIter = iters: the whole routine
+// as the reference runs it (filter, coordinates, initial assignment, `iters`
+// Lloyd iterations each with its host centroid update, pdist2 and findMin,
+// the final per-centroid argmin and the piv build). piv: scratch int[Ng].
+double ref_bench_kmean(const double* w, const int* ng, const double* len, int mu, int iters,
+                       int* piv) {
+  LogCapture cap;
+  Domain dom = make_domain(ng, len);
+  const int n = dom.NumGridTotal();
+  DblNumVec weight(n);
+  std::memcpy(weight.Data(), w, sizeof(double) * n);
+  std::memset(piv, 0, sizeof(int) * n);
+  Int rk = mu;
+  const double t0 = MPI_Wtime();
+  KMEAN(n, weight, rk, 1e-5, iters, 1e-8, dom, piv);
+  return MPI_Wtime() - t0;
 }
 
 // The QRCP sketch of src/cpu/getpoints_QRCP.cpp:143-189 at rank 0:

@@ -3,7 +3,7 @@ effective mu and iteration count)."""
 import numpy as np
 import pytest
 
-from conftest import load_golden
+from conftest import load_golden, record_parity
 from oracle import port
 
 import libisdf_b200 as isdf
@@ -113,3 +113,76 @@ def test_select_random_weights(torch_cuda, mu, seed):
                                           torch.from_numpy(w).cuda(), mu, 40)
     assert (rk, it) == (rk_o, it_o)
     assert np.array_equal(piv, piv_o)
+
+
+def _perturbed_prev(g, seed=1):
+    """Pivots of a previous solve on a slightly different weight (as an SCF
+    loop's last iteration would have left them)."""
+    ng = tuple(int(x) for x in g["ng"])
+    ln = tuple(float(x) for x in g["length"])
+    rng = np.random.default_rng(seed)
+    w2 = np.abs(g["weight"] * (1 + 0.05 * rng.standard_normal(g["weight"].shape)))
+    prev, _, _ = port.kmeans(w2, ng, ln, int(g["rk_requested"]), int(g["iters"]))
+    return prev
+
+
+@pytest.mark.parametrize("name", ["si8_example", "small_s1s2", "small_mu0", "small_iters0"])
+def test_warm_start_matches_reference(torch_cuda, name):
+    """K-means warm start (utility.cpp:725-749) through ISDF() with
+    kmeans_warm_start: the same piv, effective mu, iteration count and number
+    of reused pivots as the port, and as the reference's own KMEAN called
+    with the same previous piv where the reference build is present."""
+    torch = torch_cuda
+    g = load_golden(name)
+    ng = tuple(int(x) for x in g["ng"])
+    ln = tuple(float(x) for x in g["length"])
+    a = (int(g["nocc"]), int(g["nv1"]), int(g["nc1"]), int(g["nv2"]), int(g["nc2"]))
+    mu, iters = int(g["rk_requested"]), int(g["iters"])
+    prev = _perturbed_prev(g)
+    piv_o, rk_o, it_o, used_o = port.kmeans_warm(g["weight"], ng, ln, mu, iters, prev)
+    from oracle import ref
+
+    if ref.available():
+        r = ref.kmeans_warm(g["weight"], ng, ln, mu, iters, prev)
+        assert np.array_equal(r[0], piv_o) and r[1:] == (rk_o, it_o, used_o)
+    psi = g["psi"]
+    d_psi = _dev(torch, psi)
+    d_theta = torch.empty((mu, psi.shape[0]), dtype=torch.float64, device="cuda")
+    piv = prev.copy()
+    rep = isdf.ISDF(d_psi, isdf.Domain(length=ln, num_grid=ng), a[0], psi.shape[1], *a[1:], mu,
+                    d_theta, piv, iters, options=isdf.Options(kmeans_warm_start=True))
+    assert (rep.rk_eff, rep.kmeans_iters, rep.kmeans_warm_pivots) == (rk_o, it_o, used_o)
+    assert np.array_equal(piv, piv_o)
+    # without the option the caller's piv is ignored, as in the reference
+    piv = prev.copy()
+    rep = isdf.ISDF(d_psi, isdf.Domain(length=ln, num_grid=ng), a[0], psi.shape[1], *a[1:], mu,
+                    d_theta, piv, iters)
+    assert rep.kmeans_warm_pivots == -1 and np.array_equal(piv, g["piv"])
+
+
+def test_warm_start_si8_perturbed_orbitals(torch_cuda):
+    """An SCF-like step on the Si8-like shape: the orbitals change slightly
+    between two solves; the second solve starts from the first one's piv and
+    equals the port's warm start bit for bit."""
+    torch = torch_cuda
+    s = synth.SI8
+    psi = synth.shape_orbitals(s, 0)
+    rng = np.random.default_rng(9)
+    psi2 = np.asfortranarray(np.linalg.qr(psi + 1e-3 * rng.standard_normal(psi.shape))[0])
+    ng, ln = (s.n,) * 3, (s.length,) * 3
+    a = (s.nocc, s.nv1, s.nc1, s.nv2, s.nc2)
+    dom = isdf.Domain(length=ln, num_grid=ng)
+    d_theta = torch.empty((s.mu, s.ng), dtype=torch.float64, device="cuda")
+    piv = np.zeros(s.ng, dtype=np.int32)
+    rep1 = isdf.ISDF(_dev(torch, psi), dom, s.nocc, s.nstate, *a[1:], s.mu, d_theta, piv,
+                     s.kmeans_iters)
+    prev = piv.copy()
+    w2 = port.weight(psi2, *a)
+    piv_o, rk_o, it_o, used_o = port.kmeans_warm(w2, ng, ln, s.mu, s.kmeans_iters, prev)
+    cold = port.kmeans(w2, ng, ln, s.mu, s.kmeans_iters)
+    rep2 = isdf.ISDF(_dev(torch, psi2), dom, s.nocc, s.nstate, *a[1:], s.mu, d_theta, piv,
+                     s.kmeans_iters, options=isdf.Options(kmeans_warm_start=True))
+    assert (rep2.rk_eff, rep2.kmeans_iters, rep2.kmeans_warm_pivots) == (rk_o, it_o, used_o)
+    assert np.array_equal(piv, piv_o)
+    record_parity("K-means warm start Si8-like", "Lloyd iterations warm / cold",
+                  f"{rep2.kmeans_iters} / {cold[2]} (first solve {rep1.kmeans_iters})")

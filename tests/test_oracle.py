@@ -123,3 +123,23 @@ def test_sampled_row_fit_equals_full_fit_rows():
     for a in [(5, 5, 5, 5, 5), (5, 5, 3, 2, 4)]:
         full = ofit.getbasis(psi, *a, 40, piv)
         assert np.array_equal(full[rows], ofit.getbasis_rows(psi, *a, 40, piv, rows))
+
+
+@pytest.mark.parametrize("name", CASES[:4])
+def test_port_warm_start_matches_reference_live(name):
+    """The port's K-means warm start (previous pivots as initial centroids,
+    utility.cpp:725-749) against the reference's own KMEAN given the same
+    previous piv."""
+    ref = pytest.importorskip("oracle.ref")
+    if not ref.available():
+        pytest.skip("oracle/_ref not built on this machine")
+    g = load_golden(name)
+    ng, length = tuple(int(x) for x in g["ng"]), tuple(float(x) for x in g["length"])
+    mu, iters = int(g["rk_requested"]), int(g["iters"])
+    rng = np.random.default_rng(1)
+    w2 = np.abs(g["weight"] * (1 + 0.05 * rng.standard_normal(g["weight"].shape)))
+    prev, _, _ = port.kmeans(w2, ng, length, mu, iters)
+    a = port.kmeans_warm(g["weight"], ng, length, mu, iters, prev)
+    b = ref.kmeans_warm(g["weight"], ng, length, mu, iters, prev)
+    assert np.array_equal(a[0], b[0]) and a[1:] == b[1:]
+    assert a[3] > 0  # previous pivots were reused
