@@ -94,3 +94,18 @@ def test_ctypes_structs_match_the_c_layout(tmp_path):
         assert c_layout[(py_name, "size")] == ctypes.sizeof(cls), py_name
         for field, _ in cls._fields_:
             assert c_layout[(py_name, field)] == getattr(cls, field).offset, (py_name, field)
+
+
+def test_cxx_drop_in_caller_links(tmp_path):
+    """tests/cxx/drop_in.cpp, a caller written like the reference's example
+    driver, compiles against include/isdf.hpp and links to libisdf_b200.so
+    (it is run on the GPU by tests/test_cxx_drop_in_gpu.py)."""
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    libdir = os.path.join(ROOT, "libisdf_b200")
+    isdf.lib()
+    r = subprocess.run(["g++", "-std=c++14", os.path.join(ROOT, "tests", "cxx", "drop_in.cpp"),
+                        "-o", str(tmp_path / "drop_in"), "-I", os.path.join(ROOT, "include"),
+                        "-I", os.path.join(cuda, "include"), "-L", libdir, "-l:libisdf_b200.so",
+                        "-L", os.path.join(cuda, "lib64"), "-lcudart"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
