@@ -1,14 +1,20 @@
 """ISDF solves/s on B200 (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config si64|si8|si216] [--precision fp64|mixed]
+                    [--config si216|si64|si8] [--precision mixed|fp64]
 
 A step is one full ISDF solve (weight -> K-means selection -> Z C^T GEMM with
 the Hadamard epilogue -> C C^T -> Cholesky -> triangular solves) through the
 public API, check = false, on synthetic Kohn-Sham-like orbitals of the
-configured shape (libisdf_b200/synth.py, seeded). Default workload: the
-Si64-like shape (80^3 grid, 256 states, S1 = S2 = all states, mu = 2048,
-100 K-means iterations, plain FP64).
+configured shape (libisdf_b200/synth.py, seeded per configuration).
+
+Default: the headline comparison, the Si216-like shape (108^3 grid, 864
+states, S1 = S2 = all states, mu = 4320, 100 K-means iterations, seed 3) in
+the mixed-precision form (value) and in the plain FP64 form of the same run
+(plain_fp64, mixed_over_plain), each timed over its own region with its own
+clock record, both checked against the oracle's FP64 fit on sampled grid rows
+and state pairs (accuracy_vs_oracle); beside them a short Si64-like plain
+FP64 run (secondary).
 
 value: solves/s with psi resident in HBM (device time, CUDA events on the
 solve stream; max over ranks). e2e: the same through the public API from
@@ -19,7 +25,9 @@ data path).
 
 --impl reference times the reference's own CPU implementation
 (oracle/_ref: the reference sources compiled with single-rank shims) on a
-bounded sample of the same workload and extrapolates to solves/s.
+bounded sample of the same workload and extrapolates to solves/s (the line
+says so); it also times one whole reference solve at the Si8-like size beside
+the model's estimate of it, and the model's scaling with the sampled points.
 """
 from __future__ import annotations
 
@@ -136,43 +144,147 @@ def replica_value(world: int, steps: int, t_ms: float) -> float:
     return world * steps / (t_ms * 1e-3)
 
 
+SEEDS = {"si8": 0, "si64": 1, "si216": 3, "si64c": 1}  # the benchmark configurations' seeds
+
+
+def _shape_psi(synth, shape, name):
+    """Synthetic orbitals of a workload on the GPU, returned on the host."""
+    import torch
+
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    return synth.shape_orbitals(shape, SEEDS.get(name, 1), device=dev)
+
+
 # ------------------------------------------------------------------ reference arm
-def reference_sample(shape, iters: int, repeats: int = 1):
-    """Seconds per solve of the reference's CPU path, from a bounded sample:
-    one K-means Lloyd step of the reference (its pdist2 + findMin over all
-    grid points, utility.cpp:878-901) timed at full size, times the iteration
-    count, plus the reference's getbasis_MPI fit on a 1/16 row block of the
-    grid (its cost is linear in the rows), times 16."""
+def _slab(shape, mu):
+    """A z-slab of the grid with enough points that the reference's Npt x mu
+    distance matrix (0.5 GB at least) no longer fits in the host caches, so
+    that its cost per point is the full grid's; the whole grid when that is
+    smaller."""
+    per_plane = shape.n * shape.n
+    pts = max(shape.ng // 64, (1 << 29) // (8 * mu))
+    nz = min(shape.n, -(-pts // per_plane))
+    return nz
+
+
+def _slab_grid(shape, nz):
+    return ((shape.n, shape.n, nz), (shape.length, shape.length, shape.length * nz / shape.n),
+            shape.n * shape.n * nz)
+
+
+def _kmean_model(w, g, ln, mu, best_of=2):
+    """(fixed s, s per Lloyd iteration) of the reference's KMEAN on a grid,
+    from its whole-routine time with 1 and 3 iterations."""
     from oracle import ref
+
+    t1 = min(ref.bench_kmean(w, g, ln, mu, 1) for _ in range(best_of))
+    t3 = min(ref.bench_kmean(w, g, ln, mu, 3) for _ in range(best_of))
+    per_iter = max(0.0, (t3 - t1) / 2)
+    return max(0.0, t1 - per_iter), per_iter
+
+
+def calibrate(shape, w):
+    """The split of the reference's KMEAN time into a fixed part and a part
+    per Lloyd iteration, on the sampled slab (done once per run)."""
+    nz = _slab(shape, shape.mu)
+    g, ln, npl = _slab_grid(shape, nz)
+    fixed, per_iter = _kmean_model(w[:npl], g, ln, shape.mu)
+    return {"planes": nz, "fixed_s": fixed, "per_iteration_s": per_iter}
+
+
+def reference_sample(shape, psi, w, iters: int, cal):
+    """Seconds per solve of the reference's CPU path (oracle/_ref: its own
+    sources), extrapolated from a bounded sample:
+      * K-means: the reference's whole KMEAN (utility.cpp:631-988: filter,
+        initial assignment, each Lloyd iteration with its host centroid
+        update, pdist2 and findMin, the final argmin, the piv build) with one
+        Lloyd iteration on a z-slab of the grid, scaled to `iters` iterations
+        by the slab's calibrated split (KMEAN with 1 and 3 iterations:
+        fixed part + part per iteration) and to the whole grid by the slab's
+        share of the points (the work is Npt x mu per pass);
+      * fit: the reference's getbasis_MPI on the same share of the grid rows
+        with the full mu, scaled by the rows.
+    Returns (seconds per solve, info)."""
+    from oracle import ref
+
+    nz = cal["planes"]
+    frac = nz / shape.n
+    g, ln, npl = _slab_grid(shape, nz)
+    t1 = ref.bench_kmean(w[:npl], g, ln, shape.mu, 1)
+    fixed, per = cal["fixed_s"], cal["per_iteration_s"]
+    scale = (fixed + iters * per) / (fixed + per) if fixed + per > 0 else 1.0
+    t_kmeans = t1 * scale / frac
+    rows = npl if nz < shape.n else shape.ng
+    t_fit = ref.bench_getbasis_rows(psi, shape, shape.ng // rows) * (shape.ng / rows)
+    info = {"kind": "reference", "cores": os.cpu_count(), "extrapolated": nz < shape.n,
+            "sample": (f"{shape.name}: the reference's KMEAN with one Lloyd iteration on {nz} "
+                       f"of {shape.n} z-planes ({npl} points x {shape.mu} centroids), scaled "
+                       f"to {iters} iterations by the calibrated split ({fixed:.3f} s fixed + "
+                       f"{per:.3f} s per iteration on that slab) and to the whole grid by "
+                       f"points; the reference's getbasis_MPI on {rows} of {shape.ng} rows, "
+                       f"scaled by rows; OpenBLAS threads = {os.cpu_count()}, K-means "
+                       "single-threaded as in the reference"),
+            "kmeans_s": t_kmeans, "fit_s": t_fit, "calibration": cal}
+    return t_kmeans + t_fit, info
+
+
+def extrapolation_check(shape, w):
+    """Two checks of the sampling model, reported beside its estimate:
+      * one whole reference CPU solve at the Si8-like size (40^3, mu = 320,
+        100 K-means iterations) timed end to end, beside the model's estimate
+        of it (KMEAN with 1 and 3 iterations and getbasis_MPI on the same
+        grid): the fixed + per-iteration split;
+      * at the workload's own size, the per-iteration time on the sampled
+        slab and on a slab twice as thick: the scaling with the points."""
+    import time
+
+    from oracle import port, ref
     from libisdf_b200 import synth
 
-    psi = synth.shape_orbitals(shape, 1)
-    t_iter = ref.bench_kmeans_step(psi.shape[0], shape.mu, repeats)
-    t_fit = ref.bench_getbasis_rows(psi, shape, 16, repeats)
-    return iters * t_iter + 16 * t_fit, {
-        "kind": "reference", "cores": os.cpu_count(),
-        "sample": (f"{shape.name}: one reference K-means step (pdist2+findMin over {shape.ng} "
-                   f"points x {shape.mu} centroids) x {iters} iterations + reference getbasis_MPI "
-                   f"on {shape.ng // 16} rows x 16; OpenBLAS threads = {os.cpu_count()}, "
-                   "K-means single-threaded as in the reference")}
+    s = synth.SI8
+    psi = _shape_psi(synth, s, "si8")
+    a = (s.nocc, s.nv1, s.nc1, s.nv2, s.nc2)
+    t0 = time.perf_counter()
+    piv, rk, it, _ = ref.kmeans_piv(psi, (s.n,) * 3, (s.length,) * 3, *a, s.mu, s.kmeans_iters)
+    ref.getbasis(psi, (s.n,) * 3, (s.length,) * 3, *a, rk, piv)
+    t_full = time.perf_counter() - t0
+    w8 = port.weight(psi, *a)
+    fixed, per_iter = _kmean_model(w8, (s.n,) * 3, (s.length,) * 3, s.mu)
+    est = fixed + it * per_iter + ref.bench_getbasis_rows(psi, s, 1)
+    out = {"si8_whole_solve": {"measured_s": t_full, "model_estimate_s": est,
+                               "kmeans_iters": it}}
+    nz = _slab(shape, shape.mu)
+    if 2 * nz <= shape.n:
+        per = []
+        for z in (nz, 2 * nz):
+            g, ln, npl = _slab_grid(shape, z)
+            per.append(_kmean_model(w[:npl], g, ln, shape.mu, best_of=1)[1])
+        out["slab_scaling"] = {"planes": [nz, 2 * nz], "s_per_iteration": per,
+                               "ratio": per[1] / per[0] if per[0] > 0 else None,
+                               "expected_ratio": 2.0}
+    return out
 
 
 def run_reference(args, shape):
     rank, world, _ = _rank_env()
     if rank != 0:
         return
-    from oracle import ref
+    from oracle import port, ref
+    from libisdf_b200 import synth
 
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable":
                           "oracle/_ref/libisdf_ref.so not built (needs the reference checkout)"}))
         return
+    psi = _shape_psi(synth, shape, args.config)
+    w = port.weight(psi, shape.nocc, shape.nv1, shape.nc1, shape.nv2, shape.nc2)
+    cal = calibrate(shape, w)
     for _ in range(args.warmup):
-        reference_sample(shape, shape.kmeans_iters)
+        reference_sample(shape, psi, w, shape.kmeans_iters, cal)
     times = []
     info = None
     for _ in range(args.steps):
-        t, info = reference_sample(shape, shape.kmeans_iters)
+        t, info = reference_sample(shape, psi, w, shape.kmeans_iters, cal)
         times.append(t)
     t = float(np.mean(times))
     v = 1.0 / t
@@ -180,13 +292,364 @@ def run_reference(args, shape):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": shape.name, "ng": shape.ng, "nstate": shape.nstate,
-                       "mu": shape.mu, "kmeans_iters": shape.kmeans_iters,
-                       "selector": "Kmeans", "precision": "fp64"},
+            "config": _config(shape, args),
+            "extrapolated": bool(info["extrapolated"]),
             "cpu_baseline": dict(info, value=v, unit="solves/s"),
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    if not args.no_cpu_check:
+        line["extrapolation_check"] = extrapolation_check(shape, w)
     print(json.dumps(line), flush=True)
+
+
+def _config(shape, args, rep=None):
+    c = {"workload": shape.name, "ng": shape.ng, "nstate": shape.nstate, "mu": shape.mu,
+         "kmeans_iters_cap": shape.kmeans_iters, "selector": args.selector,
+         "precision": args.precision, "seed": SEEDS.get(args.config, 1)}
+    if args.selector == "qrcp":
+        c.update(qrcp_oversample=args.qrcp_factor, qrcp_seed=args.qrcp_seed)
+    if args.precision == "mixed":
+        c["mixed_slices"] = args.mixed_slices
+    if rep is not None:
+        c.update(rk_eff=rep.rk_eff, kmeans_iters=rep.kmeans_iters, npt=rep.npt,
+                 kmeans_search_frac=round(float(rep.kmeans_search_frac), 4))
+    return c
+
+
+def accuracy_vs_oracle(shape, psi, th_rows, rows, piv, rk, pairs_i, pairs_j, oracle_rows=None):
+    """Relative Frobenius error of theta and of the fitted pair densities
+    theta C on sampled grid rows and state pairs against the oracle's FP64 fit
+    of the same rows (oracle.fit.getbasis_rows: those rows of the full-size
+    fit, given the same pivots)."""
+    from oracle import fit as ofit
+
+    a = (shape.nocc, shape.nv1, shape.nc1, shape.nv2, shape.nc2)
+    th_o = oracle_rows if oracle_rows is not None else ofit.getbasis_rows(psi, *a, rk, piv, rows)
+    pm = psi[np.asarray(piv[:rk], dtype=np.int64)]
+    C = pm[:, pairs_i] * pm[:, pairs_j]
+    fd, fd_o = th_rows[:, :rk] @ C, th_o @ C
+    return {"fitted_densities_rel": float(np.linalg.norm(fd - fd_o) / np.linalg.norm(fd_o)),
+            "theta_rel": float(np.linalg.norm(th_rows[:, :rk] - th_o) / np.linalg.norm(th_o)),
+            "rows": int(len(rows)), "pairs": int(len(pairs_i)),
+            "against": "the oracle's FP64 fit (numpy restatement of getbasis_MPI) on those rows"}, th_o
+
+
+# ------------------------------------------------------------------ our arm
+class Timed:
+    """K solves on `stream` between two CUDA events, with per-solve events,
+    the library's stage times and an nvidia-smi clock record over the region."""
+
+    def __init__(self, torch, solve, stream, steps, device_index, dist=None):
+        lat, stage, launches = [], [], []
+        with ClockSampler(device_index) as clk:
+            e_start = torch.cuda.Event(enable_timing=True)
+            e_end = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            e_start.record(stream)
+            for _ in range(steps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                rep = solve()
+                e1.record(stream)
+                e1.synchronize()
+                lat.append(e0.elapsed_time(e1))
+                stage.append((rep.t_select_ms, rep.t_fit_ms, rep.t_solve_ms, rep.t_zct_ms,
+                              rep.t_chol_ms, rep.t_gemm_ms))
+                launches.append(rep.kernel_launches)
+            e_end.record(stream)
+            torch.cuda.synchronize()
+        self.t_ms = max_over_ranks(e_start.elapsed_time(e_end), dist, "cuda")
+        self.steps = steps
+        self.rep = rep
+        self.lat = lat
+        self.launches = int(sum(launches))
+        self.clocks = clk.summary()
+        med = lambda k: float(np.median([s_[k] for s_ in stage]))  # noqa: E731
+        self.stages = {"select_wall": med(0), "fit_wall": med(1), "zct_gemm": med(3),
+                       "cct_cholesky": med(4), "triangular_solve": med(2),
+                       "triangular_gemms": med(5)}
+
+    def summary(self, world):
+        return {"value": replica_value(world, self.steps, self.t_ms), "unit": "solves/s",
+                "steps": self.steps, "ms_per_step": self.t_ms / self.steps,
+                "latency_ms": {"p50": float(np.percentile(self.lat, 50)),
+                               "p99": float(np.percentile(self.lat, 99))},
+                "stages_ms": self.stages, "clocks": self.clocks}
+
+
+def _e2e(torch, solve, stream, d_psi, d_theta, h_psi, steps, dist):
+    """End to end from host buffers, as a caller that consumes theta on the
+    host runs it: every step copies its psi in (pinned host -> HBM), solves,
+    and copies theta out (HBM -> pinned host), in a steady pipeline: the psi
+    of step i+1 is copied in on an H2D stream and the theta of step i copied
+    out on a D2H stream while step i+1 solves (two device psi and theta
+    buffers when HBM allows, else one of each and those copies do not
+    overlap). Returns (ms, theta buffers, psi buffers, D2H bytes per step)."""
+    h_theta = torch.empty(d_theta.shape, dtype=torch.float64).pin_memory()
+    free_b, _ = torch.cuda.mem_get_info()
+    thetas = [d_theta]
+    if free_b > d_theta.numel() * 8 + (8 << 30):
+        thetas.append(torch.empty_like(d_theta))
+        free_b -= d_theta.numel() * 8
+    psis = [d_psi]
+    if free_b > d_psi.numel() * 8 + (8 << 30):
+        psis.append(torch.empty_like(d_psi))
+    copy_stream = torch.cuda.Stream()
+    h2d_stream = torch.cuda.Stream()
+    done = [None] * len(thetas)  # theta buffer copied out
+    used = [None] * len(psis)    # psi buffer no longer read by a solve
+    ready = [None] * len(psis)   # psi buffer holds its step's input
+
+    def fetch(k):
+        b = k % len(psis)
+        if used[b] is not None:
+            h2d_stream.wait_event(used[b])
+        with torch.cuda.stream(h2d_stream):
+            psis[b].copy_(h_psi, non_blocking=True)
+        ready[b] = torch.cuda.Event()
+        ready[b].record(h2d_stream)
+
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    h2d_stream.wait_event(e0)
+    fetch(0)
+    for i in range(steps):
+        pb, tb = i % len(psis), i % len(thetas)
+        stream.wait_event(ready[pb])
+        if done[tb] is not None:
+            stream.wait_event(done[tb])
+        if len(psis) > 1 and i + 1 < steps:
+            fetch(i + 1)  # into the other buffer, beside this solve
+        solve(thetas[tb], psis[pb])
+        solved = torch.cuda.Event()
+        solved.record(stream)
+        used[pb] = solved
+        if len(psis) == 1 and i + 1 < steps:
+            fetch(i + 1)
+        copy_stream.wait_event(solved)
+        with torch.cuda.stream(copy_stream):
+            # in 256 MB pieces, so that the library's small state reads of the
+            # next solve are not queued behind one long copy
+            src, dst = thetas[tb].view(-1), h_theta.view(-1)
+            piece = 1 << 25
+            for o in range(0, src.numel(), piece):
+                dst[o:o + piece].copy_(src[o:o + piece], non_blocking=True)
+        done[tb] = torch.cuda.Event()
+        done[tb].record(copy_stream)
+    stream.wait_stream(copy_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+    nb = (len(thetas), len(psis), int(h_theta.numel() * 8))
+    del thetas, psis, h_theta
+    return (ms,) + nb
+
+
+def run_ours(args, shape):
+    import torch
+
+    import libisdf_b200 as isdf
+    from libisdf_b200 import synth
+
+    rank, world, local = _rank_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    psi = _shape_psi(synth, shape, args.config)
+    ng, mu = shape.ng, shape.mu
+    h_psi = torch.from_numpy(np.ascontiguousarray(psi.T)).pin_memory()
+    d_psi = h_psi.cuda()
+    d_theta = torch.empty((mu, ng), dtype=torch.float64, device="cuda")
+    piv = np.zeros(ng, dtype=np.int32)
+    dom = isdf.Domain(length=(shape.length,) * 3, num_grid=(shape.n,) * 3)
+    stream = torch.cuda.Stream()
+    s1 = "QRCP" if args.selector == "qrcp" else "Kmeans"
+    mixed = args.precision == "mixed"
+    compare = mixed and not args.no_compare
+
+    def options(prec):
+        return isdf.Options(stream=stream.cuda_stream, precision=prec,
+                            qrcp_oversample=args.qrcp_factor, qrcp_seed=args.qrcp_seed,
+                            mixed_slices=args.mixed_slices)
+
+    opts = options(isdf.PRECISION_MIXED if mixed else isdf.PRECISION_FP64)
+    opts64 = options(isdf.PRECISION_FP64)
+
+    def solve(theta=None, psi_d=None, o=None):
+        return isdf.ISDF(d_psi if psi_d is None else psi_d, dom, shape.nocc, shape.nstate,
+                         shape.nv1, shape.nc1, shape.nv2, shape.nc2, mu,
+                         d_theta if theta is None else theta, piv, shape.kmeans_iters, s1=s1,
+                         options=o or opts)
+
+    fp64_peak = _fp64_peak_tflops(torch)
+    int8_peak = _int8_peak_tops(torch) if mixed else None
+    rng = np.random.default_rng(0)
+    rows = np.sort(rng.choice(ng, size=min(2048, ng), replace=False))
+    pi = shape.nocc - shape.nv1 + rng.integers(0, shape.nv1 + shape.nc1, size=1024)
+    pj = shape.nocc - shape.nv2 + rng.integers(0, shape.nv2 + shape.nc2, size=1024)
+    d_rows = torch.from_numpy(rows).cuda()
+
+    def theta_rows(rk):
+        return d_theta[:rk].index_select(1, d_rows).T.cpu().numpy()
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, args.warmup)):
+            solve()
+        main = Timed(torch, solve, stream, args.steps, local, dist)
+        rep = main.rep
+        rk = rep.rk_eff
+        th_main = theta_rows(rk) if rank == 0 else None
+        piv_main = piv[:rk].copy()
+        plain = None
+        if compare:
+            solve64 = lambda: solve(o=opts64)  # noqa: E731
+            for _ in range(3):
+                solve64()
+            plain = Timed(torch, solve64, stream, max(3, min(args.steps, 8)), local, dist)
+            th_plain = theta_rows(rk) if rank == 0 else None
+            assert np.array_equal(piv[:rk], piv_main), "piv differs between the forms"
+        if dist:
+            dist.barrier()
+        e2e_steps = max(8, args.steps)
+        e2e_ms, e2e_bufs, e2e_psi_bufs, d2h_theta = _e2e(
+            torch, lambda th, ps: solve(th, ps), stream, d_psi, d_theta, h_psi, e2e_steps, dist)
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    accuracy = {}
+    acc_main, th_o = accuracy_vs_oracle(shape, psi, th_main, rows, piv_main, rk, pi, pj)
+    accuracy["mixed" if mixed else "fp64"] = acc_main
+    if plain is not None:
+        accuracy["fp64"], _ = accuracy_vs_oracle(shape, psi, th_plain, rows, piv_main, rk, pi,
+                                                 pj, th_o)
+    peaks, peak_src = _measured_peaks()
+    v = replica_value(world, args.steps, main.t_ms)
+    S = args.mixed_slices
+    gemm_ms = main.stages["triangular_gemms"]
+    solve_ms = (plain or main).stages["triangular_solve"]
+    roof64 = None
+    if plain is not None or not mixed:
+        # k_trsm_ws, the two triangular sweeps of the FP64 form as in-place FP64
+        # tensor-core GEMMs: 2*Ng*rk^2 flops per solve over the stage's
+        # CUDA-event time (the k_trsm_ws launches plus the small k_build_w
+        # launches between them, so a slight underestimate of the kernel's
+        # own rate). DRAM traffic per launch: 8.40 B per grid row and solved
+        # column (ncu on the 40^3-grid case) x the mean solved width (rk/2 + 32).
+        ach = 2.0 * ng * rk * rk / (solve_ms * 1e-3) / 1e12 if solve_ms > 0 else None
+        roof64 = {"kernel": "k_trsm_ws (both sweeps of the FP64 triangular solve)",
+                  "bound": "tensor", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                  "frac": (ach / fp64_peak) if ach else None,
+                  "peak_source": ("cuBLAS DGEMM 8192^3 measured in this run: the FP64 "
+                                  "denominator (the measured-peaks file holds HBM and BF16 "
+                                  f"figures only; HBM {peaks.get('hbm_gbs')} GB/s from "
+                                  f"{peak_src})"),
+                  "traffic": 8.40 * ng * (rk / 2 + 32),
+                  "traffic_note": "bytes per launch (mean over the sweep), scaled from the "
+                                  "ncu capture at Ng = 64000 by rows x solved columns"}
+    if mixed:
+        # k_ozaki_gemm, the two triangular products Y = Z L^-T and theta = Y L^-1
+        # as INT8 digit-pair GEMMs: issued INT8 ops per solve 2 GEMMs x 2 x Ng x
+        # rk x (rk/2 + 32) x S(S+1)/2 (each tile runs the K range its triangular
+        # factor leaves nonzero), over CUDA events around the two launches.
+        ops = 2 * 2.0 * ng * rk * (rk / 2 + 32) * S * (S + 1) / 2
+        ach = ops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
+        roofline = {"kernel": "k_ozaki_gemm (Y = Z L^-T and theta = Y L^-1, INT8 digit pairs)",
+                    "bound": "tensor", "achieved": ach, "peak": int8_peak[0],
+                    "unit": "TOPS (INT8)", "frac": (ach / int8_peak[0]) if ach else None,
+                    "peak_source": int8_peak[1],
+                    "emulated_fp64_tflops": (2.0 * 2 * ng * rk * (rk / 2 + 32) /
+                                             (gemm_ms * 1e-3) / 1e12) if gemm_ms > 0 else None,
+                    "traffic": None}
+    else:
+        roofline = roof64
+    line = {
+        "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": main.t_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": dict(_config(shape, args, rep), parallelism=f"replicas x{world}",
+                       l2=(f"inputs larger than L2 (psi {ng * shape.nstate * 8 / 1e9:.2f} GB, "
+                           f"theta {ng * mu * 8 / 1e9:.2f} GB; L2 126 MB)")),
+        "latency_ms": main.summary(world)["latency_ms"],
+        "stages_ms": main.stages,
+        "roofline": roofline,
+        "e2e": {"value": replica_value(world, e2e_steps, e2e_ms), "unit": "solves/s",
+                "h2d_bytes_per_step": int(h_psi.numel() * 8),
+                "d2h_bytes_per_step": int(d2h_theta + piv.nbytes),
+                "steps": e2e_steps, "theta_buffers": e2e_bufs, "psi_buffers": e2e_psi_bufs,
+                "form": args.precision},
+        "gpu_launches": main.launches,
+        "accuracy_vs_oracle": accuracy,
+        "clocks": main.clocks,
+    }
+    if plain is not None:
+        p = plain.summary(world)
+        line["plain_fp64"] = dict(p, roofline=roof64)
+        line["mixed_over_plain"] = v / p["value"]
+    if not args.no_secondary and shape is not synth.SI64 and world == 1:
+        # the headline's buffers go first (the solve closures hold them)
+        d_psi = d_theta = h_psi = d_rows = None
+        line["secondary"] = secondary_si64(torch, isdf, synth, fp64_peak)
+    if world == 1 and not args.no_cpu_baseline and s1 == "QRCP":
+        line["cpu_baseline"] = {"value": None, "unit": "solves/s",
+                                "unavailable": "the reference's QRCP selector runs ScaLAPACK "
+                                               "pdgeqpf, which cannot be built here"}
+    elif world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import port
+
+            w = port.weight(psi, shape.nocc, shape.nv1, shape.nc1, shape.nv2, shape.nc2)
+            t_cpu, info = reference_sample(shape, psi, w, rep.kmeans_iters, calibrate(shape, w))
+            line["cpu_baseline"] = dict(info, value=1.0 / t_cpu, unit="solves/s")
+        except Exception as e:  # the reference build is optional on the box
+            line["cpu_baseline"] = {"value": None, "unit": "solves/s",
+                                    "unavailable": str(e)[:200]}
+    print(json.dumps(line), flush=True)
+
+
+def secondary_si64(torch, isdf, synth, fp64_peak):
+    """The Si64-like plain FP64 solve (80^3, 256 states, mu = 2048, K-means),
+    a short run beside the headline: solves/s, stages and clocks."""
+    torch.cuda.empty_cache()
+    s = synth.SI64
+    psi = _shape_psi(synth, s, "si64")
+    d_psi = torch.from_numpy(np.ascontiguousarray(psi.T)).cuda()
+    d_theta = torch.empty((s.mu, s.ng), dtype=torch.float64, device="cuda")
+    piv = np.zeros(s.ng, dtype=np.int32)
+    dom = isdf.Domain(length=(s.length,) * 3, num_grid=(s.n,) * 3)
+    stream = torch.cuda.Stream()
+    opts = isdf.Options(stream=stream.cuda_stream)
+
+    def solve():
+        return isdf.ISDF(d_psi, dom, s.nocc, s.nstate, s.nv1, s.nc1, s.nv2, s.nc2, s.mu, d_theta,
+                         piv, s.kmeans_iters, options=opts)
+
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            solve()
+        t = Timed(torch, solve, stream, 5, 0)
+    out = t.summary(1)
+    rk = t.rep.rk_eff
+    ms = out["stages_ms"]["triangular_solve"]
+    ach = 2.0 * s.ng * rk * rk / (ms * 1e-3) / 1e12 if ms > 0 else None
+    out.update(workload=s.name, precision="fp64", rk_eff=rk, kmeans_iters=t.rep.kmeans_iters,
+               roofline={"kernel": "k_trsm_ws", "achieved": ach, "peak": fp64_peak,
+                         "unit": "TFLOP/s", "frac": (ach / fp64_peak) if ach else None})
+    return out
 
 
 def _int8_peak_tops(torch):
@@ -213,279 +676,6 @@ def _int8_peak_tops(torch):
         peaks, _ = _measured_peaks()
         return 2.0 * peaks["bf16_tflops"], f"2 x measured dense BF16 (INT8 GEMM unavailable: {e})"
 
-
-def mixed_vs_fp64(torch, shape, psi, d_theta, piv, rk, solve_fp64, n_rows=2048, n_pairs=1024,
-                  seed=0):
-    """Accuracy of the mixed-precision result in d_theta against the FP64
-    form on the same inputs: relative Frobenius error of the fitted pair
-    densities theta C (and of theta) on sampled grid rows and pairs. Runs one
-    FP64 solve into d_theta (outside any timed region)."""
-    rng = np.random.default_rng(seed)
-    ng = psi.shape[0]
-    rows = np.sort(rng.choice(ng, size=min(n_rows, ng), replace=False))
-    idx = torch.from_numpy(rows).cuda()
-    th_m = d_theta[:rk].index_select(1, idx).T.cpu().numpy()
-    piv_m = piv[:rk].copy()
-    solve_fp64()
-    th_f = d_theta[:rk].index_select(1, idx).T.cpu().numpy()
-    if not np.array_equal(piv_m, piv[:rk]):
-        return {"error": "piv differs between the forms"}
-    lo1, lo2 = shape.nocc - shape.nv1, shape.nocc - shape.nv2
-    i = lo1 + rng.integers(0, shape.nv1 + shape.nc1, size=n_pairs)
-    j = lo2 + rng.integers(0, shape.nv2 + shape.nc2, size=n_pairs)
-    pm = psi[piv_m]  # rk x nstate
-    C = pm[:, i] * pm[:, j]
-    fd_m, fd_f = th_m @ C, th_f @ C
-    return {"fitted_densities_rel": float(np.linalg.norm(fd_m - fd_f) / np.linalg.norm(fd_f)),
-            "theta_rel": float(np.linalg.norm(th_m - th_f) / np.linalg.norm(th_f)),
-            "rows": int(len(rows)), "pairs": int(n_pairs),
-            "against": "the FP64 form on the same inputs (parity-tested against the oracle)"}
-
-
-# ------------------------------------------------------------------ our arm
-def run_ours(args, shape):
-    import torch
-
-    import libisdf_b200 as isdf
-    from libisdf_b200 import synth
-
-    rank, world, local = _rank_env()
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    psi = synth.shape_orbitals(shape, 1, device="cuda")
-    ng, mu = shape.ng, shape.mu
-    h_psi = torch.from_numpy(np.ascontiguousarray(psi.T)).pin_memory()
-    d_psi = h_psi.cuda()
-    d_theta = torch.empty((mu, ng), dtype=torch.float64, device="cuda")
-    piv = np.zeros(ng, dtype=np.int32)
-    dom = isdf.Domain(length=(shape.length,) * 3, num_grid=(shape.n,) * 3)
-    stream = torch.cuda.Stream()
-    prec = isdf.PRECISION_MIXED if args.precision == "mixed" else isdf.PRECISION_FP64
-    opts = isdf.Options(stream=stream.cuda_stream, precision=prec,
-                        qrcp_oversample=args.qrcp_factor, qrcp_seed=args.qrcp_seed,
-                        mixed_slices=args.mixed_slices)
-    s1 = "QRCP" if args.selector == "qrcp" else "Kmeans"
-
-    def solve(theta=None, psi_d=None):
-        return isdf.ISDF(d_psi if psi_d is None else psi_d, dom, shape.nocc, shape.nstate,
-                         shape.nv1, shape.nc1, shape.nv2, shape.nc2, mu,
-                         d_theta if theta is None else theta, piv, shape.kmeans_iters, s1=s1,
-                         options=opts)
-
-    fp64_peak = _fp64_peak_tflops(torch)
-    int8_peak = _int8_peak_tops(torch) if args.precision == "mixed" else None
-    with torch.cuda.stream(stream):
-        for _ in range(max(3, args.warmup)):
-            rep = solve()
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        lat = []
-        stage = []
-        launches = []
-        with ClockSampler(local) as clk:
-            e_start = torch.cuda.Event(enable_timing=True)
-            e_end = torch.cuda.Event(enable_timing=True)
-            torch.cuda.synchronize()
-            e_start.record(stream)
-            for _ in range(args.steps):
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                rep = solve()
-                e1.record(stream)
-                e1.synchronize()
-                lat.append(e0.elapsed_time(e1))
-                stage.append((rep.t_select_ms, rep.t_fit_ms, rep.t_solve_ms, rep.t_zct_ms,
-                              rep.t_chol_ms, rep.t_gemm_ms))
-                launches.append(rep.kernel_launches)
-            e_end.record(stream)
-            torch.cuda.synchronize()
-        t_ms = max_over_ranks(e_start.elapsed_time(e_end), dist, "cuda")
-        if dist:
-            dist.barrier()
-
-        # End to end from host buffers, as a caller that consumes theta on the
-        # host runs it: every step copies its psi in (pinned host -> HBM),
-        # solves, and copies theta out (HBM -> pinned host), in a steady
-        # pipeline: the psi of step i+1 is copied in on an H2D stream and the
-        # theta of step i copied out on a D2H stream while step i+1 solves
-        # (two device psi and theta buffers when HBM allows, else one of each
-        # and those copies do not overlap). At least 8 steps, so that the
-        # pipeline's fill and drain are a small part of the timed region.
-        h_theta = torch.empty((mu, ng), dtype=torch.float64).pin_memory()
-        e2e_steps = max(8, args.steps)
-        free_b, _ = torch.cuda.mem_get_info()
-        thetas = [d_theta]
-        if free_b > d_theta.numel() * 8 + (8 << 30):
-            thetas.append(torch.empty_like(d_theta))
-            free_b -= d_theta.numel() * 8
-        psis = [d_psi]
-        if free_b > d_psi.numel() * 8 + (8 << 30):
-            psis.append(torch.empty_like(d_psi))
-        copy_stream = torch.cuda.Stream()
-        h2d_stream = torch.cuda.Stream()
-        done = [None] * len(thetas)      # theta buffer copied out
-        used = [None] * len(psis)        # psi buffer no longer read by a solve
-        ready = [None] * len(psis)       # psi buffer holds its step's input
-
-        def fetch(k):
-            b = k % len(psis)
-            if used[b] is not None:
-                h2d_stream.wait_event(used[b])
-            with torch.cuda.stream(h2d_stream):
-                psis[b].copy_(h_psi, non_blocking=True)
-            ready[b] = torch.cuda.Event()
-            ready[b].record(h2d_stream)
-
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        h2d_stream.wait_event(e0)
-        fetch(0)
-        for i in range(e2e_steps):
-            pb, tb = i % len(psis), i % len(thetas)
-            stream.wait_event(ready[pb])
-            if done[tb] is not None:
-                stream.wait_event(done[tb])
-            if len(psis) > 1 and i + 1 < e2e_steps:
-                fetch(i + 1)  # into the other buffer, beside this solve
-            rep = solve(thetas[tb], psis[pb])
-            solved = torch.cuda.Event()
-            solved.record(stream)
-            used[pb] = solved
-            if len(psis) == 1 and i + 1 < e2e_steps:
-                fetch(i + 1)
-            copy_stream.wait_event(solved)
-            with torch.cuda.stream(copy_stream):
-                # in 256 MB pieces, so that the library's small state reads
-                # of the next solve are not queued behind one long copy
-                src, dst = thetas[tb].view(-1), h_theta.view(-1)
-                piece = 1 << 25
-                for o in range(0, src.numel(), piece):
-                    dst[o:o + piece].copy_(src[o:o + piece], non_blocking=True)
-            done[tb] = torch.cuda.Event()
-            done[tb].record(copy_stream)
-        stream.wait_stream(copy_stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
-        e2e_bufs = len(thetas)
-        e2e_psi_bufs = len(psis)
-        del thetas, psis
-
-    if dist:
-        dist.destroy_process_group()
-    if rank != 0:
-        return
-    accuracy = None
-    if args.precision == "mixed":
-        opts64 = isdf.Options(stream=stream.cuda_stream, precision=isdf.PRECISION_FP64,
-                              qrcp_oversample=args.qrcp_factor, qrcp_seed=args.qrcp_seed)
-
-        def solve_fp64():
-            with torch.cuda.stream(stream):
-                isdf.ISDF(d_psi, dom, shape.nocc, shape.nstate, shape.nv1, shape.nc1, shape.nv2,
-                          shape.nc2, mu, d_theta, piv, shape.kmeans_iters, s1=s1, options=opts64)
-            torch.cuda.synchronize()
-
-        accuracy = mixed_vs_fp64(torch, shape, psi, d_theta, piv, rep.rk_eff, solve_fp64)
-    peaks, peak_src = _measured_peaks()
-    v = replica_value(world, args.steps, t_ms)
-    rk = rep.rk_eff
-    t_solve_ms = float(np.median([s[2] for s in stage]))
-    t_gemm_ms = float(np.median([s[5] for s in stage]))
-    if args.precision == "mixed":
-        # Dominant kernel: k_ozaki_gemm, the two triangular products
-        # Y = Z L^-T and theta = Y L^-1 as INT8 digit-pair GEMMs; issued INT8
-        # ops per solve: 2 GEMMs x 2 x Ng x rk x (rk/2 + 32) x S(S+1)/2 (each
-        # tile runs the K range its triangular factor leaves nonzero). Time:
-        # CUDA events around the two launches on the solve stream.
-        S = args.mixed_slices
-        ops = 2 * 2.0 * ng * rk * (rk / 2 + 32) * S * (S + 1) / 2
-        achieved = ops / (t_gemm_ms * 1e-3) / 1e12 if t_gemm_ms > 0 else None
-        roofline = {"kernel": "k_ozaki_gemm (Y = Z L^-T and theta = Y L^-1, INT8 digit pairs)",
-                    "bound": "tensor", "achieved": achieved, "peak": int8_peak[0],
-                    "unit": "TOPS (INT8)", "frac": (achieved / int8_peak[0]) if achieved else None,
-                    "peak_source": int8_peak[1],
-                    "emulated_fp64_tflops": (2.0 * 2 * ng * rk * (rk / 2 + 32) /
-                                             (t_gemm_ms * 1e-3) / 1e12) if t_gemm_ms > 0 else None,
-                    "traffic": None}
-    else:
-        # Dominant kernel: k_trsm_ws, the two triangular sweeps as in-place
-        # FP64 tensor-core GEMMs (warp-specialised bulk-copy tile). Algorithmic flops per solve: 2*Ng*rk^2
-        # (Ng*rk^2 per sweep). Its time is the triangular-solve stage on the
-        # solve stream (CUDA events in the library around the stage: the
-        # k_trsm_ws launches plus the small k_build_w launches between
-        # them), so the rate is a slight underestimate of the kernel's own.
-        achieved = 2.0 * ng * rk * rk / (t_solve_ms * 1e-3) / 1e12 if t_solve_ms > 0 else None
-        # DRAM traffic of one launch: 8.40 B per grid row and solved column
-        # (dram__bytes_read.sum + dram__bytes_write.sum of ncu on the 40^3-grid
-        # case), times the mean solved width of a launch over both sweeps
-        # (rk/2 + 32 columns).
-        roofline = {"kernel": "k_trsm_ws (both sweeps of the triangular solve)",
-                    "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
-                    "unit": "TFLOP/s", "frac": (achieved / fp64_peak) if achieved else None,
-                    "peak_source": ("cuBLAS DGEMM 8192^3 measured in this run: the FP64 "
-                                    "denominator (the measured-peaks file holds HBM and BF16 "
-                                    f"figures only; HBM {peaks.get('hbm_gbs')} GB/s from "
-                                    f"{peak_src})"),
-                    "traffic": 8.40 * ng * (rk / 2 + 32),
-                    "traffic_note": "bytes per launch (mean over the sweep), scaled from the "
-                                    "ncu capture at Ng = 64000 by rows x solved columns"}
-    line = {
-        "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-        "warmup": max(3, args.warmup), "ms_per_step": t_ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
-        "config": {"workload": shape.name, "ng": ng, "nstate": shape.nstate, "mu": mu,
-                   "rk_eff": rk, "kmeans_iters": rep.kmeans_iters, "npt": rep.npt,
-                   "kmeans_search_frac": round(float(rep.kmeans_search_frac), 4), "selector": s1,
-                   **({"qrcp_oversample": args.qrcp_factor, "qrcp_seed": args.qrcp_seed}
-                      if s1 == "QRCP" else {}),
-                   "precision": args.precision,
-                   **({"mixed_slices": args.mixed_slices} if args.precision == "mixed" else {}),
-                   "parallelism": f"replicas x{world}",
-                   "l2": (f"inputs larger than L2 (psi {ng * shape.nstate * 8 / 1e9:.2f} GB, "
-                          f"theta {ng * mu * 8 / 1e9:.2f} GB; L2 126 MB)")},
-        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
-        "stages_ms": {"select_wall": float(np.median([s[0] for s in stage])),
-                      "fit_wall": float(np.median([s[1] for s in stage])),
-                      "zct_gemm": float(np.median([s[3] for s in stage])),
-                      "cct_cholesky": float(np.median([s[4] for s in stage])),
-                      "triangular_solve": t_solve_ms,
-                      "triangular_gemms": t_gemm_ms},
-        "roofline": roofline,
-        "e2e": {"value": replica_value(world, e2e_steps, e2e_ms), "unit": "solves/s",
-                "h2d_bytes_per_step": int(h_psi.numel() * 8),
-                "d2h_bytes_per_step": int(h_theta.numel() * 8 + piv.nbytes),
-                "steps": e2e_steps, "theta_buffers": e2e_bufs, "psi_buffers": e2e_psi_bufs},
-        "gpu_launches": int(sum(launches)),
-        "mixed_vs_fp64": accuracy,
-        "clocks": clk.summary(),
-    }
-    if world == 1 and not args.no_cpu_baseline and s1 == "QRCP":
-        line["cpu_baseline"] = {"value": None, "unit": "solves/s",
-                                "unavailable": "the reference's QRCP selector runs ScaLAPACK "
-                                               "pdgeqpf, which cannot be built here"}
-    elif world == 1 and not args.no_cpu_baseline:
-        try:
-            t_cpu, info = reference_sample(shape, rep.kmeans_iters)
-            line["cpu_baseline"] = dict(info, value=1.0 / t_cpu, unit="solves/s")
-        except Exception as e:  # the reference build is optional on the box
-            line["cpu_baseline"] = {"value": None, "unit": "solves/s",
-                                    "unavailable": str(e)[:200]}
-    print(json.dumps(line), flush=True)
 
 
 def run_select(args, shape):
@@ -662,8 +852,14 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["si8", "si64", "si216", "si64c"], default="si64")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--config", choices=["si8", "si64", "si216", "si64c"], default="si216")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="mixed precision: skip the plain FP64 run of the same workload")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the short Si64-like plain FP64 run beside the headline")
+    ap.add_argument("--no-cpu-check", action="store_true",
+                    help="reference arm: skip the whole Si8-like reference solve")
     ap.add_argument("--mixed-slices", type=int, choices=[5, 6, 7], default=6,
                     help="INT8 digits per operand in the mixed form (Options.mixed_slices)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -675,7 +871,7 @@ def main():
                     help="select: time the K-means selection alone (profiling aid)")
     ap.add_argument("--serve", action="store_true",
                     help="the serving mix through isdf_server_* (Poisson arrivals)")
-    ap.add_argument("--requests", type=int, default=128)
+    ap.add_argument("--requests", type=int, default=512)
     ap.add_argument("--rate", type=float, default=4.0, help="arrivals per second (--serve)")
     ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--serve-seed", type=int, default=7)
