@@ -49,12 +49,15 @@ def getbasis(psi, nocc, nv1, nc1, nv2, nc2, rk, piv):
     return np.asfortranarray(th.T)
 
 
-def getbasis_rows(psi, nocc, nv1, nc1, nv2, nc2, rk, piv, rows):
+def getbasis_rows(psi, nocc, nv1, nc1, nv2, nc2, rk, piv, rows, solver="cholesky"):
     """theta restricted to the grid rows `rows` (len(rows) x rk): the same
     operations as getbasis, but Z C^T is formed only on those rows and on the
     rk interpolation rows that C C^T is gathered from (getbasis_MPI.cpp:188-214).
     Each row of theta depends only on its own row of Z C^T, so this is the
-    full-size fit evaluated where it is compared, at a cost independent of Ng."""
+    full-size fit evaluated where it is compared, at a cost independent of Ng.
+    solver="lu" solves the same system by LU instead of Cholesky and two
+    triangular solves: a second correct FP64 ordering, whose distance from the
+    first measures how far FP64 rounding alone moves the result."""
     psi = np.asarray(psi)
     p = np.asarray(piv[:rk], dtype=np.int64)
     rows = np.asarray(rows, dtype=np.int64)
@@ -70,8 +73,10 @@ def getbasis_rows(psi, nocc, nv1, nc1, nv2, nc2, rk, piv, rows):
     # Z C^T on the interpolation rows: row j is grid row piv[j], so C C^T
     # gathers cc[mu, nu] = zp[nu, mu]
     cc, _ = cct(z(p), rk, np.arange(rk))
-    L = np.linalg.cholesky(cc)
     zr = z(rows)
+    if solver == "lu":
+        return np.asfortranarray(sl.solve(cc.T, zr.T, assume_a="gen").T)
+    L = np.linalg.cholesky(cc)
     y = sl.solve_triangular(L, zr.T, lower=True)
     th = sl.solve_triangular(L, y, lower=True, trans="T")
     return np.asfortranarray(th.T)

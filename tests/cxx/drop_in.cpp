@@ -5,7 +5,7 @@
 // d_thetaCol, piv, KmeansMaxIter_ISDF, check)), compiled against
 // include/isdf.hpp and linked to libisdf_b200.so instead of the reference.
 //
-// usage: drop_in psi.bin nx ny nz L nstate nocc nv1 nc1 nv2 nc2 mu iters out_prefix
+// usage: drop_in psi.bin nx ny nz L nstate nocc nv1 nc1 nv2 nc2 mu iters qrcp_mu out_prefix
 // psi.bin: Ng x nstate doubles, column-major. Writes out_prefix.kmeans.piv and
 // out_prefix.qrcp.piv (int32[Ng]) and prints one line per call.
 #include <cuda_runtime.h>
@@ -29,8 +29,9 @@ static bool write_ints(const std::string& path, const std::vector<int>& v) {
 }
 
 int main(int argc, char** argv) {
-  if (argc != 15) {
-    std::fprintf(stderr, "usage: %s psi.bin nx ny nz L nstate nocc nv1 nc1 nv2 nc2 mu iters out\n",
+  if (argc != 16) {
+    std::fprintf(stderr,
+                 "usage: %s psi.bin nx ny nz L nstate nocc nv1 nc1 nv2 nc2 mu iters qrcp_mu out\n",
                  argv[0]);
     return 2;
   }
@@ -44,7 +45,9 @@ int main(int argc, char** argv) {
   const int Nv1 = std::atoi(argv[8]), Nc1 = std::atoi(argv[9]);
   const int Nv2 = std::atoi(argv[10]), Nc2 = std::atoi(argv[11]);
   const int Nu = std::atoi(argv[12]), KmeansMaxIter_ISDF = std::atoi(argv[13]);
-  const std::string out = argv[14];
+  // the QRCP sketch width IRound(sqrt(1.5 mu)) must not exceed a state window
+  const int NuQ = std::atoi(argv[14]);
+  const std::string out = argv[15];
   const int Nr = domain_.NumGridTotal();
 
   std::vector<double> psirow((size_t)Nr * nstate);
@@ -73,7 +76,7 @@ int main(int argc, char** argv) {
 
   // 2. the overload with the selector of the reference's CPU entry point
   std::string s1 = "QRCP";
-  isdffunc::ISDF(d_psirow, domain_, nocc, nstate, Nv1, Nc1, Nv2, Nc2, Nu, d_theta, piv.data(),
+  isdffunc::ISDF(d_psirow, domain_, nocc, nstate, Nv1, Nc1, Nv2, Nc2, NuQ, d_theta, piv.data(),
                  KmeansMaxIter_ISDF, s1, false);
   std::printf("qrcp ok piv0=%d\n", piv[0]);
   if (!write_ints(out + ".qrcp.piv", piv)) return 4;

@@ -3,7 +3,8 @@ the reference's example driver does (examples/si8/readpsi.cpp:219-237), is
 compiled against include/isdf.hpp and linked to libisdf_b200.so, and runs the
 reference's own Si8 example data (16^3 grid, 35 states, Nv = 16, Nc = 0,
 mu = 192, 500 K-means iterations, check on). piv must equal the reference's
-(the golden made by the reference's own code), the QRCP overload must give
+(the golden made by the reference's own code), the QRCP overload (mu = 160:
+the sketch width IRound(sqrt(1.5 mu)) must fit the 16-state window) must give
 the same pivots as the Python binding, and failures must arrive as
 std::runtime_error with the library's message."""
 import os
@@ -45,8 +46,9 @@ def test_cxx_caller_runs_the_reference_example(torch_cuda, tmp_path):
     (tmp_path / "psi.bin").write_bytes(psi.tobytes(order="F"))
     exe = _build(tmp_path)
     out = tmp_path / "out"
+    mu_q = 160
     r = subprocess.run([str(exe), str(tmp_path / "psi.bin"), *map(str, n), repr(length),
-                        str(nstate), *map(str, a), str(mu), str(iters), str(out)],
+                        str(nstate), *map(str, a), str(mu), str(iters), str(mu_q), str(out)],
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     lines = r.stdout.splitlines()
@@ -55,10 +57,10 @@ def test_cxx_caller_runs_the_reference_example(torch_cuda, tmp_path):
     # the QRCP overload against the Python binding on the same inputs
     piv_q = np.fromfile(str(out) + ".qrcp.piv", dtype=np.int32)
     d_psi = torch_cuda.from_numpy(np.ascontiguousarray(psi.T)).cuda()
-    d_theta = torch_cuda.empty((mu, ng), dtype=torch_cuda.float64, device="cuda")
+    d_theta = torch_cuda.empty((mu_q, ng), dtype=torch_cuda.float64, device="cuda")
     piv_py = np.zeros(ng, dtype=np.int32)
     isdf.ISDF(d_psi, isdf.Domain(length=(length,) * 3, num_grid=tuple(n)), a[0], nstate, *a[1:],
-              mu, d_theta, piv_py, iters, s1="QRCP")
+              mu_q, d_theta, piv_py, iters, s1="QRCP")
     assert np.array_equal(piv_q, piv_py)
     assert "caught: Wrong select points method" in lines
     assert any(l.startswith("caught: mu outside") for l in lines), lines
