@@ -155,6 +155,23 @@ int isdf_check(const isdf_domain_t* dom, const double* d_psi, int nocc, int nsta
                int nc1, int nv2, int nc2, int rk, const int* piv, const double* d_theta,
                double* fit_err, double* coul_err, void* stream);
 
+/* No counterpart in the reference: its check (src/common/checkcode.cpp:54-313)
+ * covers all Npair = (nv1+nc1)(nv2+nc2) pairs at O(Ng * Npair^2) and is out of
+ * reach beyond the Si8-like size. This extension computes the same two errors
+ * restricted to a caller-chosen list of state pairs (pair index
+ * (k - (nocc-nv1)) * (nv2+nc2) + (j - (nocc-nv2)), the reference's numbering,
+ * checkcode.cpp:62-73): the fit error ||rho - theta C||_F / ||rho||_F over all
+ * grid points of those pairs, and the relative truncated-Coulomb error of the
+ * pair block (ij|V|kl), ij, kl in the list, with the ISDF form evaluated from
+ * the spectra of the fitted densities theta c_ij (by linearity of the FFT the
+ * reference's c_ij^T Re(zeta^H V zeta) c_kl). With the list of all pairs it
+ * gives isdf_check()'s numbers. pairs: host int[npair_sample], 1 <=
+ * npair_sample <= 4096; piv: host, first rk entries used. */
+int isdf_check_sampled(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate,
+                       int nv1, int nc1, int nv2, int nc2, int rk, const int* piv,
+                       const double* d_theta, int npair_sample, const int* pairs,
+                       double* fit_err, double* coul_err, void* stream);
+
 /* Size of the fixed device scratch array behind isdf_fit_noalloc(). */
 #define ISDF_NOALLOC_SCRATCH_BYTES (8u << 20)
 

@@ -196,6 +196,9 @@ def lib() -> ctypes.CDLL:
         L.isdf_fit.restype = I
         L.isdf_check.argtypes = [ctypes.POINTER(_Domain), P, I, I, I, I, I, I, I, P, P, P, P, P]
         L.isdf_check.restype = I
+        L.isdf_check_sampled.argtypes = [ctypes.POINTER(_Domain), P, I, I, I, I, I, I, I, P, P, I,
+                                         P, P, P, P]
+        L.isdf_check_sampled.restype = I
         L.isdf_last_error.restype = ctypes.c_char_p
         L.isdf_status_string.argtypes = [I]
         L.isdf_status_string.restype = ctypes.c_char_p
@@ -297,6 +300,23 @@ def check(domain: Domain, d_psi, nocc: int, nstate: int, nv1: int, nc1: int, nv2
     _check(lib().isdf_check(ctypes.byref(d), _dptr(d_psi), nocc, nstate, nv1, nc1, nv2, nc2, rk,
                             piv.ctypes.data, _dptr(d_theta), ctypes.addressof(fe),
                             ctypes.addressof(ce), stream or None))
+    return fe.value, ce.value
+
+
+def check_sampled(domain: Domain, d_psi, nocc: int, nstate: int, nv1: int, nc1: int, nv2: int,
+                  nc2: int, rk: int, piv: np.ndarray, d_theta, pairs, stream: int = 0):
+    """(fit error, Coulomb error) of theta restricted to the listed state pairs
+    (pair index (k - (nocc-nv1)) * (nv2+nc2) + (j - (nocc-nv2))): the check at
+    sizes where all pairs are out of reach. No counterpart in the reference."""
+    piv = np.ascontiguousarray(piv, dtype=np.int32)
+    pairs = np.ascontiguousarray(pairs, dtype=np.int32)
+    fe = ctypes.c_double(0.0)
+    ce = ctypes.c_double(0.0)
+    d = domain._c()
+    _check(lib().isdf_check_sampled(ctypes.byref(d), _dptr(d_psi), nocc, nstate, nv1, nc1, nv2,
+                                    nc2, rk, piv.ctypes.data, _dptr(d_theta), len(pairs),
+                                    pairs.ctypes.data, ctypes.addressof(fe),
+                                    ctypes.addressof(ce), stream or None))
     return fe.value, ce.value
 
 

@@ -483,6 +483,53 @@ int isdf_check(const isdf_domain_t* dom, const double* d_psi, int nocc, int nsta
   }
 }
 
+int isdf_check_sampled(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate,
+                       int nv1, int nc1, int nv2, int nc2, int rk, const int* piv,
+                       const double* d_theta, int npair_sample, const int* pairs,
+                       double* fit_err, double* coul_err, void* stream) {
+  try {
+    if (!dom || !d_psi || !d_theta || !piv || !pairs || !fit_err || !coul_err)
+      return record_error(ISDF_ERR_ARG, "null pointer");
+    const long long ng = (long long)dom->num_grid[0] * dom->num_grid[1] * dom->num_grid[2];
+    if (ng <= 0 || rk <= 0 || rk > ng) return record_error(ISDF_ERR_ARG, "sizes");
+    ISDF_TRY(check_state_ranges(nocc, nstate, nv1, nc1, nv2, nc2));
+    const int npair = (nv1 + nc1) * (nv2 + nc2);
+    if (npair_sample < 1 || npair_sample > 4096)
+      return record_error(ISDF_ERR_ARG, "sampled check: npair_sample in [1, 4096]");
+    for (int i = 0; i < npair_sample; ++i)
+      if (pairs[i] < 0 || pairs[i] >= npair)
+        return record_error(ISDF_ERR_ARG, "sampled check: pair index outside [0, Npair)");
+    for (int j = 0; j < rk; ++j)
+      if (piv[j] < 0 || piv[j] >= ng) return record_error(ISDF_ERR_ARG, "pivot outside the grid");
+    const size_t need = check_sampled_workspace_bytes(dom->num_grid, rk, npair_sample);
+    if (need > kCheckMaxBytes)
+      return record_error(ISDF_ERR_UNSUPPORTED, "sampled check: buffers exceed the device budget");
+    std::lock_guard<std::mutex> lock(workspace_mutex());
+    Arena arena;
+    cudaStream_t ls;
+    ISDF_TRY(acquire_workspace(need + 4096, &arena, &ls));
+    CheckArgs ca;
+    ca.d_psi = d_psi;
+    for (int i = 0; i < 3; ++i) {
+      ca.num_grid[i] = dom->num_grid[i];
+      ca.length[i] = dom->length[i];
+    }
+    ca.nstate = nstate;
+    ca.nocc = nocc;
+    ca.nv1 = nv1;
+    ca.nc1 = nc1;
+    ca.nv2 = nv2;
+    ca.nc2 = nc2;
+    ca.rk = rk;
+    ca.piv = piv;
+    ca.d_theta = d_theta;
+    return check_sampled_run(ca, pairs, npair_sample, arena, stream ? (cudaStream_t)stream : ls,
+                             fit_err, coul_err);
+  } catch (const std::exception& e) {
+    return record_error(ISDF_ERR_NOMEM, e.what());
+  }
+}
+
 const char* isdf_last_error(void) { return last_error_message(); }
 
 const char* isdf_status_string(int code) {

@@ -95,6 +95,35 @@ __global__ void k_cmat(const double* __restrict__ psi, long long ng, const int* 
   }
 }
 
+// Sampled pairs: rho columns [p0, p0 + b) of the listed pairs, pair index
+// (k - lo1) * n2 + (j - lo2) as checkcode.cpp:62-73 numbers them.
+__global__ void k_rho_list(const double* __restrict__ psi, long long ng, int lo1, int lo2, int n2,
+                           const int* __restrict__ pairs, int p0, int b,
+                           double* __restrict__ rho) {
+  const long long total = ng * b;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e % ng;
+    const int pair = pairs[p0 + (int)(e / ng)];
+    rho[e] = psi[r + (long long)(lo1 + pair / n2) * ng] * psi[r + (long long)(lo2 + pair % n2) * ng];
+  }
+}
+
+// Depth-major C of the listed pairs: Cb[mu * b + i] = psi(piv_mu, k_i) psi(piv_mu, j_i).
+__global__ void k_cmat_list(const double* __restrict__ psi, long long ng,
+                            const int* __restrict__ piv, int rk, int lo1, int lo2, int n2,
+                            const int* __restrict__ pairs, int p0, int b,
+                            double* __restrict__ Cb) {
+  const long long total = (long long)rk * b;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int mu = (int)(e / b), i = (int)(e % b);
+    const int pair = pairs[p0 + i];
+    const long long r = piv[mu];
+    Cb[e] = psi[r + (long long)(lo1 + pair / n2) * ng] * psi[r + (long long)(lo2 + pair % n2) * ng];
+  }
+}
+
 // theta C tile with ||rho - theta C||^2 and ||rho||^2 of the tile in partials.
 __global__ void __launch_bounds__(256) k_fit_err(const double* __restrict__ theta, long long ng,
                                                  int rk, const double* __restrict__ C, int npair,
@@ -313,6 +342,122 @@ int check_run(const CheckArgs& args, Arena& arena, cudaStream_t s, double* fit_e
     x2 += v.y;
   }
   *coul_err = std::sqrt(e2) / std::sqrt(x2);
+  return ISDF_OK;
+}
+
+// ---------------------------------------------------------------- sampled check
+// The check's two errors restricted to a list of state pairs, for sizes whose
+// all-pair spectra do not fit (an extension: the reference checks all pairs,
+// checkcode.cpp:54-313, which is O(Ng Npair^2)). For the listed pairs:
+//   fit error   = ||rho_s - theta C_s||_F / ||rho_s||_F over all grid points;
+//   (ij|V|kl)   = Y Y^T from the spectra of rho_ij, and the ISDF form from the
+//                 spectra of the fitted densities theta c_ij: by linearity of
+//                 the FFT, Re(FFT(theta c_ij)^H V FFT(theta c_kl)) is the
+//                 reference's c_ij^T Re(zeta^H V zeta) c_kl, at 2 npair_s
+//                 transforms instead of mu + Npair.
+namespace {
+struct SampledBuffers {
+  double *rho, *fit, *sw, *Y, *Yf, *Cb, *E, *Ef;
+  cufftDoubleComplex* spec;
+  int *piv, *pairs;
+  double2* part;
+};
+
+SampledBuffers carve_sampled(Arena& a, long long ng, long long nh, int ns, int rk) {
+  SampledBuffers b;
+  b.rho = a.take<double>((size_t)ng * kBatch);
+  b.fit = a.take<double>((size_t)ng * kBatch);
+  b.spec = a.take<cufftDoubleComplex>((size_t)nh * kBatch);
+  b.sw = a.take<double>((size_t)nh);
+  b.Y = a.take<double>((size_t)ns * 2 * nh);
+  b.Yf = a.take<double>((size_t)ns * 2 * nh);
+  b.Cb = a.take<double>((size_t)rk * kBatch);
+  b.E = a.take<double>((size_t)ns * ns);
+  b.Ef = a.take<double>((size_t)ns * ns);
+  b.piv = a.take<int>((size_t)rk);
+  b.pairs = a.take<int>((size_t)ns);
+  b.part = a.take<double2>((size_t)kDiffBlocks);
+  return b;
+}
+
+int diff_norms(const double* X, const double* Y, long long n, double2* part, cudaStream_t s,
+               double* e2, double* x2) {
+  k_diff_norms<<<kDiffBlocks, 256, 0, s>>>(X, Y, n, part);
+  ISDF_CHECK_LAUNCH();
+  std::vector<double2> h(kDiffBlocks);
+  ISDF_TRY(read_back(h.data(), part, sizeof(double2) * kDiffBlocks, s));
+  for (auto& v : h) {
+    *e2 += v.x;
+    *x2 += v.y;
+  }
+  return ISDF_OK;
+}
+}  // namespace
+
+size_t check_sampled_workspace_bytes(const int* num_grid, int rk, int npair_sample) {
+  const long long ng = (long long)num_grid[0] * num_grid[1] * num_grid[2];
+  const long long nh = (long long)(num_grid[0] / 2 + 1) * num_grid[1] * num_grid[2];
+  Arena a;
+  a.counting = true;
+  carve_sampled(a, ng, nh, npair_sample, rk);
+  return a.off;
+}
+
+int check_sampled_run(const CheckArgs& args, const int* pairs, int ns, Arena& arena,
+                      cudaStream_t s, double* fit_err, double* coul_err) {
+  const int nx = args.num_grid[0], ny = args.num_grid[1], nz = args.num_grid[2];
+  const long long ng = (long long)nx * ny * nz;
+  const long long nh = (long long)(nx / 2 + 1) * ny * nz;
+  const int n2 = args.nv2 + args.nc2, rk = args.rk;
+  const int lo1 = args.nocc - args.nv1, lo2 = args.nocc - args.nv2;
+  if (2 * nh * (long long)ns > (1LL << 31))
+    return record_error(ISDF_ERR_UNSUPPORTED, "sampled check: pair spectra above 2^31 entries");
+  SampledBuffers b = carve_sampled(arena, ng, nh, ns, rk);
+  if (arena.overflowed()) return record_error(ISDF_ERR_NOMEM, "sampled check: workspace too small");
+  ISDF_CUDA(cudaMemcpyAsync(b.piv, args.piv, sizeof(int) * rk, cudaMemcpyHostToDevice, s));
+  ISDF_CUDA(cudaMemcpyAsync(b.pairs, pairs, sizeof(int) * ns, cudaMemcpyHostToDevice, s));
+  const double vol = args.length[0] * args.length[1] * args.length[2];
+  k_weights<<<grid_for(nh, 256), 256, 0, s>>>(nx, ny, nz, args.length[0], args.length[1],
+                                             args.length[2], vol / (double)ng, b.sw);
+  Plan plan;
+  int dims[3] = {nz, ny, nx};
+  if (cufftPlanMany(&plan.h, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, kBatch) !=
+      CUFFT_SUCCESS)
+    return record_error(ISDF_ERR_CUDA, "sampled check: cufftPlanMany failed");
+  plan.ok = true;
+  if (cufftSetStream(plan.h, s) != CUFFT_SUCCESS)
+    return record_error(ISDF_ERR_CUDA, "sampled check: cufftSetStream failed");
+  double fe2 = 0, fr2 = 0;
+  for (int c0 = 0; c0 < ns; c0 += kBatch) {
+    const int bc = std::min(kBatch, ns - c0);
+    k_rho_list<<<grid_for(ng * bc, 256), 256, 0, s>>>(args.d_psi, ng, lo1, lo2, n2, b.pairs, c0,
+                                                      bc, b.rho);
+    k_cmat_list<<<grid_for((long long)rk * bc, 256), 256, 0, s>>>(args.d_psi, ng, b.piv, rk, lo1,
+                                                                  lo2, n2, b.pairs, c0, bc, b.Cb);
+    ISDF_CHECK_LAUNCH();
+    // fitted densities theta C_s of the batch (Ng x bc)
+    ISDF_TRY(dgemm_store((int)ng, bc, rk, args.d_theta, ng, b.Cb, bc, b.fit, ng, s));
+    ISDF_TRY(diff_norms(b.rho, b.fit, ng * bc, b.part, s, &fe2, &fr2));
+    if (bc < kBatch) {
+      ISDF_CUDA(cudaMemsetAsync(b.rho + (long long)bc * ng, 0,
+                                sizeof(double) * (size_t)(kBatch - bc) * ng, s));
+      ISDF_CUDA(cudaMemsetAsync(b.fit + (long long)bc * ng, 0,
+                                sizeof(double) * (size_t)(kBatch - bc) * ng, s));
+    }
+    for (int which = 0; which < 2; ++which) {
+      if (cufftExecD2Z(plan.h, which ? b.fit : b.rho, b.spec) != CUFFT_SUCCESS)
+        return record_error(ISDF_ERR_CUDA, "sampled check: cufftExecD2Z failed");
+      k_spectra_to_rows<<<grid_for(nh * bc, 256), 256, 0, s>>>(b.spec, nh, bc, b.sw, c0, ns,
+                                                               which ? b.Yf : b.Y);
+    }
+    ISDF_CHECK_LAUNCH();
+  }
+  *fit_err = std::sqrt(fe2) / std::sqrt(fr2);
+  ISDF_TRY(dgemm_store(ns, ns, (int)(2 * nh), b.Y, ns, b.Y, ns, b.E, ns, s));
+  ISDF_TRY(dgemm_store(ns, ns, (int)(2 * nh), b.Yf, ns, b.Yf, ns, b.Ef, ns, s));
+  double ce2 = 0, cx2 = 0;
+  ISDF_TRY(diff_norms(b.E, b.Ef, (long long)ns * ns, b.part, s, &ce2, &cx2));
+  *coul_err = std::sqrt(ce2) / std::sqrt(cx2);
   return ISDF_OK;
 }
 

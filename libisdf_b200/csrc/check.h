@@ -22,4 +22,10 @@ size_t check_workspace_bytes(const int* num_grid, int nstate, int rk, int npair)
 int check_run(const CheckArgs& args, Arena& arena, cudaStream_t s, double* fit_err,
               double* coul_err);
 
+// The check restricted to a list of state pairs (pair index (k - lo1) * n2 +
+// (j - lo2)); pairs: host int[npair_sample].
+size_t check_sampled_workspace_bytes(const int* num_grid, int rk, int npair_sample);
+int check_sampled_run(const CheckArgs& args, const int* pairs, int npair_sample, Arena& arena,
+                      cudaStream_t s, double* fit_err, double* coul_err);
+
 }  // namespace isdf_b200

@@ -60,3 +60,37 @@ def check(psi, ng, length, nocc, nv1, nc1, nv2, nc2, rk, piv, theta):
     isdf = c.T @ aux @ c
     coul_err = np.linalg.norm(ijkl - isdf) / np.linalg.norm(ijkl)
     return float(fit_err), float(coul_err)
+
+
+def check_sampled(psi, ng, length, nocc, nv1, nc1, nv2, nc2, rk, piv, theta, pairs,
+                  fitted_spectra=False):
+    """The check's two errors restricted to the state pairs `pairs` (pair
+    index (k - lo1) * n2 + (j - lo2), checkcode.cpp:62-73): the fit error over
+    all grid points of those pairs and the relative Coulomb error of the pair
+    block (ij|V|kl). fitted_spectra=False evaluates the ISDF form as the
+    reference does, c_ij^T Re(zeta^H V zeta) c_kl with zeta the spectra of
+    every theta column (checkcode.cpp:249-288); True takes the spectra of the
+    fitted densities theta c_ij instead (the same number by linearity of the
+    FFT, at 2 len(pairs) transforms: what sizes beyond Si8 need)."""
+    psi = np.asarray(psi)
+    pairs = np.asarray(pairs, dtype=np.int64)
+    n2 = nv2 + nc2
+    k = nocc - nv1 + pairs // n2
+    j = nocc - nv2 + pairs % n2
+    rho = psi[:, k] * psi[:, j]
+    p = np.asarray(piv[:rk], dtype=np.int64)
+    c = psi[p][:, k] * psi[p][:, j]  # rk x npair_s
+    fit = theta[:, :rk] @ c
+    fit_err = np.linalg.norm(rho - fit) / np.linalg.norm(rho)
+    v = coulomb_kernel(ng, length).reshape(-1)
+    r_hat = _spectra(rho, ng, length)
+    ijkl = np.real(np.conj(r_hat) @ (v[:, None] * r_hat.T))
+    if fitted_spectra:
+        f_hat = _spectra(fit, ng, length)
+        isdf = np.real(np.conj(f_hat) @ (v[:, None] * f_hat.T))
+    else:
+        z_hat = _spectra(np.asarray(theta[:, :rk]), ng, length)
+        aux = np.real(np.conj(z_hat) @ (v[:, None] * z_hat.T))
+        isdf = c.T @ aux @ c
+    coul_err = np.linalg.norm(ijkl - isdf) / np.linalg.norm(ijkl)
+    return float(fit_err), float(coul_err)

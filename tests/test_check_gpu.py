@@ -1,10 +1,12 @@
 """GPU check (cuFFT) against the reference's checkcode: the goldens hold the fit
 and Coulomb errors the reference printed for its own theta; the GPU check run
-on that same theta must reproduce them. Also the check inside ISDF()."""
+on that same theta must reproduce them. Also the check inside ISDF(), and the
+sampled-pair check (isdf_check_sampled) that reaches sizes the full check
+refuses."""
 import numpy as np
 import pytest
 
-from conftest import load_golden
+from conftest import load_golden, record_parity
 from oracle import check as ocheck
 
 import libisdf_b200 as isdf
@@ -49,3 +51,62 @@ def test_check_inside_isdf_si8(torch_cuda):
     assert rep.fit_err > 0 and rep.coul_err > 0
     assert abs(rep.fit_err / fe - 1) < 1e-8
     assert abs(rep.coul_err / ce - 1) < 1e-6
+
+
+def _close(x, y, rel):
+    return abs(x - y) <= rel * abs(y) + 1e-15
+
+
+@pytest.mark.parametrize("name", ["small_s1s2", "small_mu0"])
+def test_sampled_check_all_pairs_equals_full_check(torch_cuda, name):
+    """The sampled check given every pair reproduces the full check (and so
+    the reference's printed numbers); on a subset it equals the oracle's
+    restatement with the reference's c^T Re(zeta^H V zeta) c form."""
+    torch = torch_cuda
+    g = load_golden(name)
+    a = (int(g["nocc"]), int(g["nv1"]), int(g["nc1"]), int(g["nv2"]), int(g["nc2"]))
+    rk = int(g["rk_eff"])
+    ng, ln = tuple(int(x) for x in g["ng"]), tuple(g["length"])
+    dom = isdf.Domain(length=ln, num_grid=ng)
+    d_psi = torch.from_numpy(np.ascontiguousarray(g["psi"].T)).cuda()
+    d_th = torch.from_numpy(np.ascontiguousarray(g["theta"].T)).cuda()
+    npair = (a[1] + a[2]) * (a[3] + a[4])
+    full = isdf.check(dom, d_psi, a[0], g["psi"].shape[1], *a[1:], rk, g["piv"], d_th)
+    every = isdf.check_sampled(dom, d_psi, a[0], g["psi"].shape[1], *a[1:], rk, g["piv"], d_th,
+                               np.arange(npair))
+    assert _close(every[0], full[0], 1e-10) and _close(every[1], full[1], 1e-7)
+    sub = np.random.default_rng(0).choice(npair, size=npair // 3, replace=False)
+    got = isdf.check_sampled(dom, d_psi, a[0], g["psi"].shape[1], *a[1:], rk, g["piv"], d_th, sub)
+    want = ocheck.check_sampled(g["psi"], ng, ln, *a, rk, g["piv"], g["theta"], sub)
+    record_parity(f"sampled check {name}", "fit / Coulomb error (GPU; oracle)",
+                  f"{got[0]:.6e} / {got[1]:.6e}; {want[0]:.6e} / {want[1]:.6e}")
+    assert _close(got[0], want[0], 1e-9) and _close(got[1], want[1], 1e-6)
+
+
+def test_sampled_check_at_si64(torch_cuda):
+    """The check at a size the full check refuses: the Si64-like shape (80^3,
+    256 states, 65536 pairs, mu = 2048 from K-means), 192 sampled pairs,
+    against the oracle's restatement of the same pair block (fitted-density
+    spectra; numpy FFT) on the same theta."""
+    torch = torch_cuda
+    s = synth.SI64
+    psi = synth.shape_orbitals(s, 1, device="cuda")
+    dom = isdf.Domain(length=(s.length,) * 3, num_grid=(s.n,) * 3)
+    d_psi = torch.from_numpy(np.ascontiguousarray(psi.T)).cuda()
+    d_theta = torch.empty((s.mu, s.ng), dtype=torch.float64, device="cuda")
+    piv = np.zeros(s.ng, dtype=np.int32)
+    rep = isdf.ISDF(d_psi, dom, s.nocc, s.nstate, s.nv1, s.nc1, s.nv2, s.nc2, s.mu, d_theta, piv,
+                    s.kmeans_iters)
+    with pytest.raises(isdf.IsdfError):
+        isdf.check(dom, d_psi, s.nocc, s.nstate, s.nv1, s.nc1, s.nv2, s.nc2, rep.rk_eff, piv,
+                   d_theta)
+    npair = (s.nv1 + s.nc1) * (s.nv2 + s.nc2)
+    pairs = np.sort(np.random.default_rng(1).choice(npair, size=192, replace=False))
+    got = isdf.check_sampled(dom, d_psi, s.nocc, s.nstate, s.nv1, s.nc1, s.nv2, s.nc2,
+                             rep.rk_eff, piv, d_theta, pairs)
+    th = np.asfortranarray(d_theta[:rep.rk_eff].cpu().numpy().T)
+    want = ocheck.check_sampled(psi, (s.n,) * 3, (s.length,) * 3, s.nocc, s.nv1, s.nc1, s.nv2,
+                                s.nc2, rep.rk_eff, piv, th, pairs, fitted_spectra=True)
+    record_parity("sampled check Si64", "fit / Coulomb error (GPU; oracle)",
+                  f"{got[0]:.6e} / {got[1]:.6e}; {want[0]:.6e} / {want[1]:.6e}")
+    assert _close(got[0], want[0], 1e-9) and _close(got[1], want[1], 1e-6)
