@@ -172,6 +172,17 @@ int isdf_check_sampled(const isdf_domain_t* dom, const double* d_psi, int nocc, 
                        const double* d_theta, int npair_sample, const int* pairs,
                        double* fit_err, double* coul_err, void* stream);
 
+/* The ISDF Coulomb matrix A(mu, nu) = Re sum_G conj(zeta_mu(G)) V(G) zeta_nu(G),
+ * zeta_mu the spectrum of theta column mu scaled by vol/Ng and V the
+ * truncated Coulomb kernel of the check (R = 5): the matrix the reference's
+ * check forms from theta (src/common/checkcode.cpp:249-288) and the operator a
+ * GW / RPA / TDDFT code applies to interpolation-point quantities. d_theta:
+ * device Ng x rk, ld = Ng (read only); d_A: device rk x rk, column-major.
+ * Device memory: rk x 2 (nx/2+1) ny nz doubles of half spectra (Si216: 44 GB)
+ * plus two 128-column transform buffers. */
+int isdf_coulomb_matrix(const isdf_domain_t* dom, const double* d_theta, int rk, double* d_A,
+                        void* stream);
+
 /* Size of the fixed device scratch array behind isdf_fit_noalloc(). */
 #define ISDF_NOALLOC_SCRATCH_BYTES (8u << 20)
 

@@ -199,6 +199,8 @@ def lib() -> ctypes.CDLL:
         L.isdf_check_sampled.argtypes = [ctypes.POINTER(_Domain), P, I, I, I, I, I, I, I, P, P, I,
                                          P, P, P, P]
         L.isdf_check_sampled.restype = I
+        L.isdf_coulomb_matrix.argtypes = [ctypes.POINTER(_Domain), P, I, P, P]
+        L.isdf_coulomb_matrix.restype = I
         L.isdf_last_error.restype = ctypes.c_char_p
         L.isdf_status_string.argtypes = [I]
         L.isdf_status_string.restype = ctypes.c_char_p
@@ -318,6 +320,14 @@ def check_sampled(domain: Domain, d_psi, nocc: int, nstate: int, nv1: int, nc1: 
                                     pairs.ctypes.data, ctypes.addressof(fe),
                                     ctypes.addressof(ce), stream or None))
     return fe.value, ce.value
+
+
+def coulomb_matrix(domain: Domain, d_theta, rk: int, d_A, stream: int = 0):
+    """The ISDF Coulomb matrix Re(zeta^H V zeta) (rk x rk) into d_A (device,
+    column-major), zeta the spectra of the theta columns (checkcode.cpp:249-288)."""
+    d = domain._c()
+    _check(lib().isdf_coulomb_matrix(ctypes.byref(d), _dptr(d_theta), rk, _dptr(d_A),
+                                     stream or None))
 
 
 def _report(r: _Report) -> Report:

@@ -530,6 +530,26 @@ int isdf_check_sampled(const isdf_domain_t* dom, const double* d_psi, int nocc, 
   }
 }
 
+int isdf_coulomb_matrix(const isdf_domain_t* dom, const double* d_theta, int rk, double* d_A,
+                        void* stream) {
+  try {
+    if (!dom || !d_theta || !d_A) return record_error(ISDF_ERR_ARG, "null pointer");
+    const long long ng = (long long)dom->num_grid[0] * dom->num_grid[1] * dom->num_grid[2];
+    if (dom->num_grid[0] <= 0 || dom->num_grid[1] <= 0 || dom->num_grid[2] <= 0 || rk <= 0 ||
+        rk > ng)
+      return record_error(ISDF_ERR_ARG, "sizes");
+    const size_t need = coulomb_matrix_workspace_bytes(dom->num_grid, rk);
+    std::lock_guard<std::mutex> lock(workspace_mutex());
+    Arena arena;
+    cudaStream_t ls;
+    ISDF_TRY(acquire_workspace(need + 4096, &arena, &ls));
+    return coulomb_matrix_run(dom->num_grid, dom->length, d_theta, rk, d_A, arena,
+                              stream ? (cudaStream_t)stream : ls);
+  } catch (const std::exception& e) {
+    return record_error(ISDF_ERR_NOMEM, e.what());
+  }
+}
+
 const char* isdf_last_error(void) { return last_error_message(); }
 
 const char* isdf_status_string(int code) {

@@ -461,4 +461,62 @@ int check_sampled_run(const CheckArgs& args, const int* pairs, int ns, Arena& ar
   return ISDF_OK;
 }
 
+// ---------------------------------------------------------------- ISDF Coulomb matrix
+// A(mu, nu) = Re sum_G conj(zeta_mu(G)) V(G) zeta_nu(G), zeta = the spectra of
+// the theta columns scaled by vol/Ng (checkcode.cpp:249-288, which forms it
+// from FFTW full spectra with a complex GEMM): the operator a GW / RPA / TDDFT
+// code applies to interpolation-point quantities, the first consumer of theta.
+// Here: batched cuFFT D2Z half spectra weighted by sqrt(w V) into one real
+// matrix Yz (rk x 2 nh), then A = Yz Yz^T on the FP64 tensor cores.
+size_t coulomb_matrix_workspace_bytes(const int* num_grid, int rk) {
+  const long long ng = (long long)num_grid[0] * num_grid[1] * num_grid[2];
+  const long long nh = (long long)(num_grid[0] / 2 + 1) * num_grid[1] * num_grid[2];
+  Arena a;
+  a.counting = true;
+  a.take<double>((size_t)ng * kBatch);
+  a.take<cufftDoubleComplex>((size_t)nh * kBatch);
+  a.take<double>((size_t)nh);
+  a.take<double>((size_t)rk * 2 * nh);
+  return a.off;
+}
+
+int coulomb_matrix_run(const int* num_grid, const double* length, const double* d_theta, int rk,
+                       double* d_A, Arena& arena, cudaStream_t s) {
+  const int nx = num_grid[0], ny = num_grid[1], nz = num_grid[2];
+  const long long ng = (long long)nx * ny * nz;
+  const long long nh = (long long)(nx / 2 + 1) * ny * nz;
+  double* buf = arena.take<double>((size_t)ng * kBatch);
+  cufftDoubleComplex* spec = arena.take<cufftDoubleComplex>((size_t)nh * kBatch);
+  double* sw = arena.take<double>((size_t)nh);
+  double* Yz = arena.take<double>((size_t)rk * 2 * nh);
+  if (arena.overflowed()) return record_error(ISDF_ERR_NOMEM, "Coulomb matrix: workspace too small");
+  const double vol = length[0] * length[1] * length[2];
+  k_weights<<<grid_for(nh, 256), 256, 0, s>>>(nx, ny, nz, length[0], length[1], length[2],
+                                             vol / (double)ng, sw);
+  Plan plan;
+  int dims[3] = {nz, ny, nx};
+  if (cufftPlanMany(&plan.h, 3, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, kBatch) !=
+      CUFFT_SUCCESS)
+    return record_error(ISDF_ERR_CUDA, "Coulomb matrix: cufftPlanMany failed");
+  plan.ok = true;
+  if (cufftSetStream(plan.h, s) != CUFFT_SUCCESS)
+    return record_error(ISDF_ERR_CUDA, "Coulomb matrix: cufftSetStream failed");
+  for (int c0 = 0; c0 < rk; c0 += kBatch) {
+    const int bc = std::min(kBatch, rk - c0);
+    // theta is the caller's: transform a copy
+    ISDF_CUDA(cudaMemcpyAsync(buf, d_theta + (long long)c0 * ng, sizeof(double) * (size_t)bc * ng,
+                              cudaMemcpyDeviceToDevice, s));
+    if (bc < kBatch)
+      ISDF_CUDA(cudaMemsetAsync(buf + (long long)bc * ng, 0,
+                                sizeof(double) * (size_t)(kBatch - bc) * ng, s));
+    if (cufftExecD2Z(plan.h, buf, spec) != CUFFT_SUCCESS)
+      return record_error(ISDF_ERR_CUDA, "Coulomb matrix: cufftExecD2Z failed");
+    k_spectra_to_rows<<<grid_for(nh * bc, 256), 256, 0, s>>>(spec, nh, bc, sw, c0, rk, Yz);
+  }
+  ISDF_CHECK_LAUNCH();
+  const long long K = 2 * nh;  // the GEMM's depth is an int
+  if (K > (1LL << 30)) return record_error(ISDF_ERR_UNSUPPORTED, "Coulomb matrix: grid too large");
+  return dgemm_store(rk, rk, (int)K, Yz, rk, Yz, rk, d_A, rk, s);
+}
+
 }  // namespace isdf_b200

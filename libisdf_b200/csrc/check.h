@@ -22,6 +22,11 @@ size_t check_workspace_bytes(const int* num_grid, int nstate, int rk, int npair)
 int check_run(const CheckArgs& args, Arena& arena, cudaStream_t s, double* fit_err,
               double* coul_err);
 
+// A = Re(zeta^H V zeta) (rk x rk, column-major, device), zeta = FFT(theta columns).
+size_t coulomb_matrix_workspace_bytes(const int* num_grid, int rk);
+int coulomb_matrix_run(const int* num_grid, const double* length, const double* d_theta, int rk,
+                       double* d_A, Arena& arena, cudaStream_t s);
+
 // The check restricted to a list of state pairs (pair index (k - lo1) * n2 +
 // (j - lo2)); pairs: host int[npair_sample].
 size_t check_sampled_workspace_bytes(const int* num_grid, int rk, int npair_sample);

@@ -94,3 +94,11 @@ def check_sampled(psi, ng, length, nocc, nv1, nc1, nv2, nc2, rk, piv, theta, pai
         isdf = c.T @ aux @ c
     coul_err = np.linalg.norm(ijkl - isdf) / np.linalg.norm(ijkl)
     return float(fit_err), float(coul_err)
+
+
+def coulomb_matrix(theta, ng, length, rk):
+    """Re(zeta^H V zeta), zeta the full spectra of the theta columns scaled by
+    vol/Ng (checkcode.cpp:249-288)."""
+    v = coulomb_kernel(ng, length).reshape(-1)
+    z_hat = _spectra(np.asarray(theta[:, :rk]), ng, length)
+    return np.real(np.conj(z_hat) @ (v[:, None] * z_hat.T))
