@@ -134,6 +134,18 @@ int isdf_kmeans_select(const isdf_domain_t* dom, const double* d_w, int mu, int 
                        long long rand_seed, int* piv, int* rk_eff, int* iters, int* npt,
                        void* stream);
 
+/* No counterpart in the reference (one system per call): the K-means
+ * selections of `count` small systems (Ng <= 2^20, mu <= 512, cold start) in
+ * one cooperative launch, a group of CTAs per system; each result equals
+ * isdf_kmeans_select()'s on the same input, bit for bit. Arrays of `count`:
+ * doms, d_w (device weights), mu, max_iter, piv (host int[Ng] each, fully
+ * written), rk_eff / iters / npt (outputs). rand_seed as in
+ * isdf_kmeans_select (applied before each system). The serving loop batches
+ * its small requests through this. */
+int isdf_kmeans_select_batch(int count, const isdf_domain_t* doms, const double* const* d_w,
+                             const int* mu, const int* max_iter, long long rand_seed,
+                             int* const* piv, int* rk_eff, int* iters, int* npt, void* stream);
+
 /* FP64 fit for given pivots (reference src/cuda/isdf-gpu.cpp:112-402 /
  * src/cpu/getbasis_MPI.cpp:9-250): theta = (Z C^T)(C C^T + eps I)^{-1} with
  * eps = 1e-10 tr(C C^T)/rk, Z C^T = (psi_S1 psi_S1(mu)^T) o (psi_S2 psi_S2(mu)^T).

@@ -192,6 +192,8 @@ def lib() -> ctypes.CDLL:
         L.isdf_kmeans_weight.restype = I
         L.isdf_kmeans_select.argtypes = [ctypes.POINTER(_Domain), P, I, I, LL, P, P, P, P, P]
         L.isdf_kmeans_select.restype = I
+        L.isdf_kmeans_select_batch.argtypes = [I, P, P, P, P, LL, P, P, P, P, P]
+        L.isdf_kmeans_select_batch.restype = I
         L.isdf_fit.argtypes = [P, LL, I, I, I, I, I, I, I, P, P, I, I, P, P]
         L.isdf_fit.restype = I
         L.isdf_check.argtypes = [ctypes.POINTER(_Domain), P, I, I, I, I, I, I, I, P, P, P, P, P]
@@ -277,6 +279,22 @@ def kmeans_select(domain: Domain, d_w, mu: int, max_iter: int, rand_seed: int = 
                                     ctypes.addressof(out) + 4, ctypes.addressof(out) + 8,
                                     stream or None))
     return piv, out[0], out[1], out[2]
+
+
+def kmeans_select_batch(domains, d_ws, mus, max_iters, rand_seed: int = -1, stream: int = 0):
+    """The K-means selections of several small systems in one launch; returns
+    a list of (piv int32[Ng], rk_eff, iterations, npt), one per system."""
+    n = len(domains)
+    doms = (_Domain * n)(*[d._c() for d in domains])
+    w = (ctypes.c_void_p * n)(*[_dptr(x) for x in d_ws])
+    mu = (ctypes.c_int * n)(*mus)
+    it = (ctypes.c_int * n)(*max_iters)
+    pivs = [np.zeros(d.NumGridTotal(), dtype=np.int32) for d in domains]
+    pp = (ctypes.c_void_p * n)(*[p.ctypes.data for p in pivs])
+    rk, its, npt = (ctypes.c_int * n)(), (ctypes.c_int * n)(), (ctypes.c_int * n)()
+    _check(lib().isdf_kmeans_select_batch(n, doms, w, mu, it, rand_seed, pp, rk, its, npt,
+                                          stream or None))
+    return [(pivs[r], rk[r], its[r], npt[r]) for r in range(n)]
 
 
 def fit(d_psi, ng: int, nstate: int, nocc: int, nv1: int, nc1: int, nv2: int, nc2: int, rk: int,

@@ -399,6 +399,51 @@ int isdf_kmeans_select(const isdf_domain_t* dom, const double* d_w, int mu, int 
   }
 }
 
+int isdf_kmeans_select_batch(int count, const isdf_domain_t* doms, const double* const* d_w,
+                             const int* mu, const int* max_iter, long long rand_seed,
+                             int* const* piv, int* rk_eff, int* iters, int* npt, void* stream) {
+  try {
+    if (count <= 0 || !doms || !d_w || !mu || !max_iter || !piv)
+      return record_error(ISDF_ERR_ARG, "kmeans batch: null argument");
+    std::vector<KmeansArgs> args(count);
+    size_t need = 4096;
+    for (int r = 0; r < count; ++r) {
+      const isdf_domain_t& d = doms[r];
+      const long long ng = (long long)d.num_grid[0] * d.num_grid[1] * d.num_grid[2];
+      if (!d_w[r] || !piv[r] || d.num_grid[0] <= 0 || d.num_grid[1] <= 0 || d.num_grid[2] <= 0 ||
+          mu[r] <= 0 || mu[r] > ng || max_iter[r] < 0)
+        return record_error(ISDF_ERR_ARG, "kmeans batch: bad request");
+      KmeansArgs& a = args[r];
+      a.d_w = d_w[r];
+      a.ng = ng;
+      for (int i = 0; i < 3; ++i) {
+        a.num_grid[i] = d.num_grid[i];
+        a.length[i] = d.length[i];
+      }
+      a.mu = mu[r];
+      a.max_iter = max_iter[r];
+      a.rand_seed = rand_seed;
+      a.piv = piv[r];
+      need += kmeans_batch_workspace_bytes(ng, mu[r]);
+    }
+    std::lock_guard<std::mutex> lock(workspace_mutex());
+    Arena arena;
+    cudaStream_t ls;
+    ISDF_TRY(acquire_workspace(need, &arena, &ls));
+    std::vector<KmeansResult> res(count);
+    ISDF_TRY(kmeans_select_batch(args.data(), count, arena, stream ? (cudaStream_t)stream : ls,
+                                 res.data()));
+    for (int r = 0; r < count; ++r) {
+      if (rk_eff) rk_eff[r] = res[r].rk_eff;
+      if (iters) iters[r] = res[r].iters;
+      if (npt) npt[r] = res[r].npt;
+    }
+    return ISDF_OK;
+  } catch (const std::exception& e) {
+    return record_error(ISDF_ERR_NOMEM, e.what());
+  }
+}
+
 int isdf_fit(const double* d_psi, long long ng, int nstate, int nocc, int nv1, int nc1, int nv2,
              int nc2, int rk, const int* piv, double* d_theta, int precision, int refine_steps,
              int* chol_info, void* stream) {

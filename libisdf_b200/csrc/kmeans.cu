@@ -1316,4 +1316,482 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
   return ISDF_OK;
 }
 
+// ===================================================================== batched small selections
+// Several small K-means selections in one cooperative launch (the serving
+// loop's batches of small requests): a group of G CTAs runs one request's
+// whole Lloyd loop - assignment, stable counting sort by label, sequential
+// per-cluster folds, centroid update with the empty-cluster compaction, the
+// change count and the final nearest point per centroid - with software group
+// barriers between the phases, so a batch of B requests costs one launch
+// instead of ~10 launches per iteration per request. The arithmetic and every
+// order of summation are the single-request path's (and the reference's,
+// utility.cpp:813-945): piv is the same bit for bit. The assignment is a
+// brute-force scan over the centroids held in shared memory, which suits the
+// small systems this path serves (mu <= 512).
+namespace {
+
+constexpr int kBatchThreads = 256;
+constexpr int kBatchWarps = kBatchThreads / 32;
+
+struct KmBatchJob {
+  const double *px, *py, *pz, *pw;
+  const int* pidx;
+  int* label;
+  double4* sorted;
+  double4* cen;
+  double4* sums;
+  int* hist;   // per sub-block label counts, then each sub-block's first slot per label
+  int* tot;    // members per cluster
+  int* sel;    // grid index of the nearest point per centroid
+  int n, npt, mu, max_iter;
+  double max_f;
+  int rk, iters, err, any_empty;
+  int changed[2];
+  unsigned bar_count, bar_gen;
+};
+
+// All CTAs of one request's group meet here. Bounded: a CTA that waits
+// longer than ~1 s sets err and returns false, and so does every CTA that
+// sees err afterwards, so a failing group ends instead of hanging.
+__device__ bool group_barrier(KmBatchJob* J, int G) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    const unsigned gen = *(volatile unsigned*)&J->bar_gen;
+    if (atomicAdd(&J->bar_count, 1u) == (unsigned)G - 1) {
+      J->bar_count = 0;
+      __threadfence();
+      atomicAdd(&J->bar_gen, 1u);
+    } else {
+      long long spins = 0;
+      while (*(volatile unsigned*)&J->bar_gen == gen) {
+        if (++spins > (1LL << 24)) {
+          atomicExch(&J->err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    ok_s = ok && *(volatile int*)&J->err == 0;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+// Loads of data that other CTAs of the launch wrote: through L2 (L1 is not
+// coherent across SMs within a kernel).
+__device__ __forceinline__ double4 ldcg4(const double4* p) {
+  const double* d = reinterpret_cast<const double*>(p);
+  return make_double4(__ldcg(d), __ldcg(d + 1), __ldcg(d + 2), __ldcg(d + 3));
+}
+
+// Exclusive scan of v[0..m) (m <= kKmeansBatchMaxMu) into out, one block.
+__device__ void block_scan(const int* v, int m, int* out) {
+  __shared__ int part[kBatchThreads];
+  const int per = (m + kBatchThreads - 1) / kBatchThreads;
+  const int lo = min(m, (int)threadIdx.x * per), hi = min(m, lo + per);
+  int t = 0;
+  for (int i = lo; i < hi; ++i) t += __ldcg(v + i);
+  part[threadIdx.x] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int i = 0; i < kBatchThreads; ++i) {
+      const int x = part[i];
+      part[i] = run;
+      run += x;
+    }
+  }
+  __syncthreads();
+  int run = part[threadIdx.x];
+  for (int i = lo; i < hi; ++i) {
+    out[i] = run;
+    run += __ldcg(v + i);
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kBatchThreads) k_kmeans_batch(KmBatchJob* jobs, int G) {
+  KmBatchJob* J = jobs + blockIdx.x / G;
+  const int c = blockIdx.x % G;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ double cx[kKmeansBatchMaxMu], cy[kKmeansBatchMaxMu], cz[kKmeansBatchMaxMu];
+  __shared__ int run[kBatchWarps][kKmeansBatchMaxMu];
+  __shared__ int sstart[kKmeansBatchMaxMu];
+  __shared__ int red[kBatchWarps];
+  const int n = J->n, npt = J->npt;
+  const int nsub = G * kBatchWarps;
+  const int per = (n + nsub - 1) / nsub;
+  const int sb = c * kBatchWarps + warp;
+  const int sb_lo = min(n, sb * per), sb_hi = min(n, sb_lo + per);
+  const int cta_lo = min(n, c * kBatchWarps * per), cta_hi = min(n, cta_lo + kBatchWarps * per);
+  volatile KmBatchJob* VJ = J;
+
+  auto load_cen = [&](int rk) {
+    for (int i = threadIdx.x; i < rk; i += kBatchThreads) {
+      const double4 q = ldcg4(J->cen + i);
+      cx[i] = q.x;
+      cy[i] = q.y;
+      cz[i] = q.z;
+    }
+    __syncthreads();
+  };
+  // labels of this CTA's points (first minimum, pdist2's rounding); returns
+  // the number of labels that changed (valid in thread 0)
+  auto assign = [&](int rk) -> int {
+    int ch = 0;
+    for (int p = cta_lo + threadIdx.x; p < cta_hi; p += kBatchThreads) {
+      const double x = J->px[p], y = J->py[p], z = J->pz[p];
+      double best = ref_dist2(x, y, z, make_double4(cx[0], cy[0], cz[0], 0.0));
+      int bj = 0;
+      for (int j = 1; j < rk; ++j) {
+        const double d = ref_dist2(x, y, z, make_double4(cx[j], cy[j], cz[j], 0.0));
+        if (d < best) {
+          best = d;
+          bj = j;
+        }
+      }
+      if (__ldcg(J->label + p) != bj) ++ch;
+      J->label[p] = bj;
+    }
+    for (int o = 16; o > 0; o >>= 1) ch += __shfl_xor_sync(0xffffffffu, ch, o);
+    if (lane == 0) red[warp] = ch;
+    __syncthreads();
+    int t = 0;
+    if (threadIdx.x == 0)
+      for (int w = 0; w < kBatchWarps; ++w) t += red[w];
+    __syncthreads();
+    return t;
+  };
+
+  int rk = J->mu;
+  load_cen(rk);
+  assign(rk);
+  if (!group_barrier(J, G)) return;
+  int flag = n, s = 0;
+  while ((double)flag > J->max_f && s < J->max_iter) {
+    const int par = s & 1;
+    // 1. label counts per sub-block (one warp each)
+    for (int k = lane; k < rk; k += 32) run[warp][k] = 0;
+    __syncwarp();
+    for (int p = sb_lo + lane; p < sb_hi; p += 32) atomicAdd(&run[warp][__ldcg(J->label + p)], 1);
+    __syncwarp();
+    for (int k = lane; k < rk; k += 32) J->hist[(size_t)sb * kKmeansBatchMaxMu + k] = run[warp][k];
+    if (!group_barrier(J, G)) return;
+    // 2. per cluster, each sub-block's offset within the cluster and the
+    // cluster's size (every CTA has read last iteration's change count)
+    if (c == 0 && threadIdx.x == 0) {
+      VJ->changed[par ^ 1] = 0;
+      VJ->any_empty = 0;
+    }
+    for (int k = c + G * threadIdx.x; k < rk; k += G * kBatchThreads) {
+      int acc = 0;
+      for (int q = 0; q < nsub; ++q) {
+        int* h = J->hist + (size_t)q * kKmeansBatchMaxMu + k;
+        const int v = __ldcg(h);
+        *h = acc;
+        acc += v;
+      }
+      J->tot[k] = acc;
+    }
+    if (!group_barrier(J, G)) return;
+    // 3. stable scatter of (w x, w y, w z, w) into cluster order
+    block_scan(J->tot, rk, sstart);
+    for (int k = lane; k < rk; k += 32)
+      run[warp][k] = sstart[k] + __ldcg(J->hist + (size_t)sb * kKmeansBatchMaxMu + k);
+    __syncwarp();
+    for (int base = sb_lo; base < sb_hi; base += 32) {
+      const int p = base + lane;
+      const bool ok = p < sb_hi;
+      const int l = ok ? __ldcg(J->label + p) : -1;
+      const unsigned peers = __match_any_sync(0xffffffffu, l);
+      const int b = ok ? run[warp][l] : 0;
+      __syncwarp();
+      if (ok) {
+        const double w = J->pw[p];
+        const int r = __popc(peers & ((1u << lane) - 1u));
+        J->sorted[b + r] = make_double4(rmul(w, J->px[p]), rmul(w, J->py[p]), rmul(w, J->pz[p]), w);
+        if (lane == __ffs(peers) - 1) run[warp][l] = b + __popc(peers);
+      }
+      __syncwarp();
+    }
+    if (!group_barrier(J, G)) return;
+    // 4. per cluster and component, the sequential fold in point order; the
+    // zero tail (copies of grid point 0, last in their cluster) by repeat_add
+    const int tail_label = npt < n ? __ldcg(J->label + npt) : -1;
+    for (int kq = c * kBatchThreads + threadIdx.x; kq < 4 * rk; kq += G * kBatchThreads) {
+      const int k = kq >> 2, q = kq & 3;
+      int m = __ldcg(J->tot + k);
+      long long tail = 0;
+      if (k == tail_label) {
+        tail = n - npt;
+        m -= (int)tail;
+      }
+      const double* v = reinterpret_cast<const double*>(J->sorted + sstart[k]) + q;
+      double acc = 0.0;
+      for (int e = 0; e < m; ++e) acc = radd(acc, __ldcg(v + (size_t)e * 4));
+      if (tail) {
+        const double w0 = J->pw[npt];
+        const double val = q == 3 ? w0 : rmul(w0, q == 0 ? J->px[npt] : q == 1 ? J->py[npt] : J->pz[npt]);
+        acc = repeat_add(acc, val, tail);
+      }
+      reinterpret_cast<double*>(J->sums + k)[q] = acc;
+      if (q == 3 && acc == 0.0) VJ->any_empty = 1;
+    }
+    if (!group_barrier(J, G)) return;
+    // 5. new centroids = sums / count; an empty cluster takes the last one's
+    // sums and rk shrinks (utility.cpp:831-853), in order, by one thread
+    if (c == 0) {
+      if (!VJ->any_empty) {
+        for (int i = threadIdx.x; i < rk; i += kBatchThreads) {
+          const double4 q = ldcg4(J->sums + i);
+          J->cen[i] = make_double4(rdiv(q.x, q.w), rdiv(q.y, q.w), rdiv(q.z, q.w), 0.0);
+        }
+      } else if (threadIdx.x == 0) {
+        int r = rk;
+        for (int i = 0; i < r; i++) {
+          const double4 q = ldcg4(J->sums + i);
+          if (q.w != 0.0) {
+            J->sums[i] = make_double4(rdiv(q.x, q.w), rdiv(q.y, q.w), rdiv(q.z, q.w), q.w);
+          } else {
+            r--;
+            J->sums[i] = ldcg4(J->sums + r);
+            i--;
+          }
+        }
+        for (int i = 0; i < r; i++) {
+          const double4 q = ldcg4(J->sums + i);
+          J->cen[i] = make_double4(q.x, q.y, q.z, 0.0);
+        }
+        VJ->rk = r;
+      }
+    }
+    if (!group_barrier(J, G)) return;
+    // 6. reassignment and the change count
+    rk = VJ->rk;
+    load_cen(rk);
+    const int ch = assign(rk);
+    if (threadIdx.x == 0 && ch) atomicAdd(&J->changed[par], ch);
+    if (!group_barrier(J, G)) return;
+    flag = VJ->changed[par];
+    ++s;
+  }
+  // nearest point to every centroid (first minimum over points), one warp each
+  load_cen(rk);
+  for (int j = c * kBatchWarps + warp; j < rk; j += nsub) {
+    const double4 q = make_double4(cx[j], cy[j], cz[j], 0.0);
+    double best = __longlong_as_double(0x7ff0000000000000LL);
+    int bi = 0x7fffffff;
+    for (int p = lane; p < n; p += 32) {
+      const double d = ref_dist2(J->px[p], J->py[p], J->pz[p], q);
+      if (d < best) {
+        best = d;
+        bi = p;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob < best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (lane == 0) J->sel[j] = J->pidx[bi];
+  }
+  if (c == 0 && threadIdx.x == 0) VJ->iters = s;
+}
+
+struct BatchBuffers {
+  int* pidx;
+  double *px, *py, *pz, *pw;
+  int* label;
+  double4 *sorted, *cen, *sums;
+  int *hist, *tot, *sel, *tile_cnt;
+  KmState* st;
+};
+
+BatchBuffers carve_batch(Arena& a, int n, int G) {
+  BatchBuffers b;
+  const int nfilter = (n + 1023) / 1024;
+  b.pidx = a.take<int>(n);
+  b.px = a.take<double>(n);
+  b.py = a.take<double>(n);
+  b.pz = a.take<double>(n);
+  b.pw = a.take<double>(n);
+  b.label = a.take<int>(n);
+  b.sorted = a.take<double4>(n);
+  b.cen = a.take<double4>(kKmeansBatchMaxMu);
+  b.sums = a.take<double4>(kKmeansBatchMaxMu);
+  b.hist = a.take<int>((size_t)G * kBatchWarps * kKmeansBatchMaxMu);
+  b.tot = a.take<int>(kKmeansBatchMaxMu);
+  b.sel = a.take<int>(kKmeansBatchMaxMu);
+  b.tile_cnt = a.take<int>(nfilter);
+  b.st = a.take<KmState>(1);
+  return b;
+}
+
+int batch_group(long long n) {
+  long long g = (n + 4095) / 4096;
+  return (int)std::max(1LL, std::min(16LL, g));
+}
+
+}  // namespace
+
+// piv = [distinct selected points ascending | the rest ascending]
+// (unique, utility.cpp:617-629, and utility.cpp:973-983); returns rk_eff.
+static int piv_from_selection(std::vector<int>& sel, int n, int* piv) {
+  std::sort(sel.begin(), sel.end());
+  sel.erase(std::unique(sel.begin(), sel.end()), sel.end());
+  const int rk_eff = (int)sel.size();
+  int k0 = 0, k1 = 0;
+  for (int i = 0; i < n; i++) {
+    if (i == sel[k0]) {
+      piv[k0] = i;
+      k0 = std::min(k0 + 1, rk_eff - 1);
+    } else {
+      piv[rk_eff + k1] = i;
+      k1++;
+    }
+  }
+  return rk_eff;
+}
+
+size_t kmeans_batch_workspace_bytes(long long ng, int mu) {
+  (void)mu;
+  Arena a;
+  a.counting = true;
+  carve_batch(a, (int)ng, batch_group(ng));
+  a.take<KmBatchJob>(1);
+  return a.off + 512;
+}
+
+int kmeans_select_batch(const KmeansArgs* args, int count, Arena& arena, cudaStream_t stream,
+                        KmeansResult* res) {
+  if (count <= 0) return ISDF_OK;
+  int G = 1;
+  for (int r = 0; r < count; ++r) {
+    const KmeansArgs& a = args[r];
+    if (a.ng <= 1 || a.ng > kKmeansBatchMaxNg || a.mu <= 0 || a.mu > kKmeansBatchMaxMu ||
+        a.mu > a.ng || a.max_iter < 0 || a.warm)
+      return record_error(ISDF_ERR_UNSUPPORTED, "kmeans batch: request outside the batched sizes");
+    G = std::max(G, batch_group(a.ng));
+  }
+  std::vector<BatchBuffers> bufs(count);
+  for (int r = 0; r < count; ++r) bufs[r] = carve_batch(arena, (int)args[r].ng, G);
+  KmBatchJob* d_jobs = arena.take<KmBatchJob>((size_t)count);
+  if (arena.overflowed()) return record_error(ISDF_ERR_NOMEM, "kmeans batch: workspace too small");
+  // filter: maxW, kept-point compaction, zero tail (per request)
+  for (int r = 0; r < count; ++r) {
+    const int n = (int)args[r].ng;
+    const int nfilter = (n + 1023) / 1024;
+    const BatchBuffers& b = bufs[r];
+    ISDF_CUDA(cudaMemsetAsync(b.st, 0, sizeof(KmState), stream));
+    ISDF_CUDA(cudaMemsetAsync(b.pidx, 0, sizeof(int) * (size_t)n, stream));
+    k_maxw<<<kNumSMs * 4, 256, 0, stream>>>(args[r].d_w, n, b.st);
+    k_filter_count<<<nfilter, 256, 0, stream>>>(args[r].d_w, n, b.st, b.tile_cnt);
+    k_scan_small<<<1, 1024, 0, stream>>>(b.tile_cnt, nfilter, &b.st->npt);
+    k_filter_scatter<<<nfilter, 256, 0, stream>>>(args[r].d_w, n, b.st, b.tile_cnt, b.pidx);
+  }
+  ISDF_CHECK_LAUNCH();
+  std::vector<KmBatchJob> jobs;
+  std::vector<int> slot;  // request of each batched job
+  for (int r = 0; r < count; ++r) {
+    const KmeansArgs& a = args[r];
+    const int n = (int)a.ng, mu = a.mu;
+    const BatchBuffers& b = bufs[r];
+    KmState hst;
+    ISDF_TRY(read_back(&hst, b.st, sizeof(KmState), stream));
+    res[r] = KmeansResult();
+    res[r].npt = hst.npt;
+    if (a.rand_seed >= 0) std::srand((unsigned)a.rand_seed);
+    std::memset(a.piv, 0, sizeof(int) * (size_t)n);
+    if (hst.npt < mu) {
+      // utility.cpp:667-681: piv from the kept list, then a shuffled tail
+      std::vector<int> index(n, 0);
+      ISDF_TRY(read_back(index.data(), b.pidx, sizeof(int) * (size_t)hst.npt, stream));
+      int k0 = 0, k1 = 0;
+      for (int i = 0; i < hst.npt; i++) {
+        if (i == index[k0]) {
+          a.piv[k0] = i;
+          k0 = std::min(k0 + 1, mu - 1);
+        } else {
+          a.piv[hst.npt + k1] = i;
+          k1++;
+        }
+      }
+      shuffle_like_libstdcxx(a.piv + hst.npt, a.piv + n);
+      res[r].rk_eff = mu;
+      res[r].iters = -1;
+      continue;
+    }
+    const double dx0 = a.length[0] / a.num_grid[0];
+    const double dx1 = a.length[1] / a.num_grid[1];
+    const double dx2 = a.length[2] / a.num_grid[2];
+    k_points<<<grid_for(n, 256), 256, 0, stream>>>(b.pidx, a.d_w, n, a.num_grid[0], a.num_grid[1],
+                                                   dx0, dx1, dx2, b.px, b.py, b.pz, b.pw, mu,
+                                                   b.cen);
+    ISDF_CUDA(cudaMemsetAsync(b.label, 0xff, sizeof(int) * (size_t)n, stream));
+    KmBatchJob j;
+    std::memset(&j, 0, sizeof(j));
+    j.px = b.px;
+    j.py = b.py;
+    j.pz = b.pz;
+    j.pw = b.pw;
+    j.pidx = b.pidx;
+    j.label = b.label;
+    j.sorted = b.sorted;
+    j.cen = b.cen;
+    j.sums = b.sums;
+    j.hist = b.hist;
+    j.tot = b.tot;
+    j.sel = b.sel;
+    j.n = n;
+    j.npt = hst.npt;
+    j.mu = mu;
+    j.max_iter = a.max_iter;
+    j.max_f = 1e-5 * n;  // KmeansTolerance * n (utility.cpp:812)
+    j.rk = mu;
+    jobs.push_back(j);
+    slot.push_back(r);
+  }
+  ISDF_CHECK_LAUNCH();
+  if (jobs.empty()) return ISDF_OK;
+  // every CTA of the launch must be resident at once (the group barriers)
+  int dev = 0, per_sm = 0, coop = 0;
+  ISDF_CUDA(cudaGetDevice(&dev));
+  ISDF_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  if (!coop) return record_error(ISDF_ERR_UNSUPPORTED, "kmeans batch: no cooperative launch");
+  int nsm = 0;
+  ISDF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  ISDF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_kmeans_batch, kBatchThreads, 0));
+  const int max_jobs = std::max(1, per_sm * nsm / G);
+  ISDF_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(KmBatchJob) * jobs.size(),
+                            cudaMemcpyHostToDevice, stream));
+  for (size_t j0 = 0; j0 < jobs.size(); j0 += (size_t)max_jobs) {
+    const int nj = (int)std::min<size_t>((size_t)max_jobs, jobs.size() - j0);
+    KmBatchJob* dj = d_jobs + j0;
+    int g = G;
+    void* kargs[] = {(void*)&dj, (void*)&g};
+    ISDF_CUDA(cudaLaunchCooperativeKernel((const void*)k_kmeans_batch, dim3((unsigned)(nj * G)),
+                                          dim3(kBatchThreads), kargs, 0, stream));
+  }
+  std::vector<KmBatchJob> out(jobs.size());
+  ISDF_TRY(read_back(out.data(), d_jobs, sizeof(KmBatchJob) * jobs.size(), stream));
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    const int r = slot[j];
+    if (out[j].err) return record_error(ISDF_ERR_TIMEOUT, "kmeans batch: a group barrier timed out");
+    std::vector<int> sel(out[j].rk);
+    ISDF_TRY(read_back(sel.data(), bufs[r].sel, sizeof(int) * sel.size(), stream));
+    res[r].iters = out[j].iters;
+    res[r].rk_eff = piv_from_selection(sel, (int)args[r].ng, args[r].piv);
+    res[r].launches = 8 + (int)((jobs.size() + max_jobs - 1) / max_jobs);
+  }
+  return ISDF_OK;
+}
+
 }  // namespace isdf_b200

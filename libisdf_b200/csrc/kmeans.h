@@ -32,6 +32,15 @@ struct KmeansResult {
 };
 
 size_t kmeans_workspace_bytes(long long ng, int mu);
+
+// Batched selection of small systems in one cooperative launch (the serving
+// loop's batches): cold start only, ng <= kKmeansBatchMaxNg, mu <= kKmeansBatchMaxMu.
+// piv and the results equal kmeans_select()'s for each request.
+constexpr int kKmeansBatchMaxMu = 512;
+constexpr long long kKmeansBatchMaxNg = 1 << 20;
+size_t kmeans_batch_workspace_bytes(long long ng, int mu);
+int kmeans_select_batch(const KmeansArgs* args, int count, Arena& arena, cudaStream_t stream,
+                        KmeansResult* res);
 int kmeans_weight(const double* d_psi, long long ng, int nocc, int nv1, int nc1, int nv2, int nc2,
                   double* d_w, cudaStream_t stream);
 int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, KmeansResult* res);

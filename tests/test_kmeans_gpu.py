@@ -186,3 +186,43 @@ def test_warm_start_si8_perturbed_orbitals(torch_cuda):
     assert np.array_equal(piv, piv_o)
     record_parity("K-means warm start Si8-like", "Lloyd iterations warm / cold",
                   f"{rep2.kmeans_iters} / {cold[2]} (first solve {rep1.kmeans_iters})")
+
+
+def test_batched_selection_matches_reference(torch_cuda):
+    """The batched selection of small systems (one cooperative launch, a CTA
+    group per system, the serving loop's path for small requests): every
+    result equals the reference's (goldens: piv, effective mu, iteration
+    count, including the npt < mu early return) and, for the Si8-like system
+    and a random-weight grid, the port's, in one batch of mixed sizes."""
+    torch = torch_cuda
+    names = ["si8_example", "small_s1s2", "small_mu0", "small_iters0", "small_early"]
+    doms, ws, mus, its, want = [], [], [], [], []
+    for name in names:
+        g = load_golden(name)
+        doms.append(isdf.Domain(length=tuple(g["length"]), num_grid=tuple(int(x) for x in g["ng"])))
+        ws.append(torch.from_numpy(g["weight"]).cuda())
+        mus.append(int(g["rk_requested"]))
+        its.append(int(g["iters"]))
+        want.append((g["piv"], int(g["rk_eff"]), int(g["n_iter"])))
+    s = synth.SI8
+    psi = synth.shape_orbitals(s, 0)
+    w8 = port.weight(psi, s.nocc, s.nv1, s.nc1, s.nv2, s.nc2)
+    p8, r8, i8 = port.kmeans(w8, (s.n,) * 3, (s.length,) * 3, s.mu, s.kmeans_iters)
+    doms.append(isdf.Domain(length=(s.length,) * 3, num_grid=(s.n,) * 3))
+    ws.append(torch.from_numpy(w8).cuda())
+    mus.append(s.mu)
+    its.append(s.kmeans_iters)
+    want.append((p8, r8, i8))
+    rng = np.random.default_rng(3)
+    ng = (30, 25, 20)
+    wr = rng.uniform(0.0, 1.0, size=int(np.prod(ng))) ** 4
+    pr, rr, ir = port.kmeans(wr, ng, (12.0, 7.5, 9.0), 500, 40)
+    doms.append(isdf.Domain(length=(12.0, 7.5, 9.0), num_grid=ng))
+    ws.append(torch.from_numpy(wr).cuda())
+    mus.append(500)
+    its.append(40)
+    want.append((pr, rr, ir))
+    got = isdf.kmeans_select_batch(doms, ws, mus, its, rand_seed=1)
+    for k, ((piv, rk, it, _), (wp, wr_, wi)) in enumerate(zip(got, want)):
+        assert (rk, it) == (wr_, wi), k
+        assert np.array_equal(piv, wp), k
