@@ -225,16 +225,21 @@ int isdf_fit_noalloc(const double* d_psi, long long ng, int nstate, int nocc, in
  * time; `slots` solves run concurrently on their own streams (their kernels
  * overlap on the GPU); a request starts when its device workspace fits in
  * what the budget has left (small requests may pass a large head until it
- * has been passed `max_skips` times); psi / theta / piv stay the caller's
- * buffers (device, device, host) and must stay valid until the request is
- * done. Results are the same as isdf_solve() on the same request. */
+ * has been passed `max_skips` times); the K-means selections of small
+ * requests waiting together run in one launch (batch_small), their fits then
+ * on the slots; psi / theta / piv stay the caller's buffers (device, device,
+ * host) and must stay valid until the request is done. Results are the same
+ * as isdf_solve() on the same request, bit for bit. */
 typedef struct isdf_server_config_t {
   int device;              /* CUDA device of the server (default 0) */
   int slots;               /* concurrent solves (default 4) */
   size_t hbm_budget_bytes; /* workspace budget; 0 = half of the free memory at creation */
   int max_queue;           /* pending requests before submit returns ISDF_ERR_BUSY (4096) */
   int max_skips;           /* times a waiting head may be passed by smaller requests (64) */
-  int reserved[4];
+  int batch_small;         /* small K-means requests (Ng <= 2^20, mu <= 512, cold start)
+                              whose selections run together in one launch, at most this
+                              many at a time (default 32; 0: each request on its own) */
+  int reserved[3];
 } isdf_server_config_t;
 
 typedef struct isdf_request_t {

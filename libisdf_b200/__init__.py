@@ -81,7 +81,8 @@ class _Report(ctypes.Structure):
 class _ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int),
                 ("hbm_budget_bytes", ctypes.c_size_t), ("max_queue", ctypes.c_int),
-                ("max_skips", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
+                ("max_skips", ctypes.c_int), ("batch_small", ctypes.c_int),
+                ("reserved", ctypes.c_int * 3)]
 
 
 class _Request(ctypes.Structure):
@@ -362,7 +363,7 @@ class Server:
     host) until they are done."""
 
     def __init__(self, slots: int = 4, hbm_budget_bytes: int = 0, device: int = 0,
-                 max_skips: int = 64, max_queue: int = 4096):
+                 max_skips: int = 64, max_queue: int = 4096, batch_small: int = 32):
         L = lib()
         P, I, LL = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong
         L.isdf_server_create.argtypes = [ctypes.POINTER(_ServerConfig), ctypes.POINTER(P)]
@@ -377,6 +378,7 @@ class Server:
         cfg = _ServerConfig()
         cfg.device, cfg.slots, cfg.hbm_budget_bytes = device, slots, hbm_budget_bytes
         cfg.max_queue, cfg.max_skips = max_queue, max_skips
+        cfg.batch_small = batch_small
         self._h = ctypes.c_void_p()
         _check(L.isdf_server_create(ctypes.byref(cfg), ctypes.byref(self._h)))
         self._keep = {}

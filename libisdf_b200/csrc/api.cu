@@ -209,7 +209,15 @@ int solve(const isdf_domain_t* dom, const double* d_psi, int nocc, int nstate, i
   const size_t mark = arena.off;
 
   int rk_fit = rk;
-  if (selector == ISDF_SELECT_KMEANS) {
+  if (selector == ISDF_SELECT_KMEANS && res && res->preselected) {
+    const KmeansResult& kr = *res->preselected;
+    rep.rk_eff = kr.rk_eff;
+    rep.kmeans_iters = kr.iters;
+    rep.npt = kr.npt;
+    rep.kmeans_warm_pivots = -1;
+    rep.kernel_launches = kr.launches;
+    rk_fit = kr.rk_eff;
+  } else if (selector == ISDF_SELECT_KMEANS) {
     // (a) K-means selection
     KmeansArgs ka;
     ka.d_w = d_w;

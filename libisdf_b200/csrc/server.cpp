@@ -16,6 +16,14 @@
 // 1e13) run one at a time: two of them on the tensor cores at once only
 // share the units and the power cap, while another request's K-means
 // selection (FP64 CUDA cores) overlaps a running fit.
+//
+// Small K-means requests (Ng <= 2^20, mu <= 512, cold start) queue apart: a
+// batcher thread takes up to batch_small of them at once, computes their
+// weights and runs all their selections in one cooperative launch
+// (kmeans_select_batch), then puts them back at the head of the main queue,
+// where the slots run their fits. A small solve is latency bound (about a
+// hundred Lloyd iterations of ten small kernels each), so one launch for many
+// of them raises the rate at which they are served.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,6 +39,7 @@
 
 #include "../../include/isdf_c.h"
 #include "arena.h"
+#include "kmeans.h"
 #include "solve.h"
 
 namespace isdf_b200 {
@@ -47,6 +56,11 @@ struct Job {
   int skips = 0;
   isdf_report_t rep;
   Clock::time_point submit, start, finish;
+  bool small = false;     // selection by the batcher
+  bool selected = false;  // the batcher has run its selection
+  size_t batch_bytes = 0;
+  KmeansResult sel;
+  double select_ms = 0;
 };
 
 struct Server {
@@ -54,12 +68,15 @@ struct Server {
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<long long> queue;
+  std::deque<long long> small_queue;  // small K-means requests waiting for the batcher
   std::map<long long, Job> jobs;
   long long next_ticket = 1;
   size_t in_use = 0, peak_bytes = 0;
   int running = 0, peak_running = 0;
   bool stopping = false;
   std::vector<std::thread> workers;
+  std::thread batcher;
+  bool batcher_active = false;  // the batcher may still hand requests to the slots
   cudaMemPool_t pool = nullptr;
   std::vector<double> latencies_ms;
   Clock::time_point first_submit, last_finish;
@@ -98,14 +115,16 @@ void worker(Server* s, int slot) {
     long long t = -1;
     {
       std::unique_lock<std::mutex> lk(s->mu);
+      // on stop, the slots still finish the requests whose selection the
+      // batcher has done (and may still hand over) before they exit
       s->cv_work.wait(lk, [&] {
-        if (s->stopping) return true;
-        return (t = pick(s)) >= 0;
+        if ((t = pick(s)) >= 0) return true;
+        return s->stopping && !s->batcher_active;
       });
       if (t < 0) break;  // stopping and nothing startable
       Job& j = s->jobs[t];
+      if (!j.selected) j.start = Clock::now();
       j.state = 1;
-      j.start = Clock::now();
       s->in_use += j.footprint;
       s->peak_bytes = std::max(s->peak_bytes, s->in_use);
       s->running++;
@@ -117,6 +136,8 @@ void worker(Server* s, int slot) {
       jp = &s->jobs[t];
     }
     isdf_request_t req = jp->req;
+    const bool pre = jp->selected;
+    const KmeansResult sel = jp->sel;
     isdf_report_t rep;
     std::memset(&rep, 0, sizeof(rep));
     int rc = ISDF_OK;
@@ -125,7 +146,8 @@ void worker(Server* s, int slot) {
       (void)cudaGetLastError();
       rc = set_err(ISDF_ERR_NOMEM, "server: workspace allocation failed");
     } else {
-      SolveResources res{static_cast<char*>(ws), jp->footprint, stream, &s->fit_mutex};
+      SolveResources res{static_cast<char*>(ws), jp->footprint, stream, &s->fit_mutex,
+                         pre ? &sel : nullptr};
       rc = solve(&req.dom, req.d_psi, req.nocc, req.nstate, req.nv1, req.nc1, req.nv2, req.nc2,
                  req.mu_points, req.d_theta, req.piv, req.kmeans_max_iter, req.selector, req.check,
                  &req.opt, &rep, &res);
@@ -138,6 +160,7 @@ void worker(Server* s, int slot) {
       j.state = 2;
       j.status = rc;
       j.rep = rep;
+      if (j.selected) j.rep.t_select_ms = j.select_ms;
       j.finish = Clock::now();
       s->in_use -= j.footprint;
       s->running--;
@@ -153,6 +176,108 @@ void worker(Server* s, int slot) {
     s->cv_done.notify_all();
     s->cv_work.notify_all();
   }
+  cudaStreamDestroy(stream);
+}
+
+// The batcher: small K-means requests' weights and selections, many per launch.
+void batcher(Server* s) {
+  cudaSetDevice(s->cfg.device);
+  cudaStream_t stream = nullptr;
+  cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+  for (;;) {
+    std::vector<long long> batch;
+    size_t bytes = 0;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_work.wait(lk, [&] {
+        if (s->stopping) return true;
+        if (s->small_queue.empty()) return false;
+        const Job& h = s->jobs[s->small_queue.front()];
+        return s->in_use + h.batch_bytes <= s->cfg.hbm_budget_bytes;
+      });
+      if (s->stopping && s->small_queue.empty()) {
+        s->batcher_active = false;
+        break;
+      }
+      while (!s->small_queue.empty() && (int)batch.size() < s->cfg.batch_small) {
+        Job& j = s->jobs[s->small_queue.front()];
+        if (s->in_use + bytes + j.batch_bytes > s->cfg.hbm_budget_bytes) break;
+        bytes += j.batch_bytes;
+        batch.push_back(j.ticket);
+        s->small_queue.pop_front();
+        j.state = 1;
+        j.start = Clock::now();
+      }
+      if (batch.empty()) continue;
+      s->in_use += bytes;
+      s->peak_bytes = std::max(s->peak_bytes, s->in_use);
+      s->running += (int)batch.size();
+      s->peak_running = std::max(s->peak_running, s->running);
+    }
+    const auto t0 = Clock::now();
+    std::vector<KmeansArgs> args(batch.size());
+    std::vector<KmeansResult> res(batch.size());
+    int rc = ISDF_OK;
+    void* ws = nullptr;
+    if (cudaMallocFromPoolAsync(&ws, bytes + 4096, s->pool, stream) != cudaSuccess) {
+      (void)cudaGetLastError();
+      rc = set_err(ISDF_ERR_NOMEM, "server: batch workspace allocation failed");
+    } else {
+      Arena arena;
+      arena.base = static_cast<char*>(ws);
+      arena.cap = bytes + 4096;
+      arena.off = 0;
+      for (size_t i = 0; i < batch.size() && rc == ISDF_OK; ++i) {
+        isdf_request_t r;
+        {
+          std::lock_guard<std::mutex> lk(s->mu);
+          r = s->jobs[batch[i]].req;
+        }
+        const long long ng = (long long)r.dom.num_grid[0] * r.dom.num_grid[1] * r.dom.num_grid[2];
+        double* d_w = arena.take<double>((size_t)ng);
+        rc = kmeans_weight(r.d_psi, ng, r.nocc, r.nv1, r.nc1, r.nv2, r.nc2, d_w, stream);
+        KmeansArgs& a = args[i];
+        a.d_w = d_w;
+        a.ng = ng;
+        for (int k = 0; k < 3; ++k) {
+          a.num_grid[k] = r.dom.num_grid[k];
+          a.length[k] = r.dom.length[k];
+        }
+        a.mu = r.mu_points == 0 ? default_mu(r.nv1, r.nc1, r.nv2, r.nc2) : r.mu_points;
+        a.max_iter = r.kmeans_max_iter;
+        a.rand_seed = r.opt.rand_seed;
+        a.piv = r.piv;
+      }
+      if (rc == ISDF_OK) rc = kmeans_select_batch(args.data(), (int)args.size(), arena, stream, res.data());
+      cudaFreeAsync(ws, stream);
+      cudaStreamSynchronize(stream);
+    }
+    const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->in_use -= bytes;
+      s->running -= (int)batch.size();
+      // back to the head of the main queue, in arrival order, for their fits
+      for (size_t k = batch.size(); k-- > 0;) {
+        Job& j = s->jobs[batch[k]];
+        if (rc == ISDF_OK) {
+          j.selected = true;
+          j.sel = res[k];
+          j.select_ms = ms;
+          s->queue.push_front(j.ticket);
+        } else {
+          j.state = 2;
+          j.status = rc;
+          j.finish = Clock::now();
+          s->last_finish = j.finish;
+          s->failed++;
+        }
+      }
+    }
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+  }
+  s->cv_work.notify_all();
   cudaStreamDestroy(stream);
 }
 
@@ -186,6 +311,7 @@ void isdf_server_default_config(isdf_server_config_t* cfg) {
   cfg->hbm_budget_bytes = 0;
   cfg->max_queue = 4096;
   cfg->max_skips = 64;
+  cfg->batch_small = 32;
 }
 
 int isdf_server_create(const isdf_server_config_t* cfg_in, void** out) {
@@ -194,6 +320,8 @@ int isdf_server_create(const isdf_server_config_t* cfg_in, void** out) {
   isdf_server_default_config(&cfg);
   if (cfg_in) cfg = *cfg_in;
   if (cfg.slots < 1 || cfg.slots > 64) return record_error(ISDF_ERR_ARG, "server: slots in [1, 64]");
+  if (cfg.batch_small < 0 || cfg.batch_small > 1024)
+    return record_error(ISDF_ERR_ARG, "server: batch_small in [0, 1024]");
   if (cudaSetDevice(cfg.device) != cudaSuccess) return record_error(ISDF_ERR_ARG, "server: device");
   if (cfg.hbm_budget_bytes == 0) {
     size_t free_b = 0, total_b = 0;
@@ -215,6 +343,10 @@ int isdf_server_create(const isdf_server_config_t* cfg_in, void** out) {
   unsigned long long keep = cfg.hbm_budget_bytes;
   cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
   for (int i = 0; i < cfg.slots; ++i) s->workers.emplace_back(worker, s, i);
+  if (cfg.batch_small > 0) {
+    s->batcher_active = true;
+    s->batcher = std::thread(batcher, s);
+  }
   *out = s;
   return ISDF_OK;
 }
@@ -239,6 +371,21 @@ int isdf_server_submit(void* server, const isdf_request_t* req, long long* ticke
     j.req.opt.stream = nullptr;
     j.footprint = fp;
     j.submit = Clock::now();
+    {
+      const isdf_domain_t& d = req->dom;
+      const long long ng = (long long)d.num_grid[0] * d.num_grid[1] * d.num_grid[2];
+      const int rk = req->mu_points == 0 ? default_mu(req->nv1, req->nc1, req->nv2, req->nc2)
+                                         : req->mu_points;
+      j.small = s->cfg.batch_small > 0 && req->selector == ISDF_SELECT_KMEANS &&
+                !req->opt.kmeans_warm_start && ng > 1 && ng <= kKmeansBatchMaxNg && rk > 0 &&
+                rk <= kKmeansBatchMaxMu && rk <= ng && req->kmeans_max_iter >= 0 &&
+                d.num_grid[0] > 0 && d.num_grid[1] > 0 && d.num_grid[2] > 0 &&
+                req->opt.refine_steps == 0 && req->nv1 >= 0 && req->nc1 >= 0 && req->nv2 >= 0 &&
+                req->nc2 >= 0 && req->nv1 + req->nc1 > 0 && req->nv2 + req->nc2 > 0 &&
+                req->nocc - req->nv1 >= 0 && req->nocc + req->nc1 <= req->nstate &&
+                req->nocc - req->nv2 >= 0 && req->nocc + req->nc2 <= req->nstate;
+      if (j.small) j.batch_bytes = kmeans_batch_workspace_bytes(ng, rk) + sizeof(double) * ng + 512;
+    }
     std::memset(&j.rep, 0, sizeof(j.rep));
     if (!s->any_submit) {
       s->first_submit = j.submit;
@@ -246,9 +393,10 @@ int isdf_server_submit(void* server, const isdf_request_t* req, long long* ticke
     }
     *ticket = j.ticket;
     s->jobs[j.ticket] = j;
-    s->queue.push_back(j.ticket);
+    if (j.small) s->small_queue.push_back(j.ticket);
+    else s->queue.push_back(j.ticket);
   }
-  s->cv_work.notify_one();
+  s->cv_work.notify_all();
   return ISDF_OK;
 }
 
@@ -285,9 +433,15 @@ int isdf_server_cancel(void* server, long long ticket) {
   Server* s = static_cast<Server*>(server);
   if (!s) return record_error(ISDF_ERR_ARG, "server: null");
   std::lock_guard<std::mutex> lk(s->mu);
-  auto it = std::find(s->queue.begin(), s->queue.end(), ticket);
-  if (it == s->queue.end()) return record_error(ISDF_ERR_ARG, "server: not queued (running or done)");
-  s->queue.erase(it);
+  auto it = std::find(s->small_queue.begin(), s->small_queue.end(), ticket);
+  if (it != s->small_queue.end()) {
+    s->small_queue.erase(it);
+  } else {
+    auto qt = std::find(s->queue.begin(), s->queue.end(), ticket);
+    if (qt == s->queue.end() || s->jobs[ticket].selected)
+      return record_error(ISDF_ERR_ARG, "server: not queued (running or done)");
+    s->queue.erase(qt);
+  }
   Job& j = s->jobs[ticket];
   j.state = 2;
   j.status = ISDF_ERR_CANCELLED;
@@ -317,7 +471,7 @@ int isdf_server_stats(void* server, isdf_server_stats_t* st) {
   st->solves_per_s = span > 0 ? (double)s->completed / span : 0.0;
   st->peak_concurrency = s->peak_running;
   st->peak_bytes = s->peak_bytes;
-  st->queued = (int)s->queue.size();
+  st->queued = (int)(s->queue.size() + s->small_queue.size());
   st->running = s->running;
   return ISDF_OK;
 }
@@ -327,17 +481,30 @@ int isdf_server_destroy(void* server) {
   if (!s) return ISDF_OK;
   {
     std::lock_guard<std::mutex> lk(s->mu);
+    std::deque<long long> keep;  // selected small requests finish their fits
     for (long long t : s->queue) {
+      Job& j = s->jobs[t];
+      if (j.selected) {
+        keep.push_back(t);
+        continue;
+      }
+      j.state = 2;
+      j.status = ISDF_ERR_CANCELLED;
+      s->cancelled++;
+    }
+    for (long long t : s->small_queue) {
       Job& j = s->jobs[t];
       j.state = 2;
       j.status = ISDF_ERR_CANCELLED;
       s->cancelled++;
     }
-    s->queue.clear();
+    s->small_queue.clear();
+    s->queue = keep;
     s->stopping = true;
   }
   s->cv_work.notify_all();
   s->cv_done.notify_all();
+  if (s->batcher.joinable()) s->batcher.join();
   for (auto& w : s->workers) w.join();
   if (s->pool) cudaMemPoolDestroy(s->pool);
   delete s;

@@ -29,11 +29,15 @@ std::mutex& attr_mutex();
 // fit_lock (optional): held around the fit of a large system (Ng rk^2 at
 // least kSerialFitWork), so that large fits run one at a time while other
 // requests' selections and small fits overlap them.
+struct KmeansResult;
 struct SolveResources {
   char* base;
   size_t cap;
   cudaStream_t stream;
   std::mutex* fit_lock = nullptr;
+  // K-means selection already done (the serving loop's batched selections):
+  // piv holds its result and the solve starts at the fit
+  const KmeansResult* preselected = nullptr;
 };
 constexpr double kSerialFitWork = 1e13;
 

@@ -1,9 +1,10 @@
 """Continuous-batching server: a mix of systems of different grid sizes and
 mu, submitted while others run, gives for every request exactly what a solve
-of that request alone gives (bit-identical theta and piv, FP64 and mixed);
-solves overlap (peak concurrency > 1); admission by device footprint lets a
-large request wait while small ones pass, without starving it; a queued
-request can be cancelled."""
+of that request alone gives (bit-identical theta and piv, FP64 and mixed,
+with the small requests' selections batched into shared launches and with
+batching off); solves overlap (peak concurrency > 1); admission by device
+footprint lets a large request wait while small ones pass, without starving
+it; a queued request can be cancelled."""
 import numpy as np
 import pytest
 
@@ -42,12 +43,13 @@ def _alone(torch, r, prec):
     return d_theta.cpu().numpy(), piv
 
 
-@pytest.mark.parametrize("prec", [isdf.PRECISION_FP64, isdf.PRECISION_MIXED])
-def test_mix_equals_alone(torch_cuda, prec):
+@pytest.mark.parametrize("prec,batch", [(isdf.PRECISION_FP64, 32), (isdf.PRECISION_MIXED, 32),
+                                        (isdf.PRECISION_FP64, 0)])
+def test_mix_equals_alone(torch_cuda, prec, batch):
     torch = torch_cuda
     reqs = _requests(torch)
     alone = [_alone(torch, r, prec) for r in reqs]
-    with isdf.Server(slots=3) as srv:
+    with isdf.Server(slots=3, batch_small=batch) as srv:
         outs = []
         for rep in range(2):  # every request twice, interleaved
             for r in reqs:
