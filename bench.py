@@ -715,26 +715,11 @@ def run_select(args, shape):
                                  "rk_eff": rk, "kmeans_iters": iters, "npt": npt}}), flush=True)
 
 
-def run_serve(args):
-    """--serve: the serving mix (60 % Si8-like, 30 % Si64-like, 10 % Si216-like
-    requests, K-means, --precision) arriving as a Poisson process at --rate
-    requests/s, through the continuous-batching server (isdf_server_*).
-    Latency is arrival -> completion as the client sees it (it includes any
-    wait for a free output buffer); throughput is requests / (last completion
-    - first arrival). psi comes from a small pool per shape (seeds 100, 101,
-    ...), the request index picking the seed; every in-flight request has its
-    own theta and piv."""
-    import threading
-
-    import torch
-
-    import libisdf_b200 as isdf
-    from libisdf_b200 import synth
-
-    torch.cuda.set_device(0)
+def _serve_setup(args, torch, isdf, synth):
+    """psi pools per shape (seeds 100, 101, ...) and theta buffers, on the GPU."""
     shapes = [synth.SI8, synth.SI64, synth.SI216]
     pool_seeds = [4, 2, 1]
-    theta_bufs = [8, 4, 1]
+    theta_bufs = [16, 4, 2]
     mix = [0.6, 0.3, 0.1]
     if args.serve_mix != "standard":
         # one shape only (the served form's throughput at that size)
@@ -742,29 +727,39 @@ def run_serve(args):
         mix = [1.0 if k == k1 else 0.0 for k in range(3)]
         pool_seeds = [1 if k == k1 else 0 for k in range(3)]
         theta_bufs = [args.slots if k == k1 else 0 for k in range(3)]
-    rng = np.random.default_rng(args.serve_seed)
-    n_req = args.requests
-    kinds = rng.choice(3, size=n_req, p=mix)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, size=n_req))
-    prec = isdf.PRECISION_MIXED if args.precision == "mixed" else isdf.PRECISION_FP64
-    opts = isdf.Options(precision=prec)
     psi = {k: [torch.from_numpy(np.ascontiguousarray(
         synth.shape_orbitals(shapes[k], 100 + j, device="cuda").T)).cuda()
         for j in range(pool_seeds[k])] for k in range(3)}
-    free = {k: [torch.empty((shapes[k].mu, shapes[k].ng), dtype=torch.float64, device="cuda")
-                for _ in range(theta_bufs[k])] for k in range(3)}
+    thetas = {k: [torch.empty((shapes[k].mu, shapes[k].ng), dtype=torch.float64, device="cuda")
+                  for _ in range(theta_bufs[k])] for k in range(3)}
     doms = [isdf.Domain(length=(sh.length,) * 3, num_grid=(sh.n,) * 3) for sh in shapes]
     torch.cuda.synchronize()
+    return shapes, pool_seeds, theta_bufs, mix, psi, thetas, doms
 
+
+def serve_once(args, torch, isdf, setup, rate, precision, batch_small):
+    """One pass of args.requests Poisson arrivals at `rate` requests/s through
+    a fresh server. Latency is arrival -> completion as the client sees it
+    (it includes any wait for a free output buffer); throughput is requests /
+    (last completion - first arrival)."""
+    shapes, pool_seeds, theta_bufs, mix, psi, thetas, doms = setup
+    rng = np.random.default_rng(args.serve_seed)
+    n_req = args.requests
+    kinds = rng.choice(3, size=n_req, p=mix)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    prec = isdf.PRECISION_MIXED if precision == "mixed" else isdf.PRECISION_FP64
+    opts = isdf.Options(precision=prec)
+    free = {k: list(thetas[k]) for k in range(3)}
     budget = 0
     if args.hbm_budget_gb > 0:
         budget = int(args.hbm_budget_gb * (1 << 30))
     elif args.hbm_budget_gb < 0:  # all that is free now, less 4 GiB
         budget = max(0, torch.cuda.mem_get_info()[0] - (4 << 30))
-    srv = isdf.Server(slots=args.slots, hbm_budget_bytes=budget)
+    srv = isdf.Server(slots=args.slots, hbm_budget_bytes=budget, batch_small=batch_small)
     lock = threading.Condition()
     inflight = {}  # ticket -> (kind, theta, arrival index)
     done_at = np.zeros(n_req)
+    errors = []
 
     def submit(k, i, theta):
         sh = shapes[k]
@@ -797,11 +792,10 @@ def run_serve(args):
                         del inflight[t]
                         free[k].append(th)
                         if st != 0:
-                            inflight_errors.append(t)
+                            errors.append(t)
                     lock.notify_all()
             time.sleep(0.0005)
 
-    inflight_errors = []
     th_poll = threading.Thread(target=poller, daemon=True)
     th_poll.start()
     t0 = time.perf_counter()
@@ -824,25 +818,54 @@ def run_serve(args):
     srv.close()
     lat = (done_at - arr_at) * 1e3
     span = done_at.max() - arr_at[0]
-    line = {"metric": "served ISDF solves/s (serving mix)", "value": n_req / span,
-            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
-            "data": "synthetic", "precision": args.precision,
-            "config": {"workload": ("serving mix: 60 % Si8-like, 30 % Si64-like, 10 % Si216-like, "
-                                    "K-means" if args.serve_mix == "standard" else
-                                    f"served {args.serve_mix} requests only, K-means"),
-                       "requests": n_req, "rate_per_s": args.rate,
-                       "hbm_budget_bytes": budget,
-                       "slots": args.slots, "psi_pool_seeds": pool_seeds,
-                       "theta_buffers": theta_bufs,
-                       "mix_counts": [int((kinds == k).sum()) for k in range(3)]},
+    return {"rate_per_s": rate, "precision": precision, "batch_small": batch_small,
+            "solves_per_s": n_req / span, "kept_up": bool(n_req / span >= 0.95 * rate),
             "latency_ms": {"p50": float(np.percentile(lat, 50)),
                            "p99": float(np.percentile(lat, 99)),
                            "p50_by_shape": {shapes[k].name: float(np.percentile(lat[kinds == k], 50))
+                                            for k in range(3) if (kinds == k).any()},
+                           "p99_by_shape": {shapes[k].name: float(np.percentile(lat[kinds == k], 99))
                                             for k in range(3) if (kinds == k).any()}},
-            "errors": len(inflight_errors),
+            "errors": len(errors),
             "server": {k: stats[k] for k in stats if k in ("completed", "peak_concurrency",
                                                               "p50_ms", "p99_ms", "peak_bytes")},
             "clocks": clk.summary()}
+
+
+def run_serve(args):
+    """--serve: the serving mix (60 % Si8-like, 30 % Si64-like, 10 % Si216-like
+    requests, K-means; per-request orbitals from a small pool of seeds per
+    shape, every in-flight request with its own theta and piv) arriving as a
+    Poisson process through the continuous-batching server (isdf_server_*),
+    at each rate of --rates (default: --rate) and for each form of
+    --serve-forms; one JSON line with the whole sweep."""
+    import torch
+
+    import libisdf_b200 as isdf
+    from libisdf_b200 import synth
+
+    torch.cuda.set_device(0)
+    setup = _serve_setup(args, torch, isdf, synth)
+    rates = [float(x) for x in args.rates.split(",")] if args.rates else [args.rate]
+    forms = args.serve_forms.split(",")
+    sweep = [serve_once(args, torch, isdf, setup, r, f, args.batch_small)
+             for f in forms for r in rates]
+    best = {f: max((x for x in sweep if x["precision"] == f), key=lambda x: x["solves_per_s"])
+            for f in forms}
+    head = best[forms[0]]
+    line = {"metric": "served ISDF solves/s (serving mix)", "value": head["solves_per_s"],
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": ("serving mix: 60 % Si8-like, 30 % Si64-like, 10 % Si216-like, "
+                                    "K-means" if args.serve_mix == "standard" else
+                                    f"served {args.serve_mix} requests only, K-means"),
+                       "requests_per_rate": args.requests, "rates_per_s": rates,
+                       "forms": forms, "slots": args.slots, "batch_small": args.batch_small,
+                       "hbm_budget_gb": args.hbm_budget_gb},
+            "best_by_form": {f: {"rate_per_s": b["rate_per_s"], "solves_per_s": b["solves_per_s"],
+                                 "p50_ms": b["latency_ms"]["p50"],
+                                 "p99_ms": b["latency_ms"]["p99"]} for f, b in best.items()},
+            "sweep": sweep}
     print(json.dumps(line), flush=True)
 
 
@@ -873,6 +896,12 @@ def main():
                     help="the serving mix through isdf_server_* (Poisson arrivals)")
     ap.add_argument("--requests", type=int, default=512)
     ap.add_argument("--rate", type=float, default=4.0, help="arrivals per second (--serve)")
+    ap.add_argument("--rates", type=str, default="",
+                    help="--serve: comma-separated arrival rates to sweep (default: --rate)")
+    ap.add_argument("--serve-forms", type=str, default="mixed,fp64",
+                    help="--serve: comma-separated precisions to serve (mixed, fp64)")
+    ap.add_argument("--batch-small", type=int, default=32,
+                    help="--serve: small requests per batched K-means launch (0: off)")
     ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--serve-seed", type=int, default=7)
     ap.add_argument("--serve-mix", choices=["standard", "si8", "si64", "si216"], default="standard",
