@@ -681,38 +681,68 @@ def _int8_peak_tops(torch):
 def run_select(args, shape):
     """--stage select: the K-means selection alone (weight computed once),
     selections/s; a small-footprint command for profiling the K-means kernels
-    at full grid size (psi, the weight and the K-means workspace only)."""
+    at full grid size (psi, the weight and the K-means workspace only).
+    With --batch B > 1: B systems of the shape (seeds 100..), their selections
+    in one batched launch (isdf_kmeans_select_batch) against the same B run
+    one after another through isdf_kmeans_select, both timed."""
     import torch
 
     import libisdf_b200 as isdf
     from libisdf_b200 import synth
 
     torch.cuda.set_device(0)
-    psi = synth.shape_orbitals(shape, 1, device="cuda")
-    d_psi = torch.from_numpy(np.ascontiguousarray(psi.T)).cuda()
-    d_w = torch.empty(shape.ng, dtype=torch.float64, device="cuda")
+    B = max(1, args.batch)
     dom = isdf.Domain(length=(shape.length,) * 3, num_grid=(shape.n,) * 3)
     stream = torch.cuda.Stream()
-    isdf.kmeans_weight(d_psi, shape.ng, shape.nstate, shape.nocc, shape.nv1, shape.nc1, shape.nv2,
-                       shape.nc2, d_w, stream=stream.cuda_stream)
+    ws = []
+    for b in range(B):
+        psi = synth.shape_orbitals(shape, 1 if B == 1 else 100 + b, device="cuda")
+        d_psi = torch.from_numpy(np.ascontiguousarray(psi.T)).cuda()
+        d_w = torch.empty(shape.ng, dtype=torch.float64, device="cuda")
+        isdf.kmeans_weight(d_psi, shape.ng, shape.nstate, shape.nocc, shape.nv1, shape.nc1,
+                           shape.nv2, shape.nc2, d_w, stream=stream.cuda_stream)
+        ws.append(d_w)
+        del d_psi
     torch.cuda.synchronize()
-    for _ in range(max(3, args.warmup)):
-        isdf.kmeans_select(dom, d_w, shape.mu, shape.kmeans_iters, stream=stream.cuda_stream)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        _, rk, iters, npt = isdf.kmeans_select(dom, d_w, shape.mu, shape.kmeans_iters,
-                                               stream=stream.cuda_stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_ms = e0.elapsed_time(e1)
-    print(json.dumps({"metric": "K-means selections/s", "value": args.steps / (t_ms * 1e-3),
-                      "unit": "selections/s", "n_gpus": 1, "steps": args.steps,
-                      "warmup": max(3, args.warmup), "ms_per_step": t_ms / args.steps,
-                      "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-                      "config": {"workload": shape.name, "ng": shape.ng, "mu": shape.mu,
-                                 "rk_eff": rk, "kmeans_iters": iters, "npt": npt}}), flush=True)
+
+    def one_by_one():
+        out = []
+        for d_w in ws:
+            out.append(isdf.kmeans_select(dom, d_w, shape.mu, shape.kmeans_iters,
+                                          stream=stream.cuda_stream))
+        return out
+
+    def batched():
+        return isdf.kmeans_select_batch([dom] * B, ws, [shape.mu] * B,
+                                        [shape.kmeans_iters] * B, stream=stream.cuda_stream)
+
+    def timed(fn):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    t_ms, out = timed(one_by_one)
+    line = {"metric": "K-means selections/s", "value": B * args.steps / (t_ms * 1e-3),
+            "unit": "selections/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": t_ms / args.steps,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": shape.name, "ng": shape.ng, "mu": shape.mu,
+                       "systems_per_step": B, "rk_eff": out[0][1], "kmeans_iters": out[0][2],
+                       "npt": out[0][3]}}
+    if B > 1:
+        tb_ms, outb = timed(batched)
+        same = all(np.array_equal(a[0], b[0]) and a[1:] == b[1:] for a, b in zip(out, outb))
+        line["batched"] = {"value": B * args.steps / (tb_ms * 1e-3), "unit": "selections/s",
+                           "ms_per_step": tb_ms / args.steps, "identical_to_one_by_one": same,
+                           "speedup": t_ms / tb_ms}
+    print(json.dumps(line), flush=True)
 
 
 def _serve_setup(args, torch, isdf, synth):
@@ -892,6 +922,8 @@ def main():
     ap.add_argument("--qrcp-seed", type=int, default=41)
     ap.add_argument("--stage", choices=["solve", "select"], default="solve",
                     help="select: time the K-means selection alone (profiling aid)")
+    ap.add_argument("--batch", type=int, default=1,
+                    help="--stage select: systems per step, batched launch vs one by one")
     ap.add_argument("--serve", action="store_true",
                     help="the serving mix through isdf_server_* (Poisson arrivals)")
     ap.add_argument("--requests", type=int, default=512)
