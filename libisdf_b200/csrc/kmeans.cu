@@ -1635,9 +1635,11 @@ BatchBuffers carve_batch(Arena& a, int n, int G) {
   return b;
 }
 
+constexpr int kBatchMaxGroup = 16;  // CTAs per request
+
 int batch_group(long long n) {
   long long g = (n + 4095) / 4096;
-  return (int)std::max(1LL, std::min(16LL, g));
+  return (int)std::max(1LL, std::min((long long)kBatchMaxGroup, g));
 }
 
 }  // namespace
@@ -1665,7 +1667,9 @@ size_t kmeans_batch_workspace_bytes(long long ng, int mu) {
   (void)mu;
   Arena a;
   a.counting = true;
-  carve_batch(a, (int)ng, batch_group(ng));
+  // the histogram sized for the largest group: a batch runs every request
+  // with the largest group any of its requests needs
+  carve_batch(a, (int)ng, kBatchMaxGroup);
   a.take<KmBatchJob>(1);
   return a.off + 512;
 }
