@@ -92,20 +92,24 @@ def test_fit_si8_synthetic(torch_cuda):
     fd_cpu = ofit.fitted_densities(th_cpu, psi, *a, rk, piv, rows)
     th_lu = ofit.getbasis_rows(psi, *a, rk, piv, rows, solver="lu")
     spread_fd = ofit.rel(ofit.fitted_densities(th_lu, psi, *a, rk, piv), fd_cpu)
+    spread_th = ofit.rel(th_lu, th_cpu[rows])
     e_fd = ofit.rel(fd, fd_cpu)
     bound = max(FD_TOL, 20 * spread_fd)
     record_parity("fit Si8-like", "fitted densities: CPU Cholesky vs CPU LU", spread_fd)
+    record_parity("fit Si8-like", "theta: CPU Cholesky vs CPU LU", spread_th)
     record_parity("fit Si8-like", "fitted densities vs oracle", e_fd, bound)
     assert e_fd <= bound
     from oracle import ref
 
     if ref.available():
+        # the reference's getbasis_MPI and the numpy oracle make the same
+        # OpenBLAS calls in the same order (their distance measures nothing);
+        # the FP64 uncertainty of theta is the Cholesky-vs-LU distance
         th_ref = ref.getbasis(psi, (s.n,) * 3, (s.length,) * 3, *a, rk, piv)
-        spread = ofit.rel(th_cpu, th_ref)
-        e_th = ofit.rel(th, th_ref)
-        record_parity("fit Si8-like", "theta vs the reference's getbasis_MPI", e_th,
-                      max(1e-10, 20 * spread))
-        assert e_th <= max(1e-10, 20 * spread)
+        e_th = ofit.rel(th[rows], th_ref[rows])
+        bound_th = max(1e-10, 20 * spread_th, 20 * ofit.rel(th_cpu[rows], th_ref[rows]))
+        record_parity("fit Si8-like", "theta vs the reference's getbasis_MPI", e_th, bound_th)
+        assert e_th <= bound_th
         fd_ref = ofit.fitted_densities(th_ref, psi, *a, rk, piv, rows)
         e_ref = ofit.rel(fd, fd_ref)
         record_parity("fit Si8-like", "fitted densities vs the reference's getbasis_MPI", e_ref,
