@@ -749,7 +749,7 @@ def _serve_setup(args, torch, isdf, synth):
     """psi pools per shape (seeds 100, 101, ...) and theta buffers, on the GPU."""
     shapes = [synth.SI8, synth.SI64, synth.SI216]
     pool_seeds = [4, 2, 1]
-    theta_bufs = [16, 4, 2]
+    theta_bufs = [16, 3, 1]
     mix = [0.6, 0.3, 0.1]
     if args.serve_mix != "standard":
         # one shape only (the served form's throughput at that size)
@@ -938,8 +938,9 @@ def main():
     ap.add_argument("--serve-seed", type=int, default=7)
     ap.add_argument("--serve-mix", choices=["standard", "si8", "si64", "si216"], default="standard",
                     help="standard: 60/30/10 Si8/Si64/Si216; else one shape only")
-    ap.add_argument("--hbm-budget-gb", type=float, default=0.0,
-                    help="server workspace budget (0: the library default, -1: all free less 4 GiB)")
+    ap.add_argument("--hbm-budget-gb", type=float, default=-1.0,
+                    help="server workspace budget (0: the library default, half the free memory; "
+                         "-1: all free memory less 4 GiB once the request buffers are allocated)")
     args = ap.parse_args()
     from libisdf_b200 import synth
 
