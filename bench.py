@@ -570,7 +570,9 @@ def run_ours(args, shape):
         roofline = {"kernel": "k_ozaki_gemm (Y = Z L^-T and theta = Y L^-1, INT8 digit pairs)",
                     "bound": "tensor", "achieved": ach, "peak": int8_peak[0],
                     "unit": "TOPS (INT8)", "frac": (ach / int8_peak[0]) if ach else None,
-                    "peak_source": int8_peak[1],
+                    "peak_burst": int8_peak[1],
+                    "frac_of_burst": (ach / int8_peak[1]) if ach else None,
+                    "peak_source": int8_peak[2],
                     "emulated_fp64_tflops": (2.0 * 2 * ng * rk * (rk / 2 + 32) /
                                              (gemm_ms * 1e-3) / 1e12) if gemm_ms > 0 else None,
                     "traffic": None}
@@ -653,8 +655,11 @@ def secondary_si64(torch, isdf, synth, fp64_peak):
 
 
 def _int8_peak_tops(torch):
-    """cuBLASLt INT8 GEMM (torch._int_mm, 8192^3, best of 5): the INT8
-    tensor-core denominator for the mixed form's GEMMs."""
+    """cuBLASLt INT8 GEMM (torch._int_mm, 8192^3): the INT8 tensor-core
+    denominator for the mixed form's GEMMs, measured as a burst (best of 5)
+    and sustained (back to back for ~3 s, under the power cap, the condition
+    the mixed form's products run in inside a solve). Returns (sustained TOPS,
+    burst TOPS, source)."""
     try:
         a = torch.randint(-127, 128, (8192, 8192), dtype=torch.int8, device="cuda")
         b = torch.randint(-127, 128, (8192, 8192), dtype=torch.int8, device="cuda").t()
@@ -669,12 +674,23 @@ def _int8_peak_tops(torch):
             e1.record()
             torch.cuda.synchronize()
             best = min(best, e0.elapsed_time(e1))
+        burst = 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+        n = max(8, int(3.0 / (best * 1e-3)))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            torch._int_mm(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        sustained = n * 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
         del a, b
         torch.cuda.empty_cache()
-        return 2 * 8192 ** 3 / (best * 1e-3) / 1e12, "cuBLASLt INT8 GEMM 8192^3 measured in this run"
+        return sustained, burst, ("cuBLASLt INT8 GEMM 8192^3 measured in this run, back to back "
+                                  f"for ~3 s ({n} GEMMs; the burst best of 5: {burst:.0f} TOPS)")
     except Exception as e:  # noqa: BLE001
         peaks, _ = _measured_peaks()
-        return 2.0 * peaks["bf16_tflops"], f"2 x measured dense BF16 (INT8 GEMM unavailable: {e})"
+        return (2.0 * peaks["bf16_tflops_sustained"], 2.0 * peaks["bf16_tflops"],
+                f"2 x measured dense BF16 (INT8 GEMM unavailable: {e})")
 
 
 
