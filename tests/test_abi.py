@@ -109,3 +109,19 @@ def test_cxx_drop_in_caller_links(tmp_path):
                         "-L", os.path.join(cuda, "lib64"), "-lcudart"],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_request_footprint_counts_check_and_oversampling():
+    """isdf_request_workspace_bytes includes what isdf_workspace_bytes leaves
+    out: the check's buffers (they depend on the grid's shape) and the QRCP
+    oversampling; invalid requests give 0."""
+    dom = isdf.Domain(length=(10.26,) * 3, num_grid=(40, 40, 40))
+    base = isdf.request_workspace_bytes(dom, 32, 16, 16, 16, 16, 320)
+    assert base == isdf.workspace_bytes(64000, 32, 320)
+    assert isdf.request_workspace_bytes(dom, 32, 16, 16, 16, 16, 320, check=True) > base
+    q15 = isdf.request_workspace_bytes(dom, 32, 16, 16, 16, 16, 320, s1="QRCP")
+    q25 = isdf.request_workspace_bytes(dom, 32, 16, 16, 16, 16, 320, s1="QRCP",
+                                       options=isdf.Options(qrcp_oversample=2.5))
+    assert q25 > q15 == isdf.workspace_bytes(64000, 32, 320, selector=isdf.SELECT_QRCP)
+    bad = isdf.Domain(length=(1.0,) * 3, num_grid=(0, 4, 4))
+    assert isdf.request_workspace_bytes(bad, 32, 16, 16, 16, 16, 320) == 0
