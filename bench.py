@@ -772,7 +772,9 @@ def _serve_setup(args, torch, isdf, synth):
         k1 = {"si8": 0, "si64": 1, "si216": 2}[args.serve_mix]
         mix = [1.0 if k == k1 else 0.0 for k in range(3)]
         pool_seeds = [1 if k == k1 else 0 for k in range(3)]
-        theta_bufs = [args.slots if k == k1 else 0 for k in range(3)]
+        # in flight: the slots' requests plus a batch of small ones
+        inflight = args.slots + (args.batch_small if k1 == 0 else 0)
+        theta_bufs = [inflight if k == k1 else 0 for k in range(3)]
     psi = {k: [torch.from_numpy(np.ascontiguousarray(
         synth.shape_orbitals(shapes[k], 100 + j, device="cuda").T)).cuda()
         for j in range(pool_seeds[k])] for k in range(3)}
