@@ -84,9 +84,20 @@ void port_weight(const double* psi, long long ng, int nocc, int nv1, int nc1, in
 // (only the early-return branch draws from it); < 0 keeps the process state.
 // warm != 0: piv holds the previous pivots on entry (used when piv[0] !=
 // piv[1]); *warm_used receives how many of them were kept (-1: cold start).
-int port_kmeans_warm(const double* w, int n, const int* nG, const double* len, int rk,
-                     int max_iter, long long rand_seed, int* piv, int* iters_out, int warm,
-                     int* warm_used) {
+//
+// ranks > 1 restates KMEAN run as that many MPI ranks (utility.cpp:682-700,
+// 813-830, 946-969): rank r owns the points [r n/p + min(r, n%p), +n/p +
+// (r < n%p)) of the n-long index list (zero tail included) and folds its
+// own centroid sums in its point order; the ranks' sums are combined by a
+// binomial tree (at step s = 1, 2, 4, ..., rank q takes in rank q + s: the
+// order of MPICH's binomial reduce, and the only order at 2 ranks); the
+// nearest point of each centroid is each rank's first minimum, then the
+// smallest distance over the ranks with ties to the smaller grid index
+// (MPI_MINLOC). Everything else is the one-rank algorithm.
+int port_kmeans_ranks(const double* w, int n, const int* nG, const double* len, int rk,
+                      int max_iter, long long rand_seed, int* piv, int* iters_out, int warm,
+                      int* warm_used, int ranks) {
+  if (ranks < 1 || ranks > n) return -3;
   if (rand_seed >= 0) std::srand((unsigned)rand_seed);
   const double kmeans_tol = 1e-5, df_tol = 1e-8;
   std::vector<int> prev;
@@ -145,6 +156,9 @@ int port_kmeans_warm(const double* w, int n, const int* nG, const double* len, i
     double d1 = gx[i] - cx[j], d2 = gy[i] - cy[j], d3 = gz[i] - cz[j];
     return d1 * d1 + d2 * d2 + d3 * d3;
   };
+  // rank r's point range
+  std::vector<int> lo(ranks + 1);
+  for (int r = 0; r <= ranks; ++r) lo[r] = r * (n / ranks) + std::min(r, n % ranks);
   std::vector<int> label(n), last(n);
   // Each point's argmin is independent, so the points are split over
   // OpenMP threads; every distance is still evaluated exactly as above.
@@ -171,12 +185,36 @@ int port_kmeans_warm(const double* w, int n, const int* nG, const double* len, i
     std::fill(cx.begin(), cx.end(), 0.0);
     std::fill(cy.begin(), cy.end(), 0.0);
     std::fill(cz.begin(), cz.end(), 0.0);
-    for (int i = 0; i < n; i++) {
-      int t = label[i];
-      cnt[t] += wl[i];
-      cx[t] += wl[i] * gx[i];
-      cy[t] += wl[i] * gy[i];
-      cz[t] += wl[i] * gz[i];
+    if (ranks == 1) {
+      for (int i = 0; i < n; i++) {
+        int t = label[i];
+        cnt[t] += wl[i];
+        cx[t] += wl[i] * gx[i];
+        cy[t] += wl[i] * gy[i];
+        cz[t] += wl[i] * gz[i];
+      }
+    } else {
+      // per-rank sums [cnt | cx | cy | cz], then the binomial combine
+      std::vector<std::vector<double>> part(ranks, std::vector<double>(4 * (size_t)rk, 0.0));
+      for (int r = 0; r < ranks; ++r) {
+        double* q = part[r].data();
+        for (int i = lo[r]; i < lo[r + 1]; i++) {
+          int t = label[i];
+          q[t] += wl[i];
+          q[rk + t] += wl[i] * gx[i];
+          q[2 * rk + t] += wl[i] * gy[i];
+          q[3 * rk + t] += wl[i] * gz[i];
+        }
+      }
+      for (int st = 1; st < ranks; st *= 2)
+        for (int r = 0; r + st < ranks; r += 2 * st)
+          for (size_t e = 0; e < 4 * (size_t)rk; ++e) part[r][e] = part[r][e] + part[r + st][e];
+      for (int t = 0; t < rk; ++t) {
+        cnt[t] = part[0][t];
+        cx[t] = part[0][rk + t];
+        cy[t] = part[0][2 * rk + t];
+        cz[t] = part[0][3 * rk + t];
+      }
     }
     for (int i = 0; i < rk; i++) {
       if (cnt[i] != 0.0) {
@@ -204,20 +242,31 @@ int port_kmeans_warm(const double* w, int n, const int* nG, const double* len, i
     s++;
   }
   *iters_out = s;
-  // Nearest point to each centroid (first minimum over points).
+  // Nearest point to each centroid: each rank's first minimum over its
+  // points, then the smallest distance over the ranks, ties to the smaller
+  // grid index (at one rank: the first minimum over all points).
   std::vector<int> sel(rk);
 #pragma omp parallel for schedule(dynamic, 16)
   for (int j = 0; j < rk; j++) {
-    double best = dist(0, j);
-    int bi = 0;
-    for (int i = 1; i < n; i++) {
-      double d = dist(i, j);
-      if (d < best) {
-        best = d;
-        bi = i;
+    double gbest = 0.0;
+    int gsel = -1;
+    for (int r = 0; r < ranks; ++r) {
+      double best = dist(lo[r], j);
+      int bi = lo[r];
+      for (int i = lo[r] + 1; i < lo[r + 1]; i++) {
+        double d = dist(i, j);
+        if (d < best) {
+          best = d;
+          bi = i;
+        }
+      }
+      const int g = index[bi];
+      if (gsel < 0 || best < gbest || (best == gbest && g < gsel)) {
+        gbest = best;
+        gsel = g;
       }
     }
-    sel[j] = index[bi];
+    sel[j] = gsel;
   }
   std::sort(sel.begin(), sel.end());
   sel.erase(std::unique(sel.begin(), sel.end()), sel.end());
@@ -233,6 +282,13 @@ int port_kmeans_warm(const double* w, int n, const int* nG, const double* len, i
     }
   }
   return rk;
+}
+
+int port_kmeans_warm(const double* w, int n, const int* nG, const double* len, int rk,
+                     int max_iter, long long rand_seed, int* piv, int* iters_out, int warm,
+                     int* warm_used) {
+  return port_kmeans_ranks(w, n, nG, len, rk, max_iter, rand_seed, piv, iters_out, warm,
+                           warm_used, 1);
 }
 
 int port_kmeans(const double* w, int n, const int* nG, const double* len, int rk, int max_iter,

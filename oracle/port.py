@@ -26,6 +26,8 @@ def lib():
         _lib.port_kmeans.restype = I
         _lib.port_kmeans_warm.argtypes = [P, I, P, P, I, I, ctypes.c_longlong, P, P, I, P]
         _lib.port_kmeans_warm.restype = I
+        _lib.port_kmeans_ranks.argtypes = [P, I, P, P, I, I, ctypes.c_longlong, P, P, I, P, I]
+        _lib.port_kmeans_ranks.restype = I
         _lib.port_num_threads.restype = I
     return _lib
 
@@ -71,6 +73,22 @@ def kmeans_warm(w, ng, length, mu, iters, prev_piv, rand_seed=1):
     if rk <= 0:
         raise RuntimeError(f"port_kmeans_warm failed: {rk}")
     return piv, rk, int(it[0]), int(used[0])
+
+
+def kmeans_ranks(w, ng, length, mu, iters, ranks, rand_seed=1):
+    """K-means as `ranks` MPI ranks would run the reference's KMEAN (the point
+    partition, per-rank sums combined in binomial-tree order, MINLOC for the
+    nearest points; oracle/kmeans_port.cpp). Returns (piv, rk_eff, iterations)."""
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    g = np.ascontiguousarray(ng, dtype=np.int32)
+    ln = np.ascontiguousarray(length, dtype=np.float64)
+    piv = np.zeros(w.shape[0], dtype=np.int32)
+    it = np.zeros(1, dtype=np.int32)
+    rk = lib().port_kmeans_ranks(_ptr(w), w.shape[0], _ptr(g), _ptr(ln), mu, iters, rand_seed,
+                                 _ptr(piv), _ptr(it), 0, None, ranks)
+    if rk <= 0:
+        raise RuntimeError(f"port_kmeans_ranks failed: {rk}")
+    return piv, rk, int(it[0])
 
 
 def kmeans_piv(psi, ng, length, nocc, nv1, nc1, nv2, nc2, mu, iters, rand_seed=1):

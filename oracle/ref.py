@@ -15,7 +15,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_ref", "libisdf_ref.so")
+LIB_MP_PATH = os.path.join(_HERE, "_ref", "libisdf_ref_mp.so")
 _lib = None
+_lib_mp = None
 
 
 def available() -> bool:
@@ -177,3 +179,31 @@ def qrcp_sketch(k1: int, k2: int, num_pre: int, seed: int, orth: bool = True):
     f = lib().ref_qrcp_sketch if orth else lib().ref_qrcp_gaussians
     f(k1, k2, num_pre, seed, _ptr(g1), _ptr(g2))
     return g1, g2
+
+
+def available_ranks() -> bool:
+    return os.path.exists(LIB_MP_PATH)
+
+
+def kmeans_ranks(w, ng, length, mu, iters, ranks, rand_seed=1, timeout_s=600.0):
+    """The reference's own KMEAN (src/common/utility.cpp:631-988) run as
+    `ranks` MPI ranks: forked processes over the shared-memory MPI stand-in of
+    oracle/shims_mp (reductions in binomial-tree order). Tolerances of the GPU
+    path (1e-5, 1e-8), piv zeroed first. Returns (piv, rk_eff, iterations)."""
+    global _lib_mp
+    if _lib_mp is None:
+        _lib_mp = ctypes.CDLL(LIB_MP_PATH)
+        P, I = ctypes.c_void_p, ctypes.c_int
+        _lib_mp.ref_kmeans_ranks.argtypes = [I, P, P, P, I, I, I, ctypes.c_uint, P, P, P,
+                                             ctypes.c_double]
+        _lib_mp.ref_kmeans_ranks.restype = I
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    g, ln = _geom(ng, length)
+    piv = np.zeros(w.shape[0], dtype=np.int32)
+    rk = np.zeros(1, dtype=np.int32)
+    it = np.zeros(1, dtype=np.int32)
+    rc = _lib_mp.ref_kmeans_ranks(ranks, _ptr(w), _ptr(g), _ptr(ln), mu, iters, 0, rand_seed,
+                                  _ptr(piv), _ptr(rk), _ptr(it), float(timeout_s))
+    if rc != 0:
+        raise OracleError(f"ref_kmeans_ranks({ranks}) failed: {rc}")
+    return piv, int(rk[0]), int(it[0])
