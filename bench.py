@@ -761,6 +761,70 @@ def run_select(args, shape):
     print(json.dumps(line), flush=True)
 
 
+def run_sharded(args, shape):
+    """--shard: one system split by grid rows over the ranks torchrun starts
+    (the reference's p-rank layout; NCCL between the GPUs, its id handed out
+    over the torch process group). Strong scaling: every step is one solve of
+    the whole system; value = steps / (max over ranks of the timed region)."""
+    import datetime
+
+    import torch
+    import torch.distributed as tdist
+
+    import libisdf_b200 as isdf
+    from libisdf_b200 import synth
+
+    rank, world, local = _rank_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+        dist = tdist
+    psi = _shape_psi(synth, shape, args.config)
+    ng, mu = shape.ng, shape.mu
+    start, cnt = isdf.row_block(ng, world, rank)
+    d_rows = torch.from_numpy(np.ascontiguousarray(psi[start:start + cnt].T)).cuda()
+    del psi
+    layout = isdf.THETA_CYCLIC if args.theta_layout == "cyclic" else isdf.THETA_ROWS
+    width = mu // world + (1 if rank < mu % world else 0)
+    d_theta = (torch.empty((width, ng), dtype=torch.float64, device="cuda")
+               if layout == isdf.THETA_CYCLIC else
+               torch.empty((mu, cnt), dtype=torch.float64, device="cuda"))
+    piv = np.zeros(ng, dtype=np.int32)
+    dom = isdf.Domain(length=(shape.length,) * 3, num_grid=(shape.n,) * 3)
+    comm = (isdf.Comm.nccl_from_torch() if dist else
+            isdf.Comm.nccl(isdf.nccl_unique_id(), 0, 1))
+    stream = torch.cuda.Stream()
+    prec = isdf.PRECISION_MIXED if args.precision == "mixed" else isdf.PRECISION_FP64
+    opts = isdf.Options(stream=stream.cuda_stream, precision=prec, mixed_slices=args.mixed_slices)
+
+    def solve():
+        return isdf.solve_sharded(comm, d_rows, dom, shape.nocc, shape.nstate, shape.nv1,
+                                  shape.nc1, shape.nv2, shape.nc2, mu, d_theta, piv,
+                                  shape.kmeans_iters, layout=layout, options=opts)
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, args.warmup)):
+            solve()
+        main = Timed(torch, solve, stream, args.steps, local, dist)
+    t_ms = main.t_ms
+    if rank == 0:
+        line = {"metric": METRIC, "value": args.steps / (t_ms * 1e-3), "unit": "solves/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(_config(shape, args, main.rep), parallelism=f"shard{world}",
+                               theta_layout=args.theta_layout),
+                "stages_ms": main.stages, "gpu_launches": main.launches,
+                "clocks": main.clocks}
+        print(json.dumps(line), flush=True)
+    comm.close()
+    if dist:
+        tdist.barrier()
+        tdist.destroy_process_group()
+
+
 def _serve_setup(args, torch, isdf, synth):
     """psi pools per shape (seeds 100, 101, ...) and theta buffers, on the GPU."""
     shapes = [synth.SI8, synth.SI64, synth.SI216]
@@ -956,6 +1020,11 @@ def main():
     ap.add_argument("--serve-seed", type=int, default=7)
     ap.add_argument("--serve-mix", choices=["standard", "si8", "si64", "si216"], default="standard",
                     help="standard: 60/30/10 Si8/Si64/Si216; else one shape only")
+    ap.add_argument("--shard", action="store_true",
+                    help="split one system by grid rows over the ranks (strong scaling) "
+                         "instead of one replica per GPU")
+    ap.add_argument("--theta-layout", choices=["rows", "cyclic"], default="rows",
+                    help="--shard: theta as each rank's rows, or the reference's cyclic columns")
     ap.add_argument("--hbm-budget-gb", type=float, default=-1.0,
                     help="server workspace budget (0: the library default, half the free memory; "
                          "-1: all free memory less 4 GiB once the request buffers are allocated)")
@@ -967,6 +1036,8 @@ def main():
         run_reference(args, shape)
     elif args.serve:
         run_serve(args)
+    elif args.shard:
+        run_sharded(args, shape)
     elif args.stage == "select":
         run_select(args, shape)
     else:

@@ -39,6 +39,7 @@ extern "C" {
 #define ISDF_ERR_UNSUPPORTED (-6) /* shape or option outside what is built */
 #define ISDF_ERR_CANCELLED (-7)   /* serving: request cancelled */
 #define ISDF_ERR_BUSY (-8)        /* serving: queue full */
+#define ISDF_ERR_COMM (-9)        /* sharded solve: a collective failed or a rank did not arrive */
 
 #define ISDF_SELECT_KMEANS 0
 #define ISDF_SELECT_QRCP 1
@@ -276,6 +277,88 @@ int isdf_server_cancel(void* server, long long ticket);
 int isdf_server_stats(void* server, isdf_server_stats_t* stats);
 /* Cancels queued requests, waits for running ones, frees the server. */
 int isdf_server_destroy(void* server);
+
+/* ---------------------------------------------------------------- sharded
+ * Grid-row sharding over several GPUs, one rank per GPU: the layout of the
+ * reference's p-rank GPU ISDF() (src/common/isdf.cpp:132-188 ->
+ * src/cuda/isdf-gpu.cpp:9-403). Rank r holds grid rows [start_r, start_r +
+ * count_r) of psi, start_r = r (Ng / p) + min(r, Ng % p) and count_r = Ng / p +
+ * (r < Ng % p) (isdf_row_block), as d_psirow (count_r x nstate, ld =
+ * count_r). The ranks exchange the weights (an all-gather), run the
+ * reference's p-rank KMEAN (each rank owns a block of the filtered point
+ * list, folds its centroid sums in its point order; the partial sums are
+ * combined in binomial-tree order, the order of MPICH's binomial reduce and
+ * the only possible one at two ranks; the nearest point of each centroid is
+ * the smallest distance over the ranks, ties to the smaller grid index, as
+ * MPI_MINLOC), gather the psi rows at the pivots, and fit their own grid
+ * rows (C C^T and its Cholesky factor are computed on every rank). piv (host
+ * int[Ng]) is the same on every rank and equals the reference's p-rank piv bit
+ * for bit (its one-rank piv in all but rare rounding and tie cases); theta's
+ * rows are those of the one-rank solve with the same piv.
+ *
+ * theta layouts:
+ *  ISDF_THETA_ROWS    d_theta = this rank's rows, count_r x mu, ld = count_r:
+ *                     no exchange (the B200 form);
+ *  ISDF_THETA_CYCLIC  the reference's d_thetaCol: Ng x w_r, ld = Ng, holding
+ *                     theta's columns r, r + p, r + 2p, ... (w_r = mu / p +
+ *                     (r < mu % p)), the layout GPU_AlltoallBackward produces
+ *                     (src/common/utility.cpp:444-526); one all-to-all of theta.
+ * Columns past the effective mu are zero in both. */
+#define ISDF_THETA_ROWS 0
+#define ISDF_THETA_CYCLIC 1
+
+typedef struct isdf_comm isdf_comm_t;
+
+/* Transport callbacks for callers with their own collectives (for instance a
+ * CUDA-aware MPI: MPI_Allgatherv / MPI_Alltoallv on device buffers, after
+ * synchronising `stream`). Sizes and displacements are in bytes, one entry per
+ * rank. Return 0 on success. The operation must be complete, or ordered on
+ * `stream`, when the callback returns. */
+typedef struct isdf_comm_ops_t {
+  int (*allgatherv)(void* ctx, const void* d_send, size_t send_bytes, void* d_recv,
+                    const size_t* recv_bytes, const size_t* recv_displs, void* stream);
+  int (*alltoallv)(void* ctx, const void* d_send, const size_t* send_bytes,
+                   const size_t* send_displs, void* d_recv, const size_t* recv_bytes,
+                   const size_t* recv_displs, void* stream);
+} isdf_comm_ops_t;
+
+/* NCCL transport (NCCL is opened at run time: libnccl.so.2). Rank 0 makes
+ * the id, the caller hands it to every rank (any out-of-band channel), and
+ * each rank, with its own GPU current, creates its communicator. */
+int isdf_comm_nccl_unique_id(unsigned char id[128]);
+int isdf_comm_create_nccl(const unsigned char id[128], int rank, int size, isdf_comm_t** comm);
+/* `size` ranks inside this process (one host thread per rank calls the
+ * sharded functions with its comms[r]); devices[r]: rank r's GPU (NULL: all on
+ * the current device). A rank that does not reach a collective within
+ * timeout_s seconds fails it with ISDF_ERR_COMM, and the group with it. */
+int isdf_comm_create_local(int size, const int* devices, double timeout_s, isdf_comm_t** comms);
+int isdf_comm_create_callbacks(const isdf_comm_ops_t* ops, void* ctx, int rank, int size,
+                               isdf_comm_t** comm);
+int isdf_comm_rank(const isdf_comm_t* comm, int* rank, int* size);
+/* Fails this rank's outstanding and later collectives (NCCL: ncclCommAbort;
+ * local group: the whole group). For failure handling. */
+int isdf_comm_abort(isdf_comm_t* comm);
+/* Frees the communicator and the rank's workspace. */
+int isdf_comm_destroy(isdf_comm_t* comm);
+/* The reference's row block of rank `rank`: start and count of n items. */
+int isdf_row_block(long long n, int size, int rank, long long* start, long long* count);
+
+/* The sharded ISDF solve (K-means selector, no check): every rank calls it
+ * with the same arguments except d_psirow and d_theta. opt->stream: the
+ * rank's stream (NULL: the communicator's own). opt->rand_seed (only the
+ * npt < mu branch draws): each rank draws from its own copy of libc's rand()
+ * sequence for that seed, a negative seed standing for 1, the state every
+ * rank process of the reference starts from. Synchronous. */
+int isdf_solve_sharded(isdf_comm_t* comm, const isdf_domain_t* dom, const double* d_psirow,
+                       int nocc, int nstate, int nv1, int nc1, int nv2, int nc2, int mu_points,
+                       double* d_theta, int theta_layout, int* piv, int kmeans_max_iter,
+                       const isdf_options_t* opt, isdf_report_t* rep);
+
+/* The p-rank K-means selection alone, from the full weight vector on every
+ * rank (d_w: device double[Ng]); outputs as isdf_kmeans_select. */
+int isdf_kmeans_select_sharded(isdf_comm_t* comm, const isdf_domain_t* dom, const double* d_w,
+                               int mu, int max_iter, long long rand_seed, int* piv, int* rk_eff,
+                               int* iters, int* npt);
 
 /* Message for the last error on this thread ("" if none). */
 const char* isdf_last_error(void);

@@ -36,11 +36,14 @@ ISDF_ERR_TIMEOUT = -5
 ISDF_ERR_UNSUPPORTED = -6
 ISDF_ERR_CANCELLED = -7
 ISDF_ERR_BUSY = -8
+ISDF_ERR_COMM = -9
 
 SELECT_KMEANS = 0
 SELECT_QRCP = 1
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+THETA_ROWS = 0
+THETA_CYCLIC = 1
 
 
 class IsdfError(RuntimeError):
@@ -213,6 +216,26 @@ def lib() -> ctypes.CDLL:
                                                    I, ctypes.POINTER(_Options)]
         L.isdf_request_workspace_bytes.restype = ctypes.c_size_t
         L.isdf_default_options.argtypes = [ctypes.POINTER(_Options)]
+        L.isdf_comm_nccl_unique_id.argtypes = [P]
+        L.isdf_comm_nccl_unique_id.restype = I
+        L.isdf_comm_create_nccl.argtypes = [P, I, I, ctypes.POINTER(P)]
+        L.isdf_comm_create_nccl.restype = I
+        L.isdf_comm_create_local.argtypes = [I, P, ctypes.c_double, P]
+        L.isdf_comm_create_local.restype = I
+        L.isdf_comm_rank.argtypes = [P, ctypes.POINTER(I), ctypes.POINTER(I)]
+        L.isdf_comm_rank.restype = I
+        L.isdf_comm_abort.argtypes = [P]
+        L.isdf_comm_abort.restype = I
+        L.isdf_comm_destroy.argtypes = [P]
+        L.isdf_comm_destroy.restype = I
+        L.isdf_row_block.argtypes = [LL, I, I, ctypes.POINTER(LL), ctypes.POINTER(LL)]
+        L.isdf_row_block.restype = I
+        L.isdf_solve_sharded.argtypes = [P, ctypes.POINTER(_Domain), P, I, I, I, I, I, I, I, P, I,
+                                         P, I, ctypes.POINTER(_Options), ctypes.POINTER(_Report)]
+        L.isdf_solve_sharded.restype = I
+        L.isdf_kmeans_select_sharded.argtypes = [P, ctypes.POINTER(_Domain), P, I, I, LL, P, P,
+                                                 P, P]
+        L.isdf_kmeans_select_sharded.restype = I
         _lib = L
     return _lib
 
@@ -457,3 +480,116 @@ def request_workspace_bytes(domain: Domain, nstate: int, nv1: int, nc1: int, nv2
     return int(lib().isdf_request_workspace_bytes(ctypes.byref(d), nstate, nv1, nc1, nv2, nc2,
                                                   mu_points, sel, int(bool(check)),
                                                   ctypes.byref(o)))
+
+
+# ------------------------------------------------------------------ sharded
+def row_block(n: int, size: int, rank: int):
+    """(start, count) of rank's block of n grid rows: the reference's rule
+    (src/common/isdf.cpp:137-141), the first n % size ranks one row more."""
+    a, b = ctypes.c_longlong(), ctypes.c_longlong()
+    _check(lib().isdf_row_block(n, size, rank, ctypes.byref(a), ctypes.byref(b)))
+    return a.value, b.value
+
+
+def nccl_unique_id() -> bytes:
+    """A new NCCL unique id (128 bytes) for Comm.nccl (NCCL opened at run time)."""
+    buf = ctypes.create_string_buffer(128)
+    _check(lib().isdf_comm_nccl_unique_id(buf))
+    return buf.raw
+
+
+def share_nccl_unique_id(group=None) -> bytes:
+    """A new NCCL unique id made on the group's first rank and handed to every
+    rank of a torch.distributed group (broadcast_object_list: any backend,
+    gloo included)."""
+    import torch.distributed as dist
+    box = [nccl_unique_id() if dist.get_rank(group) == 0 else None]
+    src = 0 if group is None else dist.get_global_rank(group, 0)
+    dist.broadcast_object_list(box, src=src, group=group)
+    return box[0]
+
+
+class Comm:
+    """A rank's communicator for the sharded solve (isdf_comm_t)."""
+
+    def __init__(self, handle: int):
+        self._h = ctypes.c_void_p(handle)
+        r, n = ctypes.c_int(), ctypes.c_int()
+        _check(lib().isdf_comm_rank(self._h, ctypes.byref(r), ctypes.byref(n)))
+        self.rank, self.size = r.value, n.value
+
+    @classmethod
+    def nccl(cls, unique_id: bytes, rank: int, size: int) -> "Comm":
+        """NCCL transport; the current CUDA device is this rank's GPU."""
+        if len(unique_id) != 128:
+            raise ValueError("an NCCL unique id has 128 bytes")
+        h = ctypes.c_void_p()
+        _check(lib().isdf_comm_create_nccl(ctypes.create_string_buffer(unique_id, 128), rank,
+                                           size, ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def nccl_from_torch(cls, group=None) -> "Comm":
+        """NCCL transport for the ranks of a torch.distributed group (any
+        backend carries the unique id, see share_nccl_unique_id); the current
+        CUDA device is this rank's GPU."""
+        import torch.distributed as dist
+        uid = share_nccl_unique_id(group)
+        return cls.nccl(uid, dist.get_rank(group), dist.get_world_size(group))
+
+    @classmethod
+    def local_group(cls, size: int, devices=None, timeout_s: float = 60.0) -> list:
+        """`size` ranks inside this process (one host thread per rank calls the
+        sharded functions); devices: rank r's GPU (None: all on the current
+        device)."""
+        hs = (ctypes.c_void_p * size)()
+        dv = (ctypes.c_int * size)(*devices) if devices is not None else None
+        _check(lib().isdf_comm_create_local(size, dv, float(timeout_s), hs))
+        return [cls(hs[r]) for r in range(size)]
+
+    def abort(self):
+        _check(lib().isdf_comm_abort(self._h))
+
+    def close(self):
+        if self._h:
+            lib().isdf_comm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_sharded(comm: Comm, d_psirow, domain: Domain, nocc: int, nstate: int, nv1: int,
+                  nc1: int, nv2: int, nc2: int, mu_points: int, d_theta, piv: np.ndarray,
+                  KmeansMaxIter_ISDF: int, layout: int = THETA_ROWS,
+                  options: Options | None = None) -> Report:
+    """The reference's p-rank GPU ISDF() for this rank (isdf_solve_sharded):
+    d_psirow holds the rank's grid rows (row_block), d_theta receives its
+    theta rows (THETA_ROWS: count x mu) or the reference's column-cyclic block
+    (THETA_CYCLIC: Ng x (mu / p + (rank < mu % p)))."""
+    piv = _host_int32(piv, domain.NumGridTotal())
+    d = domain._c()
+    o = (options or Options())._c()
+    r = _Report()
+    _check(lib().isdf_solve_sharded(comm._h, ctypes.byref(d), _dptr(d_psirow), nocc, nstate, nv1,
+                                    nc1, nv2, nc2, mu_points, _dptr(d_theta), layout,
+                                    piv.ctypes.data, KmeansMaxIter_ISDF, ctypes.byref(o),
+                                    ctypes.byref(r)))
+    return _report(r)
+
+
+def kmeans_select_sharded(comm: Comm, domain: Domain, d_w, mu: int, max_iter: int,
+                          rand_seed: int = -1):
+    """This rank's part of the p-rank K-means selection from the full weight
+    vector; returns (piv int32[Ng], rk_eff, iterations, npt), the same on every rank."""
+    n = domain.NumGridTotal()
+    piv = np.zeros(n, dtype=np.int32)
+    out = (ctypes.c_int * 3)()
+    d = domain._c()
+    _check(lib().isdf_kmeans_select_sharded(comm._h, ctypes.byref(d), _dptr(d_w), mu, max_iter,
+                                            rand_seed, piv.ctypes.data, ctypes.addressof(out),
+                                            ctypes.addressof(out) + 4, ctypes.addressof(out) + 8))
+    return piv, out[0], out[1], out[2]

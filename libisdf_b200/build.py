@@ -69,7 +69,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         msg = "\n".join(f"{s}:\n{o}" for s, o in failed)
         raise RuntimeError(f"nvcc failed:\n{msg}")
     tmp = LIB + ".tmp"
-    cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcufft", "-lcublas"]
+    cmd = [NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcufft", "-lcublas", "-ldl"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     return LIB

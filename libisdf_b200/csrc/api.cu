@@ -616,6 +616,7 @@ const char* isdf_status_string(int code) {
     case ISDF_ERR_UNSUPPORTED: return "unsupported shape or option";
     case ISDF_ERR_CANCELLED: return "cancelled";
     case ISDF_ERR_BUSY: return "queue full";
+    case ISDF_ERR_COMM: return "collective failed";
     default: return "unknown status";
   }
 }

@@ -519,10 +519,14 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
   res->launches = 1 + (same_ ? 1 : 2) + 2 + (nblk_ + 2 * (nblk_ - 1) + 1) + 4 * nblk_ +
                   (readback_mailbox() ? 2 : 0);
 
-  ISDF_CUDA(cudaMemcpyAsync(b.piv, args.piv, sizeof(int) * rk, cudaMemcpyHostToDevice, s));
   ISDF_CUDA(cudaMemsetAsync(b.info, 0, 2 * sizeof(int), s));
-  k_gather_psimu<<<grid_for((long long)args.nstate * rk, 256), 256, 0, s>>>(
-      args.d_psi, ng, args.nstate, b.piv, rk, b.Bm);
+  if (args.d_psimu) {
+    b.Bm = const_cast<double*>(args.d_psimu);
+  } else {
+    ISDF_CUDA(cudaMemcpyAsync(b.piv, args.piv, sizeof(int) * rk, cudaMemcpyHostToDevice, s));
+    k_gather_psimu<<<grid_for((long long)args.nstate * rk, 256), 256, 0, s>>>(
+        args.d_psi, ng, args.nstate, b.piv, rk, b.Bm);
+  }
 
   // Z C^T into theta
   const int lo1 = args.nocc - args.nv1, K1 = args.nv1 + args.nc1;
@@ -555,7 +559,20 @@ int fit_fp64(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* res, 
 
   // C C^T, regularisation, Cholesky
   ISDF_CUDA(mark(1));
-  k_gather_cct<<<grid_for((long long)rk * rk, 256), 256, 0, s>>>(args.d_theta, ng, b.piv, rk, b.P);
+  if (args.d_psimu) {
+    // the Z C^T GEMM on the pivot rows (C C^T is symmetric element for element:
+    // the product of rows j and nu sums the same terms in the same order)
+    dim3 cg((unsigned)((rk + CoreZ::BN - 1) / CoreZ::BN), (unsigned)((rk + CoreZ::BM - 1) / CoreZ::BM));
+    if (same) {
+      k_gemm_z<0, 1><<<cg, 256, zs, s>>>(rk, rk, K1, B1, rk, B1, rk, b.P, rk);
+    } else {
+      k_gemm_z<1, 1><<<cg, 256, zs, s>>>(rk, rk, K1, B1, rk, B1, rk, b.P, rk);
+      k_gemm_z<2, 1><<<cg, 256, zs, s>>>(rk, rk, K2, B2, rk, B2, rk, b.P, rk);
+    }
+  } else {
+    k_gather_cct<<<grid_for((long long)rk * rk, 256), 256, 0, s>>>(args.d_theta, ng, b.piv, rk,
+                                                                  b.P);
+  }
   k_regularise<<<1, 256, 0, s>>>(b.P, rk, b.eps);
   ISDF_TRY(cholesky(b, rk, s));
   ISDF_CUDA(mark(2));
@@ -821,11 +838,15 @@ int fit_mixed_s(const FitArgs& args, Arena& arena, cudaStream_t s, FitResult* re
   ISDF_TRY(ev.create());
   const int mp = round_up(ng, ozaki::BM);
   const int np = round_up(rk, 128);
-  ISDF_CUDA(cudaMemcpyAsync(b.piv, args.piv, sizeof(int) * rk, cudaMemcpyHostToDevice, s));
   ISDF_CUDA(cudaMemsetAsync(b.info, 0, 2 * sizeof(int), s));
   ISDF_CUDA(cudaMemsetAsync(mb.err, 0, sizeof(int), s));
-  k_gather_psimu<<<grid_for((long long)args.nstate * rk, 256), 256, 0, s>>>(
-      args.d_psi, ng, args.nstate, b.piv, rk, b.Bm);
+  if (args.d_psimu) {
+    b.Bm = const_cast<double*>(args.d_psimu);
+  } else {
+    ISDF_CUDA(cudaMemcpyAsync(b.piv, args.piv, sizeof(int) * rk, cudaMemcpyHostToDevice, s));
+    k_gather_psimu<<<grid_for((long long)args.nstate * rk, 256), 256, 0, s>>>(
+        args.d_psi, ng, args.nstate, b.piv, rk, b.Bm);
+  }
   ISDF_CUDA(cudaEventRecord(ev.e[0], s));
 
   // Z C^T = (psi_S1 psi_S1(mu)^T) o (psi_S2 psi_S2(mu)^T)

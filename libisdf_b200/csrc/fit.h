@@ -15,6 +15,11 @@ struct FitArgs {
   int rk;
   const int* piv;   // host, first rk entries used
   double* d_theta;  // Ng x rk, ld = Ng
+  // Sharded fit (d_psi holds this rank's grid rows): psi at the pivots,
+  // gathered over the ranks, depth-major (B(k, j) = d_psimu[k*rk + j]); C C^T
+  // is then formed from it (every element the same product and order of
+  // summation as the pivot rows of Z C^T), not gathered from this rank's rows.
+  const double* d_psimu = nullptr;
 };
 
 struct FitResult {

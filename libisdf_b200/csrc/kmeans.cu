@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "arena.h"
+#include "comm.h"
 #include "common.cuh"
 #include "solve.h"
 #include "kmeans.h"
@@ -257,21 +258,30 @@ struct CellGrid {
 // zero-tail points p >= npt (copies of grid point 0) follow the bricks one
 // per thread. Linear mode: thread t takes point t. Either way every point is
 // assigned once and the result does not depend on the map.
+// A rank of a sharded selection assigns only its points [p_lo, p_hi): its
+// kept points lie in a z range of bricks (launched from brick thread t0 on),
+// its zero-tail points follow them.
 struct AssignMap {
   int brick;  // 0: linear
   int nx, ny, nz;
   int nbx, nby;    // bricks along x and y
-  long long nbt;   // brick threads: bricks x 32
+  long long nbt;   // brick threads launched: bricks x 32
+  long long t0;    // first brick thread
   int npt, n;
+  int p_lo, p_hi;  // the points this launch assigns
   const int* g2p;  // grid index -> kept-point index (or -1); nullptr: identity
 };
 
 __device__ __forceinline__ int assign_point(long long t, const AssignMap& am) {
-  if (!am.brick) return (int)t;
-  if (t >= am.nbt) {
-    const long long p = am.npt + (t - am.nbt);
-    return p < am.n ? (int)p : -1;
+  if (!am.brick) {
+    const long long p = am.p_lo + t;
+    return p < am.p_hi ? (int)p : -1;
   }
+  if (t >= am.nbt) {
+    const long long p = (long long)max(am.npt, am.p_lo) + (t - am.nbt);
+    return p < am.p_hi ? (int)p : -1;
+  }
+  t += am.t0;
   const long long b = t >> 5;
   const int l = (int)(t & 31);
   const int bx = (int)(b % am.nbx);
@@ -280,7 +290,8 @@ __device__ __forceinline__ int assign_point(long long t, const AssignMap& am) {
   const int ix = bx * 4 + (l & 3), iy = by * 4 + ((l >> 2) & 3), iz = bz * 2 + (l >> 4);
   if (ix >= am.nx || iy >= am.ny || iz >= am.nz) return -1;
   const int g = ix + am.nx * (iy + am.ny * iz);
-  return am.g2p ? am.g2p[g] : g;
+  const int p = am.g2p ? am.g2p[g] : g;
+  return (p >= am.p_lo && p < am.p_hi) ? p : -1;
 }
 
 // Inverse of the kept-point list: g2p[pidx[p]] = p for p < npt (the rest -1).
@@ -568,9 +579,10 @@ __global__ void k_iter_begin(KmState* st, double max_f, int max_iter) {
   st->maxshift_bits = 0;
 }
 
-__global__ void k_iter_end(KmState* st) {
+// set_flag = 0 in a sharded selection, whose flag is the ranks' total (k_shard_begin).
+__global__ void k_iter_end(KmState* st, int set_flag) {
   if (st->done) return;
-  st->flag = st->changed;
+  if (set_flag) st->flag = st->changed;
   st->s += 1;
 }
 
@@ -760,6 +772,9 @@ __device__ __forceinline__ void seg_load(const double4* __restrict__ v, int q, i
   }
 }
 
+// n, npt: the points folded and how many of them are kept points (the rest
+// is zero tail); flag_empty: record an empty cluster in st (off when the sums
+// are one rank's partial sums).
 __global__ void __launch_bounds__(256) k_segsum(const double4* __restrict__ sorted,
                                                 const int* __restrict__ start,
                                                 const int* __restrict__ members,
@@ -767,14 +782,14 @@ __global__ void __launch_bounds__(256) k_segsum(const double4* __restrict__ sort
                                                 const double* __restrict__ py,
                                                 const double* __restrict__ pz,
                                                 const double* __restrict__ pw,
-                                                const int* __restrict__ label, int n,
-                                                KmState* st, double4* __restrict__ sums) {
+                                                const int* __restrict__ label, int n, int npt,
+                                                int flag_empty, KmState* st,
+                                                double4* __restrict__ sums) {
   if (st->done) return;
   const int rk = st->rk;
   const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (c >= rk) return;
-  const int npt = st->npt;
   const double4* v = sorted + start[c];
   int m = members[c];
   long long tail = 0;
@@ -822,7 +837,7 @@ __global__ void __launch_bounds__(256) k_segsum(const double4* __restrict__ sort
       az = repeat_add(az, rmul(w0, pz[npt]), tail);
     }
     sums[c] = make_double4(ax, ay, az, aw);
-    if (aw == 0.0) st->any_empty = 1;
+    if (flag_empty && aw == 0.0) st->any_empty = 1;
   }
 }
 
@@ -975,6 +990,104 @@ __global__ void k_final_reduce(const double* __restrict__ part_d, const int* __r
   sel[j] = pidx[bi];
 }
 
+// ---------------------------------------------------------------- sharded
+// A rank's record per Lloyd iteration: entry 0 carries the labels its last
+// assignment changed (.x), entries 1..rk its partial centroid sums.
+__global__ void k_shard_header(const KmState* st, double4* __restrict__ send) {
+  send[0] = make_double4((double)st->changed, 0.0, 0.0, 0.0);
+}
+
+// The loop test of utility.cpp:812 on the ranks' total of changed labels
+// (the reference's MPI_Reduce + MPI_Bcast of flag, utility.cpp:908-917),
+// then the per-iteration resets of k_iter_begin.
+__global__ void k_shard_begin(KmState* st, const double4* __restrict__ recv, int ranks, int stride,
+                              double max_f, int max_iter) {
+  if (st->done) return;
+  if (st->s > 0) {
+    long long f = 0;
+    for (int q = 0; q < ranks; ++q) f += (long long)recv[(size_t)q * stride].x;
+    st->flag = (int)f;
+  }
+  if (!((double)st->flag > max_f && st->s < max_iter)) {
+    st->done = 1;
+    return;
+  }
+  st->changed = 0;
+  st->any_empty = 0;
+  st->reset_bounds = 0;
+  st->maxshift_bits = 0;
+}
+
+__device__ __forceinline__ double4 add4(const double4& a, const double4& b) {
+  return make_double4(radd(a.x, b.x), radd(a.y, b.y), radd(a.z, b.z), radd(a.w, b.w));
+}
+
+// The ranks' partial sums combined in binomial-tree order (at step s = 1, 2,
+// 4, ..., rank q takes in rank q + s: the reduce of utility.cpp:825-826 as
+// MPICH's binomial algorithm runs it), evaluated rank by rank with a stack of
+// completed subtrees: (r0 + r1) + (r2 + r3) for 4 ranks, (r0 + r1) + r2 for 3.
+__global__ void k_shard_sums(KmState* st, const double4* __restrict__ recv, int ranks, int stride,
+                             double4* __restrict__ sums) {
+  if (st->done) return;
+  const int rk = st->rk;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= rk) return;
+  double4 val[8];
+  int lev[8];
+  int top = 0;
+  for (int q = 0; q < ranks; ++q) {
+    double4 v = recv[(size_t)q * stride + 1 + c];
+    int l = 0;
+    while (top > 0 && lev[top - 1] == l) {
+      v = add4(val[top - 1], v);
+      --top;
+      ++l;
+    }
+    val[top] = v;
+    lev[top] = l;
+    ++top;
+  }
+  double4 acc = val[top - 1];
+  for (int i = top - 2; i >= 0; --i) acc = add4(val[i], acc);
+  sums[c] = acc;
+  if (acc.w == 0.0) st->any_empty = 1;
+}
+
+// One rank's nearest point per centroid: the first minimum over its points
+// (findMin, utility.cpp:926-945), as (distance, grid index).
+__global__ void k_final_local(const double* __restrict__ part_d, const int* __restrict__ part_i,
+                              int nchunks, const KmState* st, const int* __restrict__ pidx,
+                              double2* __restrict__ out) {
+  const int rk = st->rk;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= rk) return;
+  double best = __longlong_as_double(0x7ff0000000000000LL);
+  int bi = 0;
+  for (int c = 0; c < nchunks; ++c) {
+    double d = part_d[(size_t)c * rk + j];
+    if (d < best) {
+      best = d;
+      bi = part_i[(size_t)c * rk + j];
+    }
+  }
+  out[j] = make_double2(best, (double)pidx[bi]);
+}
+
+// MPI_MINLOC over the ranks (utility.cpp:946-969): the smallest distance,
+// ties to the smaller grid index.
+__global__ void k_minloc(const double2* __restrict__ recv, int ranks, int stride,
+                         const KmState* st, int* __restrict__ sel) {
+  const int rk = st->rk;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= rk) return;
+  double2 best = recv[j];
+  for (int q = 1; q < ranks; ++q) {
+    const double2 v = recv[(size_t)q * stride + j];
+    if (v.x < best.x || (v.x == best.x && v.y < best.y)) best = v;
+  }
+  sel[j] = (int)best.y;
+}
+
 // Dynamic shared memory above 48 KB needs an opt-in per kernel and device.
 int set_kmeans_smem_attrs() {
   std::lock_guard<std::mutex> attr_lock(attr_mutex());
@@ -1052,12 +1165,37 @@ KmBuffers carve(Arena& a, int n, int mu) {
   return b;
 }
 
+// Exchange buffers of a sharded selection.
+struct ShardBuffers {
+  double4* send;  // (mu + 1): changed count, partial sums
+  double4* recv;  // ranks x (mu + 1)
+  double2* fsend;  // mu: nearest point per centroid
+  double2* frecv;  // ranks x mu
+};
+
+ShardBuffers carve_shard(Arena& a, int mu, int ranks) {
+  ShardBuffers b;
+  b.send = a.take<double4>((size_t)mu + 1);
+  b.recv = a.take<double4>((size_t)ranks * (mu + 1));
+  b.fsend = a.take<double2>((size_t)mu);
+  b.frecv = a.take<double2>((size_t)ranks * mu);
+  return b;
+}
+
 }  // namespace
 
 size_t kmeans_workspace_bytes(long long ng, int mu) {
   Arena a;
   a.counting = true;
   carve(a, (int)ng, mu);
+  return a.off;
+}
+
+size_t kmeans_shard_workspace_bytes(long long ng, int mu, int ranks) {
+  Arena a;
+  a.counting = true;
+  carve(a, (int)ng, mu);
+  carve_shard(a, mu, ranks);
   return a.off;
 }
 
@@ -1073,26 +1211,59 @@ int kmeans_weight(const double* d_psi, long long ng, int nocc, int nv1, int nc1,
 }
 
 // libstdc++'s std::random_shuffle(first, last) loop, driven by std::rand(),
-// which the reference calls on its npt < mu branch (utility.cpp:679).
-static void shuffle_like_libstdcxx(int* first, int* last) {
+// which the reference calls on its npt < mu branch (utility.cpp:679); draw()
+// stands in for std::rand().
+template <class Draw>
+static void shuffle_like_libstdcxx(int* first, int* last, Draw draw) {
   if (first == last) return;
   for (int* i = first + 1; i != last; ++i) {
-    int* j = first + std::rand() % ((i - first) + 1);
+    int* j = first + draw() % ((i - first) + 1);
     if (i != j) std::swap(*i, *j);
   }
 }
+static void shuffle_like_libstdcxx(int* first, int* last) {
+  shuffle_like_libstdcxx(first, last, [] { return std::rand(); });
+}
 
-int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, KmeansResult* res) {
+// The sequence std::rand() gives after std::srand(seed), from glibc's own
+// generator on a private state (initstate_r / random_r, the generator behind
+// rand()), so that ranks sharing one process do not share their draws.
+struct SeededRand {
+  random_data data;
+  char state[128];
+  explicit SeededRand(unsigned seed) {
+    std::memset(&data, 0, sizeof(data));
+    std::memset(state, 0, sizeof(state));
+    initstate_r(seed, state, sizeof(state), &data);
+  }
+  int operator()() {
+    int32_t r = 0;
+    random_r(&data, &r);
+    return (int)r;
+  }
+};
+
+int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, KmeansResult* res,
+                  Transport* shard) {
   const int n = (int)args.ng;
   const int mu = args.mu;
   if (n <= 0 || mu <= 0 || mu > kKmeansMaxMu) return record_error(ISDF_ERR_ARG, "kmeans: bad n/mu");
   if (args.ng > 0x7fffffffLL) return record_error(ISDF_ERR_UNSUPPORTED, "kmeans: Ng >= 2^31");
+  const int ranks = shard ? shard->size : 1;
+  if (ranks > kKmeansMaxRanks || ranks > n)
+    return record_error(ISDF_ERR_UNSUPPORTED, "kmeans: more ranks than supported or points");
   KmBuffers b = carve(arena, n, mu);
+  ShardBuffers sb{};
+  if (shard) sb = carve_shard(arena, mu, ranks);
   if (arena.overflowed()) return record_error(ISDF_ERR_NOMEM, "kmeans: workspace too small");
+  // this rank's points of the n-long list (utility.cpp:682-689); all of them at one rank
+  const int lo = shard ? (int)block_start(n, ranks, shard->rank) : 0;
+  const int cnt = shard ? (int)block_count(n, ranks, shard->rank) : n;
   const int ntiles = (n + kTile - 1) / kTile;
   const int nfilter = (n + 1023) / 1024;
   const int nchunks = (n + kFinalChunk - 1) / kFinalChunk;
-  if (args.rand_seed >= 0) std::srand((unsigned)args.rand_seed);
+  // a rank of a sharded selection draws from its own generator (below)
+  if (args.rand_seed >= 0 && !shard) std::srand((unsigned)args.rand_seed);
   // warm start: the caller's previous pivots, read before piv is rewritten
   std::vector<int> prev;
   if (args.warm && n > 1 && args.piv[0] != args.piv[1]) {
@@ -1130,7 +1301,14 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
         k1++;
       }
     }
-    shuffle_like_libstdcxx(args.piv + npt, args.piv + n);
+    if (shard) {
+      // every rank process of the reference starts from libc's initial
+      // state (seed 1) unless the caller seeds it
+      SeededRand draw(args.rand_seed >= 0 ? (unsigned)args.rand_seed : 1u);
+      shuffle_like_libstdcxx(args.piv + npt, args.piv + n, [&] { return draw(); });
+    } else {
+      shuffle_like_libstdcxx(args.piv + npt, args.piv + n);
+    }
     res->rk_eff = mu;
     res->iters = -1;
     res->launches = 4 + (readback_mailbox() ? 2 : 0);
@@ -1203,8 +1381,11 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
   am.nbx = (am.nx + 3) / 4;
   am.nby = (am.ny + 3) / 4;
   am.nbt = (long long)am.nbx * am.nby * ((am.nz + 1) / 2) * 32;
+  am.t0 = 0;
   am.npt = npt;
   am.n = n;
+  am.p_lo = lo;
+  am.p_hi = lo + cnt;
   am.brick = ((long long)am.nx * am.ny * am.nz == n && am.nbt + n < 0x7fffffffLL);
   am.g2p = nullptr;
   if (am.brick && npt < n) {
@@ -1212,8 +1393,25 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     k_grid_to_point<<<grid_for(npt, 256), 256, 0, stream>>>(b.pidx, npt, b.g2p);
     am.g2p = b.g2p;
   }
-  const unsigned pgrid = am.brick ? grid_for(am.nbt + (n - npt), kAssignThreads)
-                                  : grid_for(n, kAssignThreads);
+  const int kept_hi = std::min(lo + cnt, npt);  // this rank's kept points: [lo, kept_hi)
+  const int tail_loc = std::max(0, lo + cnt - std::max(npt, lo));
+  if (am.brick && shard) {
+    // the bricks of the z planes that hold this rank's kept points
+    if (lo < kept_hi) {
+      int ends[2];
+      ISDF_TRY(read_back(&ends[0], b.pidx + lo, sizeof(int), stream));
+      ISDF_TRY(read_back(&ends[1], b.pidx + kept_hi - 1, sizeof(int), stream));
+      const long long plane = (long long)am.nx * am.ny;
+      const long long bz0 = ends[0] / plane / 2, bz1 = ends[1] / plane / 2;
+      const long long per_bz = (long long)am.nbx * am.nby * 32;
+      am.t0 = bz0 * per_bz;
+      am.nbt = (bz1 - bz0 + 1) * per_bz;
+    } else {
+      am.nbt = 0;
+    }
+  }
+  const unsigned pgrid = am.brick ? grid_for(am.nbt + tail_loc, kAssignThreads)
+                                  : grid_for(cnt, kAssignThreads);
   k_point_cells<<<grid_for(n, 256), 256, 0, stream>>>(b.px, b.py, b.pz, n, cg, b.pcell, b.pd12);
   k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
                                                 b.cell_of);
@@ -1244,7 +1442,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
       k_scatter<<<ntiles, 128, scatter_smem, stream>>>(b.label, n, b.st, b.hist, b.start, b.px,
                                                        b.py, b.pz, b.pw, b.sorted);
       k_segsum<<<grid_for(mu, 8), 256, 0, stream>>>(b.sorted, b.start, b.members, b.px, b.py,
-                                                    b.pz, b.pw, b.label, n, b.st, b.sums);
+                                                    b.pz, b.pw, b.label, n, npt, 1, b.st, b.sums);
       k_centroids<<<1, 1024, cmax_smem, stream>>>(b.sums, b.st, b.cen, b.shift, b.cell_of, cg,
                                                   b.nbshift);
       k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
@@ -1253,11 +1451,52 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
                                                           b.cell_start, b.cell_cen, cg, am, b.st,
                                                           b.label, 1, b.bnd, b.shift, b.nbshift,
                                                           b.pcell, b.pd12);
-      k_iter_end<<<1, 1, 0, stream>>>(b.st);
+      k_iter_end<<<1, 1, 0, stream>>>(b.st, 1);
     }
   };
+  // Sharded: the rank folds its own points [lo, lo + cnt) (utility.cpp:813-822),
+  // the ranks exchange their partial sums and changed-label counts (one
+  // all-gather per iteration, utility.cpp:825-826,908-917), and every rank
+  // combines them in the same order, so that all ranks hold the same
+  // centroids without a broadcast. Its collectives keep the chunk out of a
+  // CUDA graph.
+  const int ntl = (cnt + kTile - 1) / kTile;
+  const int npt_loc = std::max(0, std::min(npt - lo, cnt));
+  const size_t rec_bytes = sizeof(double4) * ((size_t)mu + 1);
+  std::vector<size_t> rcounts(ranks, rec_bytes), rdispls(ranks);
+  for (int q = 0; q < ranks; ++q) rdispls[q] = (size_t)q * rec_bytes;
+  auto launch_chunk_sharded = [&]() -> int {
+    for (int it = 0; it < kIterChunk; ++it) {
+      k_hist<<<ntl, 256, hist_smem, stream>>>(b.label + lo, cnt, b.st, b.hist);
+      k_hist_scan<<<grid_for(mu, 256), 256, 0, stream>>>(b.hist, ntl, b.st, b.members);
+      k_label_start<<<1, 1024, 0, stream>>>(b.members, b.st, b.start);
+      k_scatter<<<ntl, 128, scatter_smem, stream>>>(b.label + lo, cnt, b.st, b.hist, b.start,
+                                                    b.px + lo, b.py + lo, b.pz + lo, b.pw + lo,
+                                                    b.sorted);
+      k_segsum<<<grid_for(mu, 8), 256, 0, stream>>>(b.sorted, b.start, b.members, b.px + lo,
+                                                    b.py + lo, b.pz + lo, b.pw + lo, b.label + lo,
+                                                    cnt, npt_loc, 0, b.st, sb.send + 1);
+      k_shard_header<<<1, 1, 0, stream>>>(b.st, sb.send);
+      ISDF_CHECK_LAUNCH();
+      ISDF_TRY(shard->allgatherv(sb.send, rec_bytes, sb.recv, rcounts.data(), rdispls.data(),
+                                 stream));
+      k_shard_begin<<<1, 1, 0, stream>>>(b.st, sb.recv, ranks, mu + 1, max_f, args.max_iter);
+      k_shard_sums<<<grid_for(mu, 128), 128, 0, stream>>>(b.st, sb.recv, ranks, mu + 1, b.sums);
+      k_centroids<<<1, 1024, cmax_smem, stream>>>(b.sums, b.st, b.cen, b.shift, b.cell_of, cg,
+                                                  b.nbshift);
+      k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
+                                                    b.cell_of);
+      k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen,
+                                                          b.cell_start, b.cell_cen, cg, am, b.st,
+                                                          b.label, 1, b.bnd, b.shift, b.nbshift,
+                                                          b.pcell, b.pd12);
+      k_iter_end<<<1, 1, 0, stream>>>(b.st, 0);
+      ISDF_CHECK_LAUNCH();
+    }
+    return ISDF_OK;
+  };
   cudaGraphExec_t exec = nullptr;
-  {
+  if (!shard) {
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
       launch_chunk();
@@ -1275,7 +1514,8 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     }
   } guard{exec};
   for (;;) {
-    if (exec) ISDF_CUDA(cudaGraphLaunch(exec, stream));
+    if (shard) ISDF_TRY(launch_chunk_sharded());
+    else if (exec) ISDF_CUDA(cudaGraphLaunch(exec, stream));
     else launch_chunk();
     ISDF_CHECK_LAUNCH();
     ISDF_TRY(read_back(&hst, b.st, sizeof(KmState), stream));
@@ -1283,18 +1523,34 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     if (++chunks > max_chunks) return record_error(ISDF_ERR_CUDA, "kmeans: loop did not stop");
   }
   res->iters = hst.s;
-  res->search_frac = (double)hst.searches / ((double)n * (hst.s + 1));
+  res->search_frac = (double)hst.searches / ((double)cnt * (hst.s + 1));
   // + the state, per-chunk and selection reads through the mapped mailbox
   res->launches =
-      4 + 4 + (am.g2p ? 1 : 0) + (chunks + 1) * kIterChunk * 10 + 2 +
+      4 + 4 + (am.g2p ? 1 : 0) + (chunks + 1) * kIterChunk * (shard ? 12 : 10) + 2 +
       (readback_mailbox() ? chunks + 3 : 0);
   const int rk = hst.rk;
 
-  dim3 fgrid((unsigned)((rk + 127) / 128), (unsigned)nchunks);
-  k_final_partial<<<fgrid, 128, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.st, b.part_d,
-                                             b.part_i);
-  k_final_reduce<<<grid_for(rk, 128), 128, 0, stream>>>(b.part_d, b.part_i, nchunks, b.st,
-                                                        b.pidx, b.sel);
+  if (!shard) {
+    dim3 fgrid((unsigned)((rk + 127) / 128), (unsigned)nchunks);
+    k_final_partial<<<fgrid, 128, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.st, b.part_d,
+                                               b.part_i);
+    k_final_reduce<<<grid_for(rk, 128), 128, 0, stream>>>(b.part_d, b.part_i, nchunks, b.st,
+                                                          b.pidx, b.sel);
+  } else {
+    // each rank's first minimum over its points, then MINLOC over the ranks
+    const int nch = (cnt + kFinalChunk - 1) / kFinalChunk;
+    dim3 fgrid((unsigned)((rk + 127) / 128), (unsigned)nch);
+    k_final_partial<<<fgrid, 128, 0, stream>>>(b.px + lo, b.py + lo, b.pz + lo, cnt, b.cen, b.st,
+                                               b.part_d, b.part_i);
+    k_final_local<<<grid_for(rk, 128), 128, 0, stream>>>(b.part_d, b.part_i, nch, b.st,
+                                                         b.pidx + lo, sb.fsend);
+    ISDF_CHECK_LAUNCH();
+    const size_t fb = sizeof(double2) * (size_t)mu;
+    std::vector<size_t> fc(ranks, fb), fd(ranks);
+    for (int q = 0; q < ranks; ++q) fd[q] = (size_t)q * fb;
+    ISDF_TRY(shard->allgatherv(sb.fsend, fb, sb.frecv, fc.data(), fd.data(), stream));
+    k_minloc<<<grid_for(rk, 128), 128, 0, stream>>>(sb.frecv, ranks, mu, b.st, b.sel);
+  }
   ISDF_CHECK_LAUNCH();
   std::vector<int> sel(rk);
   ISDF_TRY(read_back(sel.data(), b.sel, sizeof(int) * (size_t)rk, stream));

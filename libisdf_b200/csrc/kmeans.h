@@ -43,6 +43,15 @@ int kmeans_select_batch(const KmeansArgs* args, int count, Arena& arena, cudaStr
                         KmeansResult* res);
 int kmeans_weight(const double* d_psi, long long ng, int nocc, int nv1, int nc1, int nv2, int nc2,
                   double* d_w, cudaStream_t stream);
-int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, KmeansResult* res);
+// shard != nullptr: this rank's part of the p-rank selection (the
+// reference's KMEAN at world size p, utility.cpp:682-969): it assigns and
+// folds its own block of the point list, the partial sums are exchanged
+// through `shard` every iteration and combined in binomial-tree order, the
+// nearest points by MINLOC. Every rank gets the same piv.
+struct Transport;
+constexpr int kKmeansMaxRanks = 64;
+size_t kmeans_shard_workspace_bytes(long long ng, int mu, int ranks);
+int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, KmeansResult* res,
+                  Transport* shard = nullptr);
 
 }  // namespace isdf_b200

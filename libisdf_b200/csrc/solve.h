@@ -16,6 +16,7 @@ constexpr int kDefaultMixedSlices = 6;
 
 int iround(double a);
 int default_mu(int nv1, int nc1, int nv2, int nc2);
+int check_state_ranges(int nocc, int nstate, int nv1, int nc1, int nv2, int nc2);
 size_t solve_workspace_bytes(long long ng, int nstate, int mu, int selector, int precision,
                              int check, double qrcp_factor, const int* num_grid, int npair);
 int acquire_workspace(size_t bytes, Arena* arena, cudaStream_t* lib_stream);

@@ -111,6 +111,32 @@ def test_cxx_drop_in_caller_links(tmp_path):
     assert r.returncode == 0, r.stderr
 
 
+def test_cxx_mpi_caller_links(tmp_path):
+    """With mpi.h included first, include/isdf.hpp's ISDF() dispatches an MPI
+    communicator of more than one rank to the p-rank solve over NCCL
+    (isdf_comm_nccl_unique_id + MPI_Bcast + isdf_comm_create_nccl +
+    isdf_solve_sharded): that branch compiles and links (tests/cxx/mpi_stub
+    stands in for an MPI installation; several ranks need several GPUs)."""
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    src = tmp_path / "mpi_caller.cpp"
+    src.write_text("#include <mpi.h>\n#include \"isdf.hpp\"\n"
+                   "int main() { isdf::Domain d; d.comm = MPI_COMM_WORLD;\n"
+                   "  if (false) isdf::isdffunc::ISDF(nullptr, d, 1, 2, 1, 1, 1, 1, 4, nullptr,\n"
+                   "                                  nullptr, 10);\n"
+                   "  return isdf::isdffunc::sharded_comm(d.comm) == nullptr ? 0 : 1; }\n")
+    isdf.lib()
+    exe = tmp_path / "mpi_caller"
+    r = subprocess.run(["g++", "-std=c++14", str(src), "-o", str(exe),
+                        "-I", os.path.join(ROOT, "tests", "cxx", "mpi_stub"),
+                        "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include"),
+                        "-L", os.path.join(ROOT, "libisdf_b200"), "-l:libisdf_b200.so",
+                        "-Wl,-rpath," + os.path.join(ROOT, "libisdf_b200")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    # at world size 1 no NCCL communicator is made (the one-GPU path runs)
+    assert subprocess.run([str(exe)]).returncode == 0
+
+
 def test_request_footprint_counts_check_and_oversampling():
     """isdf_request_workspace_bytes includes what isdf_workspace_bytes leaves
     out: the check's buffers (they depend on the grid's shape) and the QRCP
