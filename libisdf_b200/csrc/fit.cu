@@ -168,6 +168,9 @@ __global__ void __launch_bounds__(256) k_potf2(double* A, int lda, int k0, int b
     x[r][c] = 0.0;
   }
   __syncthreads();
+  // right-looking: the trailing update on a 16 x 16 thread grid (thread
+  // (ty, tx) takes rows ty, ty + 16, ... and columns tx, tx + 16, ...)
+  const int ty = tid >> 4, tx = tid & 15;
   for (int j = 0; j < bs; ++j) {
     if (tid == 0) {
       double d = a[j][j];
@@ -178,24 +181,26 @@ __global__ void __launch_bounds__(256) k_potf2(double* A, int lda, int k0, int b
     const double djj = a[j][j];
     for (int i = j + 1 + tid; i < bs; i += 256) a[i][j] = a[i][j] / djj;
     __syncthreads();
-    const int rem = bs - j - 1;
-    for (int e = tid; e < rem * rem; e += 256) {
-      int i = j + 1 + e / rem, c = j + 1 + e % rem;
-      if (c <= i) a[i][c] -= a[i][j] * a[c][j];
+    for (int i = j + 1 + ty; i < bs; i += 16) {
+      const double lij = a[i][j];
+      for (int c = j + 1 + tx; c <= i; c += 16) a[i][c] -= lij * a[c][j];
     }
     __syncthreads();
   }
-  // X = L^{-1}, one thread per column
-  if (tid < bs) {
-    const int c = tid;
-    x[c][c] = 1.0 / a[c][c];
-    for (int i = c + 1; i < bs; ++i) {
-      double s = 0.0;
-      for (int k = c; k < i; ++k) s = fma(a[i][k], x[k][c], s);
-      x[i][c] = -s / a[i][i];
+  // X = L^{-1} row by row, x(i, c) = -(sum_{c <= k < i} L(i, k) x(k, c)) / L(i, i):
+  // four threads per column, each summing every fourth k
+  {
+    const int c = tid >> 2, part = tid & 3;
+    for (int i = 0; i < bs; ++i) {
+      double sum = 0.0;
+      if (c < i)
+        for (int k = c + part; k < i; k += 4) sum = fma(a[i][k], x[k][c], sum);
+      sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+      sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+      if (part == 0 && c <= i) x[i][c] = c == i ? 1.0 / a[i][i] : -sum / a[i][i];
+      __syncthreads();
     }
   }
-  __syncthreads();
   for (int e = tid; e < kNB * kNB; e += 256) {
     int r = e % kNB, c = e / kNB;
     if (r < bs && c < bs) A[(long long)(k0 + r) + (long long)(k0 + c) * lda] = r >= c ? a[r][c] : 0.0;

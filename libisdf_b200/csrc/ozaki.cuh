@@ -31,10 +31,12 @@
 // bulk copies (cp.async.bulk, no tensor map, no multicast) issued by one
 // thread and completing on the stage's mbarrier by transaction count.
 //
-// Warp roles (192 threads, one persistent CTA per SM): warps 0-3 run the
-// epilogue (warp w reads TMEM lanes 32w..32w+31), one thread of warp 4 issues
-// the MMAs and warp 4 owns the TMEM allocation, one thread of warp 5 issues
-// the copies into an NSTAGE-deep ring that runs ahead across tiles. Each ring
+// Warp roles (320 threads, one persistent CTA per SM): warps 0-7 run the
+// epilogue (warp w reads TMEM lanes 32 (w % 4) .. + 31 and half of the tile's
+// columns, so that two warps share each lane quarter and the conversion and
+// stores of a tile take half as long), one thread of warp 8 issues the MMAs
+// and warp 8 owns the TMEM allocation, one thread of warp 9 issues the copies
+// into an NSTAGE-deep ring that runs ahead across tiles. Each ring
 // slot has a "full" mbarrier (expect-tx arrival plus the copies' bytes) and
 // an "empty" mbarrier (tcgen05.commit after the slot's MMAs); acc_full /
 // acc_empty hand the accumulators between the MMA thread and the epilogue,
@@ -59,7 +61,8 @@ namespace ozaki {
 
 constexpr int BM = 128, BN = 64, BKB = 32;  // tile rows, tile columns, K bytes per stage
 constexpr int kTmemCols = 512;
-constexpr int kThreads = 192;
+constexpr int kEpiWarps = 8;  // two per TMEM lane quarter, each draining half the columns
+constexpr int kThreads = (kEpiWarps + 2) * 32;
 constexpr int kGroupM = 8;
 constexpr int kSmemLimit = 232448;  // 227 KB per CTA
 constexpr int kMaxK = 16384;        // 7 * 127^2 * kMaxK < 2^31
@@ -120,17 +123,22 @@ __host__ __device__ __forceinline__ long long tiled_offset(long long blk, int kb
                  : base + t * (R * BKB) + c * (R * 16) + r * 16;
 }
 
-#define ISDF_TMEM_LD32(v, addr)                                                              \
+#define ISDF_TMEM_LD16(v, addr)                                                              \
   asm volatile(                                                                              \
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13," \
-      "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"    \
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13," \
+      "%14,%15}, [%16];\n"                                                                    \
       : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),  \
         "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),          \
-        "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),       \
-        "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),       \
-        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),       \
-        "=r"(v[31])                                                                          \
+        "=r"(v[13]), "=r"(v[14]), "=r"(v[15])                                                \
       : "r"(addr))
+
+// 2^e: the bit pattern of a normal power of two (e in [-1022, 1023]), else
+// ldexp; the same value either way. The epilogue scales every element by two
+// of them, and the library call would cost a large share of its time.
+__device__ __forceinline__ double pow2(int e) {
+  return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52)
+                                   : ldexp(1.0, e);
+}
 
 // Tile id -> (first row, first column), grouped raster: kGroupM row blocks
 // by all column blocks per group.
@@ -194,7 +202,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t acc_empty = acc_full + 8u;
   const uint32_t done_bar = acc_full + 16u;
 
-  if (warp == 4) {
+  if (warp == kEpiWarps) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&tmem_slot)),
                  "r"(kTmemCols));
@@ -206,7 +214,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(empty_bar(i), 1);
     }
     mbar_init(acc_full, 1);
-    mbar_init(acc_empty, 128);
+    mbar_init(acc_empty, kEpiWarps * 32);
     mbar_init(done_bar, 1);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n");
@@ -216,7 +224,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   asm volatile("tcgen05.fence::after_thread_sync;\n");
   const uint32_t tmem = tmem_slot;
 
-  if (warp == 5) {
+  if (warp == kEpiWarps + 1) {
     // ---------------------------------------------------------------- copies
     if (lane == 0) {
       long long g = 0;  // stages issued so far (all tiles)
@@ -248,7 +256,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (!mbar_wait_all(full_bar((int)(t % NST)), (uint32_t)(t / NST) & 1u)) *abortp = 1;
     }
     __syncwarp();
-  } else if (warp == 4) {
+  } else if (warp == kEpiWarps) {
     // ---------------------------------------------------------------- MMA issue
     if (lane == 0) {
       long long g = 0;
@@ -297,6 +305,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncwarp();
   } else {
     // ---------------------------------------------------------------- epilogue
+    // warp w reads TMEM lanes 32 (w % 4) .. + 31 (its rows) and columns
+    // [ (w / 4) CW, + CW )
+    constexpr int CW = BN / (kEpiWarps / 4);
+    const int q = warp & 3, c_lo = (warp >> 2) * CW;
+    double w[S];  // 254^{-(d+2)}
+    w[0] = 1.0 / (kBase * kBase);
+#pragma unroll
+    for (int d = 1; d < S; ++d) w[d] = w[d - 1] / kBase;
     int it = 0;
     for (long long id = blockIdx.x; id < tiles; id += gridDim.x, ++it) {
       long long m0;
@@ -306,31 +322,28 @@ __global__ void __launch_bounds__(kThreads, 1)
       bool ready = mbar_wait(acc_full, (uint32_t)it & 1u, abortp) && *abortp == 0;
       if (!__all_sync(0xffffffffu, ready)) break;  // warp-uniform: tcgen05.ld is collective
       asm volatile("tcgen05.fence::after_thread_sync;\n");
-      const int row = warp * 32 + lane;
+      const int row = q * 32 + lane;
       const long long m = m0 + row;
-      double out[BN];
+      const uint32_t lane_base = tmem + ((uint32_t)(q * 32) << 16);
+      double out[CW];
 #pragma unroll
-      for (int j = 0; j < BN; ++j) out[j] = 0.0;
+      for (int j = 0; j < CW; ++j) out[j] = 0.0;
       if (nk > 0) {
-        double w[S];  // 254^{-(d+2)}
-        w[0] = 1.0 / (kBase * kBase);
+        // 16 columns per TMEM round trip, two levels at a time; per column the
+        // levels accumulate in order d = 0, 1, ...
 #pragma unroll
-        for (int d = 1; d < S; ++d) w[d] = w[d - 1] / kBase;
-        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-        // two levels per TMEM round trip; per column the levels still
-        // accumulate in order d = 0, 1, ...
-#pragma unroll
-        for (int c0 = 0; c0 < BN; c0 += 32) {
+        for (int c0 = 0; c0 < CW; c0 += 16) {
 #pragma unroll
           for (int d = 0; d < S; d += 2) {
-            uint32_t va[32], vb[32];
-            ISDF_TMEM_LD32(va, lane_base + (uint32_t)(d * BN + c0));
-            if (d + 1 < S) ISDF_TMEM_LD32(vb, lane_base + (uint32_t)((d + 1) * BN + c0));
+            uint32_t va[16], vb[16];
+            ISDF_TMEM_LD16(va, lane_base + (uint32_t)(d * BN + c_lo + c0));
+            if (d + 1 < S) ISDF_TMEM_LD16(vb, lane_base + (uint32_t)((d + 1) * BN + c_lo + c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
+            for (int j = 0; j < 16; ++j) {
               out[c0 + j] = __fma_rn((double)(int)va[j], w[d], out[c0 + j]);
-              if (d + 1 < S) out[c0 + j] = __fma_rn((double)(int)vb[j], w[d + 1], out[c0 + j]);
+              if (d + 1 < S)
+                out[c0 + j] = __fma_rn((double)(int)vb[j], w[d + 1], out[c0 + j]);
             }
           }
         }
@@ -339,13 +352,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       asm volatile("tcgen05.fence::before_thread_sync;\n");
       mbar_arrive(acc_empty);
       if (m < M) {
-        const double sa = ldexp(1.0, ea[m]);
+        const double sa = pow2(ea[m]);
         double amax = 0.0;
 #pragma unroll
-        for (int j = 0; j < BN; ++j) {
-          const int n = n0 + j;
+        for (int j = 0; j < CW; ++j) {
+          const int n = n0 + c_lo + j;
           if (n < N) {
-            const double val = out[j] * sa * ldexp(1.0, eb[n]);
+            const double val = out[j] * sa * pow2(eb[n]);
             double* p = C + m + (long long)n * ldc;
             double r;
             if (EPI == 0) r = val;
@@ -364,14 +377,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   asm volatile("tcgen05.fence::before_thread_sync;\n");
   __syncthreads();
   if (*abortp != 0 && tid == 0) atomicExch(err, 1);
-  if (warp == 4) {
+  if (warp == kEpiWarps) {
     asm volatile("tcgen05.fence::after_thread_sync;\n");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
                  "r"(kTmemCols));
   }
 }
 
-#undef ISDF_TMEM_LD32
+#undef ISDF_TMEM_LD16
 
 }  // namespace ozaki
 }  // namespace isdf_b200

@@ -70,7 +70,10 @@ SI216 = Shape("Si216-like 108^3", 3, 108, 864, 432, 432, 432, 432, 432, 4320)
 # Si64's states and mu on a 40^3 grid: the profiling size (theta 1 GB, larger
 # than L2, a few GB on the device in all).
 SI64C = Shape("Si64-like on 40^3 (profiling)", 2, 40, 256, 128, 128, 128, 128, 128, 2048)
-SHAPES = {"si8": SI8, "si64": SI64, "si216": SI216, "si64c": SI64C}
+# Si216's states and mu on a 40^3 grid: the profiling size of the mixed form's
+# products at Si216's K and N (theta 2.2 GB).
+SI216C = Shape("Si216-like on 40^3 (profiling)", 3, 40, 864, 432, 432, 432, 432, 432, 4320)
+SHAPES = {"si8": SI8, "si64": SI64, "si216": SI216, "si64c": SI64C, "si216c": SI216C}
 
 
 def diamond_sites(cells: int) -> np.ndarray:
