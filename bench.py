@@ -144,7 +144,7 @@ def replica_value(world: int, steps: int, t_ms: float) -> float:
     return world * steps / (t_ms * 1e-3)
 
 
-SEEDS = {"si8": 0, "si64": 1, "si216": 3, "si64c": 1, "si216c": 3}  # the benchmark configurations' seeds
+SEEDS = {"si8": 0, "si64": 1, "si216": 3, "si64c": 1, "si216c": 3, "si64vc": 1}  # the benchmark configurations' seeds
 
 
 def _shape_psi(synth, shape, name):
@@ -987,7 +987,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["si8", "si64", "si216", "si64c", "si216c"],
+    ap.add_argument("--config", choices=["si8", "si64", "si216", "si64c", "si216c", "si64vc"],
                     default="si216")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--no-compare", action="store_true",

@@ -70,10 +70,15 @@ SI216 = Shape("Si216-like 108^3", 3, 108, 864, 432, 432, 432, 432, 432, 4320)
 # Si64's states and mu on a 40^3 grid: the profiling size (theta 1 GB, larger
 # than L2, a few GB on the device in all).
 SI64C = Shape("Si64-like on 40^3 (profiling)", 2, 40, 256, 128, 128, 128, 128, 128, 2048)
+# Si64's grid and states with a valence x conduction pair window (S1 = the
+# 128 occupied states, S2 = the 128 empty ones), the pair products a GW / BSE
+# code fits; mu = 8 sqrt(128 x 128) = 1024 (the reference's default formula).
+SI64VC = Shape("Si64-like valence x conduction 80^3", 2, 80, 256, 128, 128, 0, 0, 128, 1024)
 # Si216's states and mu on a 40^3 grid: the profiling size of the mixed form's
 # products at Si216's K and N (theta 2.2 GB).
 SI216C = Shape("Si216-like on 40^3 (profiling)", 3, 40, 864, 432, 432, 432, 432, 432, 4320)
-SHAPES = {"si8": SI8, "si64": SI64, "si216": SI216, "si64c": SI64C, "si216c": SI216C}
+SHAPES = {"si8": SI8, "si64": SI64, "si216": SI216, "si64c": SI64C, "si216c": SI216C,
+          "si64vc": SI64VC}
 
 
 def diamond_sites(cells: int) -> np.ndarray:

@@ -8,6 +8,8 @@
   * Si64-like QRCP (oversampling 2.5, seed 2): a prefix of the pivots checked
     step by step against dgeqpf on the reference's MG matrix, theta against
     the oracle on sampled rows;
+  * Si64-like valence x conduction (S1 = 128 occupied, S2 = 128 empty states,
+    mu = 1024): the same checks on the two-factor (S1 != S2) path;
   * Si216-like (108^3, 864 states, mu = 4320, seed 3): the mixed form's and the
     FP64 form's theta against the oracle fit on sampled rows.
 
@@ -106,6 +108,37 @@ def test_si64_kmeans_piv_bit_exact_and_theta(torch_cuda):
     assert rep_m.rk_eff == rk_o and np.array_equal(piv, piv_o)
     _compare("Si64 mixed", _theta_rows(torch, d_theta, rk_o, rows), th_o, psi, piv_o, rk_o, pi,
              pj, 1e-6)
+
+
+def test_si64_valence_conduction(torch_cuda):
+    """S1 != S2 at the Si64 size (the two-factor epilogues): the valence x
+    conduction window of 128 occupied x 128 empty states (mu = 1024), the pair
+    products a GW / BSE code fits. piv, the effective mu and the iteration
+    count bit-exact against the K-means port with the same window; theta of the
+    FP64 and of the mixed form against the oracle on sampled rows and pairs."""
+    torch = torch_cuda
+    s = synth.SI64VC
+    psi = synth.shape_orbitals(s, 1, device="cuda")
+    a = (s.nocc, s.nv1, s.nc1, s.nv2, s.nc2)
+    piv_o, rk_o, it_o, _ = port.kmeans_piv(psi, (s.n,) * 3, (s.length,) * 3, *a, s.mu,
+                                           s.kmeans_iters)
+    d_psi = torch.from_numpy(np.ascontiguousarray(psi.T)).cuda()
+    d_theta = torch.empty((s.mu, s.ng), dtype=torch.float64, device="cuda")
+    piv = np.zeros(s.ng, dtype=np.int32)
+    rep = _solve(torch, d_psi, s, d_theta, piv, isdf.Options())
+    record_parity("Si64 valence x conduction", "rk_eff / iterations (GPU, port)",
+                  f"{rep.rk_eff}/{rep.kmeans_iters}, {rk_o}/{it_o}")
+    assert (rep.rk_eff, rep.kmeans_iters) == (rk_o, it_o)
+    assert np.array_equal(piv, piv_o), int(np.argmax(piv != piv_o))
+    rows, pi, pj = _sample(s)
+    th_o = ofit.getbasis_rows(psi, *a, rk_o, piv_o, rows)
+    bound = _spread("Si64 valence x conduction", psi, a, piv_o, rk_o, rows, th_o, pi, pj)
+    _compare("Si64 valence x conduction FP64", _theta_rows(torch, d_theta, rk_o, rows), th_o, psi,
+             piv_o, rk_o, pi, pj, bound)
+    rep_m = _solve(torch, d_psi, s, d_theta, piv, isdf.Options(precision=isdf.PRECISION_MIXED))
+    assert rep_m.rk_eff == rk_o and np.array_equal(piv, piv_o)
+    _compare("Si64 valence x conduction mixed", _theta_rows(torch, d_theta, rk_o, rows), th_o,
+             psi, piv_o, rk_o, pi, pj, 1e-6)
 
 
 def test_si64_qrcp_pivots_and_theta(torch_cuda):
