@@ -492,11 +492,31 @@ __global__ void k_point_cells(const double* __restrict__ px, const double* __res
   pd12[p] = make_double2(D1 * kRoundDown - g.tol, D2 * kRoundDown - g.tol);
 }
 
-// Two phases per block: every thread tests its point against its distance
-// bounds; the points that fail are appended (warp order kept) to a block
-// list, which the block's threads then search together, so the divergent
-// ring search runs on full warps.
-__global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
+// Warp-coherent search. A warp's points are a 4 x 4 x 2 brick of the grid
+// (or 32 consecutive points), so the points of a warp that fail the bound
+// test share their candidates: with U the largest of their seed distances
+// (squared distance to the old label, which bounds each one's nearest), every
+// centroid that can be nearest to one of them lies in a cell whose box is
+// within sqrt(U) of the points' bounding box. The warp stages those cells'
+// centroids in shared memory once and every searching lane runs the same loop
+// over them, comparing (d, index) pairs as the ring search does: the label is
+// the ring search's bit for bit. Centroids not staged are more than sqrt(U)
+// from every point of the box, which gives the lower bound. Lanes without a
+// seed (the first assignment), too many cells or too many candidates take the
+// ring search instead.
+constexpr int kWarpCand = 128;   // centroids staged per warp
+constexpr int kWarpCells = 125;  // cells a warp may scan
+
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__global__ void __launch_bounds__(kAssignThreads) k_assign_warp(
     const double* __restrict__ px, const double* __restrict__ py, const double* __restrict__ pz,
     int n, const double4* __restrict__ cen, const int* __restrict__ cell_start,
     const double4* __restrict__ cell_cen, CellGrid g, AssignMap am, KmState* st,
@@ -504,12 +524,9 @@ __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
     const double* __restrict__ shift, const float* __restrict__ nbshift,
     const int* __restrict__ pcell, const double2* __restrict__ pd12) {
   if (st->done) return;
-  __shared__ int list_p[kAssignThreads], list_old[kAssignThreads];
-  __shared__ int list_n;
-  if (threadIdx.x == 0) list_n = 0;
-  __syncthreads();
+  __shared__ double4 cand[kAssignThreads / 32][kWarpCand];
   const int rk = st->rk;
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int p = assign_point((long long)blockIdx.x * blockDim.x + threadIdx.x, am);
   bool need = false;
   int old = -1;
@@ -520,18 +537,16 @@ __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
       const double2 b = bnd[p];
       // Every other centroid moved closer by at most its shift: at most
       // the 3^3-block maximum inside the 27 cells around p, the 5^3-block
-      // maximum in the ring beyond (which started at least D1 away), the
-      // global maximum further out (at least D2 away); no bound across the
-      // domain's faces.
+      // maximum in the ring beyond (which started at least D1 = dd.x away),
+      // the global maximum further out (at least D2 = dd.y away); no bound
+      // across the domain's faces.
       const double gmax = __longlong_as_double((long long)st->maxshift_bits);
       const int cell = pcell[p];
       const double near1 = (double)nbshift[cell], near2 = (double)nbshift[kMaxCells + cell];
-      const double2 dd = pd12[p];  // distances to the outside of the 3^3 / 5^3 blocks
-      const double D1 = dd.x, D2 = dd.y;
-      // every other centroid was at least l away (and D1 / D2 beyond the blocks)
+      const double2 dd = pd12[p];
       double lo = __dsub_rd(b.y, near1);
-      lo = fmin(lo, __dsub_rd(fmax(b.y, D1), near2));
-      lo = fmin(lo, __dsub_rd(fmax(b.y, D2), gmax));
+      lo = fmin(lo, __dsub_rd(fmax(b.y, dd.x), near2));
+      lo = fmin(lo, __dsub_rd(fmax(b.y, dd.y), gmax));
       lo = fmax(0.0, lo);
       double up = __dadd_ru(b.x, shift[old]);
       if (!(up * kBoundMargin < lo))
@@ -542,28 +557,103 @@ __global__ void __launch_bounds__(kAssignThreads) k_assign_grid(
       }
     }
   }
-  // append the points that need a search, warp by warp in lane order
   const unsigned mask = __ballot_sync(0xffffffffu, need);
-  int wbase = 0;
-  if (lane == 0 && mask) wbase = atomicAdd(&list_n, __popc(mask));
-  wbase = __shfl_sync(0xffffffffu, wbase, 0);
+  if (!mask) return;
+  const double inf = __longlong_as_double(0x7ff0000000000000LL);
+  double x = 0.0, y = 0.0, z = 0.0, best = inf;
+  int bj = 0x7fffffff;
   if (need) {
-    const int slot = wbase + __popc(mask & ((1u << lane) - 1u));
-    list_p[slot] = p;
-    list_old[slot] = old;
+    x = px[p];
+    y = py[p];
+    z = pz[p];
+    if (old >= 0 && old < rk) {
+      best = ref_dist2(x, y, z, cen[old]);
+      bj = old;
+    }
   }
-  __syncthreads();
-  const int ln = list_n;
+  const double shrink = 1.0 - 2e-14;
+  bool ok = __all_sync(0xffffffffu, !need || bj != 0x7fffffff);
+  const double U = warp_max(need ? best : 0.0);
+  const double x0 = warp_min(need ? x : inf), x1 = warp_max(need ? x : -inf);
+  const double y0 = warp_min(need ? y : inf), y1 = warp_max(need ? y : -inf);
+  const double z0 = warp_min(need ? z : inf), z1 = warp_max(need ? z : -inf);
+  int total = 0;
+  if (ok) {
+    const double R = __dmul_ru(__dsqrt_ru(U), kRoundUp) + g.tol;
+    const int nc = g.nc;
+    const int i0 = min(nc - 1, max(0, (int)floor((x0 - R) / g.h[0])));
+    const int i1 = min(nc - 1, max(0, (int)floor((x1 + R) / g.h[0])));
+    const int j0 = min(nc - 1, max(0, (int)floor((y0 - R) / g.h[1])));
+    const int j1 = min(nc - 1, max(0, (int)floor((y1 + R) / g.h[1])));
+    const int k0 = min(nc - 1, max(0, (int)floor((z0 - R) / g.h[2])));
+    const int k1 = min(nc - 1, max(0, (int)floor((z1 + R) / g.h[2])));
+    const int ni = i1 - i0 + 1, nj = j1 - j0 + 1;
+    const int ncell = ni * nj * (k1 - k0 + 1);
+    if (ncell > kWarpCells) ok = false;
+    for (int base = 0; ok && base < ncell; base += 32) {
+      const int c = base + lane;
+      int cnt = 0, first = 0;
+      if (c < ncell) {
+        const int ci = i0 + c % ni, cj = j0 + (c / ni) % nj, ck = k0 + c / (ni * nj);
+        // distance from the points' box to the cell's box (widened by tol)
+        const double bx = fmax(0.0, fmax(ci * g.h[0] - g.tol - x1, x0 - (ci + 1) * g.h[0] - g.tol));
+        const double by = fmax(0.0, fmax(cj * g.h[1] - g.tol - y1, y0 - (cj + 1) * g.h[1] - g.tol));
+        const double bz = fmax(0.0, fmax(ck * g.h[2] - g.tol - z1, z0 - (ck + 1) * g.h[2] - g.tol));
+        const double lb = bx * bx + by * by + bz * bz;
+        if (!(lb * shrink > U)) {
+          const int id = ci + nc * (cj + nc * ck);
+          first = cell_start[id];
+          cnt = cell_start[id + 1] - first;
+        }
+      }
+      int off = cnt;  // inclusive scan over the warp
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, off, o);
+        if (lane >= o) off += v;
+      }
+      const int here = __shfl_sync(0xffffffffu, off, 31);
+      if (total + here > kWarpCand) {
+        ok = false;
+        break;
+      }
+      for (int q = 0; q < cnt; ++q) cand[wid][total + off - cnt + q] = cell_cen[first + q];
+      total += here;
+    }
+  }
+  __syncwarp();
   int changed = 0;
-  for (int i = threadIdx.x; i < ln; i += blockDim.x) {
-    const int q = list_p[i], o = list_old[i];
-    const int bj = ring_search(px[q], py[q], pz[q], o, rk, cen, cell_start, cell_cen, g, &bnd[q]);
-    if (count && o != bj) ++changed;
-    label[q] = bj;
+  if (need) {
+    int lab;
+    if (ok) {
+      double second = inf;
+      for (int q = 0; q < total; ++q) {
+        const double4 c = cand[wid][q];
+        const double d = ref_dist2(x, y, z, c);
+        const int j = (int)c.w;
+        if (d < best || (d == best && j < bj)) {
+          if (j != bj) second = best;
+          best = d;
+          bj = j;
+        } else if (j != bj) {
+          second = fmin(second, d);
+        }
+      }
+      // every centroid not staged is more than sqrt(U) from the point
+      const double floor2 = U * shrink;
+      bnd[p] = make_double2(__dmul_ru(__dsqrt_ru(best), kRoundUp),
+                            __dmul_rd(__dsqrt_rd(fmin(second, floor2)), kRoundDown));
+      lab = bj;
+    } else {
+      lab = ring_search(x, y, z, old, rk, cen, cell_start, cell_cen, g, &bnd[p]);
+    }
+    if (count && old != lab) ++changed;
+    label[p] = lab;
   }
   for (int o = 16; o > 0; o >>= 1) changed += __shfl_xor_sync(0xffffffffu, changed, o);
-  if (lane == 0 && count && changed) atomicAdd(&st->changed, changed);
-  if (threadIdx.x == 0 && ln) atomicAdd(&st->searches, (unsigned long long)ln);
+  if (lane == 0) {
+    if (count && changed) atomicAdd(&st->changed, changed);
+    atomicAdd(&st->searches, (unsigned long long)__popc(mask));
+  }
 }
 
 // ---------------------------------------------------------------- control
@@ -1415,7 +1505,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
   k_point_cells<<<grid_for(n, 256), 256, 0, stream>>>(b.px, b.py, b.pz, n, cg, b.pcell, b.pd12);
   k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
                                                 b.cell_of);
-  k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.cell_start,
+  k_assign_warp<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen, b.cell_start,
                                                       b.cell_cen, cg, am, b.st, b.label, 0,
                                                       b.bnd, b.shift, b.nbshift, b.pcell,
                                                       b.pd12);
@@ -1447,7 +1537,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
                                                   b.nbshift);
       k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
                                                     b.cell_of);
-      k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen,
+      k_assign_warp<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen,
                                                           b.cell_start, b.cell_cen, cg, am, b.st,
                                                           b.label, 1, b.bnd, b.shift, b.nbshift,
                                                           b.pcell, b.pd12);
@@ -1486,7 +1576,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
                                                   b.nbshift);
       k_build_cells<<<1, 1024, cell_smem, stream>>>(b.cen, b.st, cg, b.cell_start, b.cell_cen,
                                                     b.cell_of);
-      k_assign_grid<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen,
+      k_assign_warp<<<pgrid, kAssignThreads, 0, stream>>>(b.px, b.py, b.pz, n, b.cen,
                                                           b.cell_start, b.cell_cen, cg, am, b.st,
                                                           b.label, 1, b.bnd, b.shift, b.nbshift,
                                                           b.pcell, b.pd12);
