@@ -502,10 +502,10 @@ __global__ void k_point_cells(const double* __restrict__ px, const double* __res
 // over them, comparing (d, index) pairs as the ring search does: the label is
 // the ring search's bit for bit. Centroids not staged are more than sqrt(U)
 // from every point of the box, which gives the lower bound. Lanes without a
-// seed (the first assignment), too many cells or too many candidates take the
+// seed (the first assignment), more than 216 cells or more than 160 candidates take the
 // ring search instead.
-constexpr int kWarpCand = 128;   // centroids staged per warp
-constexpr int kWarpCells = 125;  // cells a warp may scan
+constexpr int kWarpCand = 160;   // centroids staged per warp
+constexpr int kWarpCells = 216;  // cells a warp may scan
 
 __device__ __forceinline__ double warp_max(double v) {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
