@@ -104,7 +104,8 @@ int nccl_api(NcclApi** out) {
     void* h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_LOCAL);
     if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_LOCAL);
     if (!h) {
-      failure = std::string("NCCL not found: ") + (dlerror() ? dlerror() : "dlopen failed");
+      const char* why = dlerror();  // read once: the call clears the message
+      failure = std::string("NCCL not found: ") + (why ? why : "dlopen failed");
     } else {
       bool ok = true;
       auto sym = [&](auto& fn, const char* name) {
