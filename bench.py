@@ -567,6 +567,19 @@ def run_ours(args, shape):
         # factor leaves nonzero), over CUDA events around the two launches.
         ops = 2 * 2.0 * ng * rk * (rk / 2 + 32) * S * (S + 1) / 2
         ach = ops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
+        # DRAM traffic per launch from ncu on the 40^3-grid case (Ng = 64000,
+        # rk = 4312, S = 6; mean of the two products): 8.855 GB read (the
+        # digits of both operands, B's re-read once per raster group, so
+        # ~ rows x rk^2) and 2.195 GB written (the FP64 output, rows x rk).
+        # Reported only near that shape, where the scaling holds.
+        if S == 6 and 0.8 <= rk / 4312 <= 1.25:
+            traffic = (8.855e9 * (ng / 64000) * (rk / 4312) ** 2 +
+                       2.195e9 * (ng / 64000) * (rk / 4312))
+            traffic_note = ("bytes per launch (mean of the two products), scaled from the ncu "
+                            "capture at Ng = 64000, rk = 4312: reads by rows x rk^2, writes "
+                            f"by rows x rk; algorithmic {(ng * rk * (S + 8)) / 1e9:.1f} GB")
+        else:
+            traffic, traffic_note = None, "no ncu capture at this rk and S"
         roofline = {"kernel": "k_ozaki_gemm (Y = Z L^-T and theta = Y L^-1, INT8 digit pairs)",
                     "bound": "tensor", "achieved": ach, "peak": int8_peak[0],
                     "unit": "TOPS (INT8)", "frac": (ach / int8_peak[0]) if ach else None,
@@ -575,7 +588,7 @@ def run_ours(args, shape):
                     "peak_source": int8_peak[2],
                     "emulated_fp64_tflops": (2.0 * 2 * ng * rk * (rk / 2 + 32) /
                                              (gemm_ms * 1e-3) / 1e12) if gemm_ms > 0 else None,
-                    "traffic": None}
+                    "traffic": traffic, "traffic_note": traffic_note}
     else:
         roofline = roof64
     line = {
