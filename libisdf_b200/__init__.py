@@ -222,6 +222,8 @@ def lib() -> ctypes.CDLL:
         L.isdf_comm_create_nccl.restype = I
         L.isdf_comm_create_local.argtypes = [I, P, ctypes.c_double, P]
         L.isdf_comm_create_local.restype = I
+        L.isdf_comm_create_callbacks.argtypes = [P, P, I, I, ctypes.POINTER(P)]
+        L.isdf_comm_create_callbacks.restype = I
         L.isdf_comm_rank.argtypes = [P, ctypes.POINTER(I), ctypes.POINTER(I)]
         L.isdf_comm_rank.restype = I
         L.isdf_comm_abort.argtypes = [P]
@@ -509,6 +511,17 @@ def share_nccl_unique_id(group=None) -> bytes:
     return box[0]
 
 
+_SizeP = ctypes.POINTER(ctypes.c_size_t)
+_AllgathervFn = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                 ctypes.c_void_p, _SizeP, _SizeP, ctypes.c_void_p)
+_AlltoallvFn = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, _SizeP, _SizeP,
+                                ctypes.c_void_p, _SizeP, _SizeP, ctypes.c_void_p)
+
+
+class _CommOps(ctypes.Structure):  # isdf_comm_ops_t
+    _fields_ = [("allgatherv", _AllgathervFn), ("alltoallv", _AlltoallvFn)]
+
+
 class Comm:
     """A rank's communicator for the sharded solve (isdf_comm_t)."""
 
@@ -546,6 +559,43 @@ class Comm:
         dv = (ctypes.c_int * size)(*devices) if devices is not None else None
         _check(lib().isdf_comm_create_local(size, dv, float(timeout_s), hs))
         return [cls(hs[r]) for r in range(size)]
+
+    @classmethod
+    def callbacks(cls, allgatherv, alltoallv, rank: int, size: int) -> "Comm":
+        """Transport over the caller's own collectives (isdf_comm_create_callbacks):
+        allgatherv(d_send, send_bytes, d_recv, recv_bytes, recv_displs, stream)
+        and alltoallv(d_send, send_bytes, send_displs, d_recv, recv_bytes,
+        recv_displs, stream) get device addresses and the cudaStream_t as ints
+        and the per-rank byte counts and displacements as lists. The data must
+        have arrived, or be ordered on the stream, when they return; an
+        exception fails the collective (ISDF_ERR_COMM)."""
+        def lst(ptr):
+            return [int(ptr[q]) for q in range(size)]
+
+        def agv(ctx, d_send, send_bytes, d_recv, counts, displs, stream):
+            try:
+                allgatherv(d_send or 0, int(send_bytes), d_recv or 0, lst(counts), lst(displs),
+                           stream or 0)
+                return 0
+            except Exception:  # noqa: BLE001 - reported to the library as a failure
+                return 1
+
+        def a2a(ctx, d_send, scounts, sdispls, d_recv, rcounts, rdispls, stream):
+            try:
+                alltoallv(d_send or 0, lst(scounts), lst(sdispls), d_recv or 0, lst(rcounts),
+                          lst(rdispls), stream or 0)
+                return 0
+            except Exception:  # noqa: BLE001 - reported to the library as a failure
+                return 1
+
+        fns = (_AllgathervFn(agv), _AlltoallvFn(a2a))
+        ops = _CommOps(*fns)
+        h = ctypes.c_void_p()
+        _check(lib().isdf_comm_create_callbacks(ctypes.byref(ops), None, rank, size,
+                                                ctypes.byref(h)))
+        c = cls(h.value)
+        c._callbacks = fns  # the library calls these for the communicator's lifetime
+        return c
 
     def abort(self):
         _check(lib().isdf_comm_abort(self._h))

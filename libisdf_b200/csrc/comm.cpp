@@ -40,21 +40,39 @@
 namespace isdf_b200 {
 
 Transport::~Transport() {
-  if (ws) {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    cudaSetDevice(device);
-    cudaFree(ws);
-    if (stream) cudaStreamDestroy(stream);
-    if (cur >= 0) cudaSetDevice(cur);
-  } else if (stream) {
-    cudaStreamDestroy(stream);
+  if (!ws && !stream && !status) return;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  cudaSetDevice(device);
+  if (ws) cudaFree(ws);
+  if (status) cudaFree(status);
+  if (stream) cudaStreamDestroy(stream);
+  if (cur >= 0) cudaSetDevice(cur);
+}
+
+int Transport::ensure_stream() {
+  ISDF_CUDA(cudaSetDevice(device));
+  if (!stream) ISDF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  return ISDF_OK;
+}
+
+int Transport::ensure_status() {
+  if (status) return ISDF_OK;
+  int cur = -1;
+  ISDF_CUDA(cudaGetDevice(&cur));
+  ISDF_CUDA(cudaSetDevice(device));
+  const cudaError_t e = cudaMalloc((void**)&status, kStatusBytes * (size_t)(size + 1));
+  cudaSetDevice(cur);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    status = nullptr;
+    return record_error(ISDF_ERR_NOMEM, "communicator: status buffer allocation failed");
   }
+  return ISDF_OK;
 }
 
 int Transport::acquire(size_t bytes, Arena* arena) {
-  ISDF_CUDA(cudaSetDevice(device));
-  if (!stream) ISDF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  ISDF_TRY(ensure_stream());
   if (ws_cap < bytes) {
     if (ws) {
       ISDF_CUDA(cudaStreamSynchronize(stream));
@@ -123,8 +141,12 @@ int nccl_api(NcclApi** out) {
       sym(api.Recv, "ncclRecv");
       sym(api.Broadcast, "ncclBroadcast");
       sym(api.AllGather, "ncclAllGather");
-      if (ok) api.h = h;
-      else failure = "NCCL library lacks an entry point this library uses";
+      if (ok) {
+        api.h = h;
+      } else {
+        failure = "NCCL library lacks an entry point this library uses";
+        dlclose(h);
+      }
     }
   }
   if (!api.h) return record_error(ISDF_ERR_UNSUPPORTED, failure.c_str());
@@ -381,6 +403,7 @@ int isdf_comm_create_nccl(const unsigned char id[128], int rank, int size, isdf_
     t->rank = rank;
     t->size = size;
     ISDF_CUDA(cudaGetDevice(&t->device));
+    ISDF_TRY(t->ensure_status());
     ncclUniqueId u;
     std::memcpy(&u, id, sizeof(u));
     ISDF_NCCL(api, api->CommInitRank(&t->comm, size, u, rank), "ncclCommInitRank");
@@ -415,6 +438,7 @@ int isdf_comm_create_local(int size, const int* devices, double timeout_s, isdf_
           cudaEventCreateWithFlags(&g->slots[r].ready, cudaEventDisableTiming) != cudaSuccess ||
           cudaEventCreateWithFlags(&g->slots[r].done, cudaEventDisableTiming) != cudaSuccess)
         rc = record_error(ISDF_ERR_CUDA, "isdf_comm_create_local: device or event setup failed");
+      if (rc == ISDF_OK) rc = t->ensure_status();
       if (rc != ISDF_OK) {
         for (auto* m : made) delete m;
         cudaSetDevice(cur);
@@ -444,6 +468,7 @@ int isdf_comm_create_callbacks(const isdf_comm_ops_t* ops, void* ctx, int rank, 
     t->rank = rank;
     t->size = size;
     ISDF_CUDA(cudaGetDevice(&t->device));
+    ISDF_TRY(t->ensure_status());
     auto* c = new isdf_comm;
     c->t = std::move(t);
     *out = c;

@@ -23,6 +23,12 @@ struct Transport {
   char* ws = nullptr;
   size_t ws_cap = 0;
   cudaStream_t stream = nullptr;
+  // (size + 1) status records of kStatusBytes for the ranks' agreement before
+  // an exchange (records 0..size-1 received, record size sent); allocated
+  // when the communicator is made, so that a rank whose solve fails can
+  // still take part
+  static constexpr size_t kStatusBytes = 256;
+  char* status = nullptr;
 
   virtual ~Transport();
   // Rank q's send_bytes (= counts[q]) land at d_recv + displs[q] on every rank.
@@ -36,6 +42,10 @@ struct Transport {
   // Ends outstanding and future collectives with an error (failure handling).
   virtual int abort() { return 0; }
 
+  // Makes the rank's stream (once) on its device.
+  int ensure_stream();
+  // Allocates the status records (once) on the rank's device.
+  int ensure_status();
   // Grows the workspace to >= bytes on this rank's device.
   int acquire(size_t bytes, Arena* arena);
 };

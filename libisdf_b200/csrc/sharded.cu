@@ -23,6 +23,7 @@
 // ordered on the rank's stream.
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -81,6 +82,63 @@ __global__ void k_pack_cyclic(const double* __restrict__ T, long long count, int
   }
 }
 
+// The ranks' agreement before an exchange. Every rank all-gathers its status
+// and the arguments the exchanges depend on. If a rank failed, or was called
+// with arguments other than rank 0's, every rank returns an error. Otherwise
+// the others would wait inside a collective that the failed rank never joins:
+// NCCL has no timeout of its own. A failed rank returns its own code and
+// message; the others return ISDF_ERR_COMM naming it, or ISDF_ERR_ARG when the
+// arguments differ.
+constexpr int kStatusWords = (int)(Transport::kStatusBytes / sizeof(long long));
+struct RankStatus {
+  long long v[kStatusWords] = {};  // v[0]: status; v[1..n): the shared arguments
+  int n = 1;
+  void add(long long x) {
+    if (n < kStatusWords) v[n++] = x;
+  }
+  void add(double x) {
+    long long b;
+    std::memcpy(&b, &x, sizeof(b));
+    add(b);
+  }
+};
+
+int agree(Transport* T, int rc, RankStatus mine, cudaStream_t s, const char* stage) {
+  const int p = T->size;
+  if (!T->status) return record_error(ISDF_ERR_COMM, "sharded solve: no status buffer");
+  mine.v[0] = rc;
+  constexpr size_t sz = Transport::kStatusBytes;
+  static_assert(sizeof(RankStatus::v) == sz, "status record size");
+  char* send = T->status + (size_t)p * sz;
+  ISDF_CUDA(cudaMemcpyAsync(send, mine.v, sz, cudaMemcpyHostToDevice, s));
+  std::vector<size_t> cnt(p, sz), dsp(p);
+  for (int q = 0; q < p; ++q) dsp[q] = (size_t)q * sz;
+  ISDF_TRY(T->allgatherv(send, sz, T->status, cnt.data(), dsp.data(), s));
+  std::vector<long long> all((size_t)p * kStatusWords);
+  ISDF_CUDA(cudaMemcpyAsync(all.data(), T->status, (size_t)p * sz, cudaMemcpyDeviceToHost, s));
+  ISDF_CUDA(cudaStreamSynchronize(s));
+  if (rc != ISDF_OK) return rc;
+  char msg[160];
+  for (int q = 0; q < p; ++q) {
+    const long long* w = all.data() + (size_t)q * kStatusWords;
+    if (w[0] != ISDF_OK) {
+      std::snprintf(msg, sizeof(msg), "%s: rank %d failed (status %lld)", stage, q, w[0]);
+      return record_error(ISDF_ERR_COMM, msg);
+    }
+  }
+  for (int q = 1; q < p; ++q) {
+    const long long* w = all.data() + (size_t)q * kStatusWords;
+    for (int k = 1; k < mine.n; ++k)
+      if (w[k] != all[k]) {
+        std::snprintf(msg, sizeof(msg),
+                      "%s: rank %d was called with other arguments than rank 0 (argument %d)",
+                      stage, q, k);
+        return record_error(ISDF_ERR_ARG, msg);
+      }
+  }
+  return ISDF_OK;
+}
+
 struct Stopwatch {
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
   double ms() const {
@@ -116,6 +174,40 @@ static size_t sharded_workspace_bytes(long long ng, long long cnt, int nstate, i
   return a.off + std::max(sel, fit) + 4096;
 }
 
+// The argument checks of the sharded solve; *ng and *rk are set on success.
+static int check_sharded_args(const isdf_domain_t* dom, const double* d_psirow,
+                              const double* d_theta, const int* piv, int p, int nocc, int nstate,
+                              int nv1, int nc1, int nv2, int nc2, int mu_points, int layout,
+                              int kmeans_max_iter, const isdf_options_t& opt, long long* ng,
+                              int* rk) {
+  if (!dom || !d_psirow || !d_theta || !piv) return record_error(ISDF_ERR_ARG, "null pointer");
+  if (dom->num_grid[0] <= 0 || dom->num_grid[1] <= 0 || dom->num_grid[2] <= 0)
+    return record_error(ISDF_ERR_ARG, "empty grid");
+  *ng = (long long)dom->num_grid[0] * dom->num_grid[1] * dom->num_grid[2];
+  if (*ng < p) return record_error(ISDF_ERR_ARG, "sharded solve: fewer grid points than ranks");
+  ISDF_TRY(check_state_ranges(nocc, nstate, nv1, nc1, nv2, nc2));
+  if (kmeans_max_iter < 0) return record_error(ISDF_ERR_ARG, "negative K-means iteration cap");
+  *rk = mu_points == 0 ? default_mu(nv1, nc1, nv2, nc2) : mu_points;
+  if (*rk <= 0 || *rk > *ng) return record_error(ISDF_ERR_ARG, "mu outside [1, Ng]");
+  if (*rk > kKmeansMaxMu) return record_error(ISDF_ERR_UNSUPPORTED, "mu above the K-means limit");
+  if (layout != ISDF_THETA_ROWS && layout != ISDF_THETA_CYCLIC)
+    return record_error(ISDF_ERR_ARG, "unknown theta layout");
+  if (opt.precision != ISDF_PRECISION_FP64 && opt.precision != ISDF_PRECISION_MIXED)
+    return record_error(ISDF_ERR_ARG, "unknown precision");
+  if (opt.precision == ISDF_PRECISION_MIXED && (opt.mixed_slices < 5 || opt.mixed_slices > 7))
+    return record_error(ISDF_ERR_ARG, "mixed_slices must be 5, 6 or 7");
+  if (opt.refine_steps != 0)
+    return record_error(ISDF_ERR_UNSUPPORTED,
+                        "refine_steps must be 0: FP64 refinement of the theta solve is not built");
+  return ISDF_OK;
+}
+
+// The grid and the K-means arguments every rank must share.
+static void add_domain(RankStatus* st, const isdf_domain_t* dom) {
+  for (int i = 0; i < 3; ++i) st->add((long long)(dom ? dom->num_grid[i] : 0));
+  for (int i = 0; i < 3; ++i) st->add(dom ? dom->length[i] : 0.0);
+}
+
 int solve_sharded(Transport* T, const isdf_domain_t* dom, const double* d_psirow, int nocc,
                   int nstate, int nv1, int nc1, int nv2, int nc2, int mu_points, double* d_theta,
                   int layout, int* piv, int kmeans_max_iter, const isdf_options_t* opt_in,
@@ -126,33 +218,32 @@ int solve_sharded(Transport* T, const isdf_domain_t* dom, const double* d_psirow
   if (opt_in) opt = *opt_in;
   isdf_report_t rep;
   std::memset(&rep, 0, sizeof(rep));
-  if (!T || !dom || !d_psirow || !d_theta || !piv) return record_error(ISDF_ERR_ARG, "null pointer");
-  if (dom->num_grid[0] <= 0 || dom->num_grid[1] <= 0 || dom->num_grid[2] <= 0)
-    return record_error(ISDF_ERR_ARG, "empty grid");
-  const long long ng = (long long)dom->num_grid[0] * dom->num_grid[1] * dom->num_grid[2];
+  if (!T) return record_error(ISDF_ERR_ARG, "null comm");
   const int p = T->size, r = T->rank;
-  if (ng < p) return record_error(ISDF_ERR_ARG, "sharded solve: fewer grid points than ranks");
-  ISDF_TRY(check_state_ranges(nocc, nstate, nv1, nc1, nv2, nc2));
-  if (kmeans_max_iter < 0) return record_error(ISDF_ERR_ARG, "negative K-means iteration cap");
-  const int rk = mu_points == 0 ? default_mu(nv1, nc1, nv2, nc2) : mu_points;
-  if (rk <= 0 || rk > ng) return record_error(ISDF_ERR_ARG, "mu outside [1, Ng]");
-  if (rk > kKmeansMaxMu) return record_error(ISDF_ERR_UNSUPPORTED, "mu above the K-means limit");
-  if (layout != ISDF_THETA_ROWS && layout != ISDF_THETA_CYCLIC)
-    return record_error(ISDF_ERR_ARG, "unknown theta layout");
-  if (opt.precision != ISDF_PRECISION_FP64 && opt.precision != ISDF_PRECISION_MIXED)
-    return record_error(ISDF_ERR_ARG, "unknown precision");
-  if (opt.precision == ISDF_PRECISION_MIXED && (opt.mixed_slices < 5 || opt.mixed_slices > 7))
-    return record_error(ISDF_ERR_ARG, "mixed_slices must be 5, 6 or 7");
-  if (opt.refine_steps != 0)
-    return record_error(ISDF_ERR_UNSUPPORTED,
-                        "refine_steps must be 0: FP64 refinement of the theta solve is not built");
-  rep.rk_requested = rk;
-  const long long start = block_start(ng, p, r), cnt = block_count(ng, p, r);
-
-  Arena arena;
-  ISDF_TRY(T->acquire(sharded_workspace_bytes(ng, cnt, nstate, rk, p, opt.precision, layout),
-                      &arena));
+  // Every check below ends in the agreement rather than in an early return,
+  // so that a rank that fails them still meets the others there.
+  int rc = T->ensure_stream();
   cudaStream_t s = opt.stream ? (cudaStream_t)opt.stream : T->stream;
+  long long ng = 0;
+  int rk = 0;
+  if (rc == ISDF_OK)
+    rc = check_sharded_args(dom, d_psirow, d_theta, piv, p, nocc, nstate, nv1, nc1, nv2, nc2,
+                            mu_points, layout, kmeans_max_iter, opt, &ng, &rk);
+  RankStatus mine;
+  add_domain(&mine, dom);
+  for (long long x : {(long long)nocc, (long long)nstate, (long long)nv1, (long long)nc1,
+                      (long long)nv2, (long long)nc2, (long long)rk, (long long)kmeans_max_iter,
+                      (long long)layout, (long long)opt.precision, (long long)opt.mixed_slices,
+                      opt.rand_seed, (long long)opt.kmeans_warm_start})
+    mine.add(x);
+  rep.rk_requested = rk;
+  const long long start = rc == ISDF_OK ? block_start(ng, p, r) : 0;
+  const long long cnt = rc == ISDF_OK ? block_count(ng, p, r) : 0;
+  Arena arena;
+  if (rc == ISDF_OK)
+    rc = T->acquire(sharded_workspace_bytes(ng, cnt, nstate, rk, p, opt.precision, layout),
+                    &arena);
+  ISDF_TRY(agree(T, rc, mine, s, "sharded solve"));
   double* d_w = arena.take<double>((size_t)ng);
   double* d_wloc = arena.take<double>((size_t)cnt);
   const size_t mark = arena.off;
@@ -242,21 +333,25 @@ int solve_sharded(Transport* T, const isdf_domain_t* dom, const double* d_psirow
   fa.d_theta = rows_out;
   fa.d_psimu = d_Bm;
   FitResult fr;
-  int rc = opt.precision == ISDF_PRECISION_MIXED ? fit_mixed(fa, arena, s, &fr, opt.mixed_slices)
-                                                 : fit_fp64(fa, arena, s, &fr);
+  rc = opt.precision == ISDF_PRECISION_MIXED ? fit_mixed(fa, arena, s, &fr, opt.mixed_slices)
+                                             : fit_fp64(fa, arena, s, &fr);
   rep.chol_info = fr.chol_info;
   rep.kernel_launches += fr.launches + 2;
   rep.t_zct_ms = fr.t_zct_ms;
   rep.t_chol_ms = fr.t_chol_ms;
   rep.t_solve_ms = fr.t_solve_ms;
   rep.t_gemm_ms = fr.t_gemm_ms > 0.f ? fr.t_gemm_ms : fr.t_solve_ms;
+  if (rc == ISDF_OK && rke < rk) {
+    const cudaError_t e = cudaMemsetAsync(rows_out + (size_t)rke * cnt, 0,
+                                          sizeof(double) * (size_t)(rk - rke) * cnt, s);
+    if (e != cudaSuccess) rc = record_cuda_error(e, "cudaMemsetAsync (theta tail)", __FILE__, __LINE__);
+  }
+  // theta's all-to-all is the one exchange after the fit
+  if (layout == ISDF_THETA_CYCLIC) rc = agree(T, rc, mine, s, "sharded solve (theta exchange)");
   if (rc != ISDF_OK) {
     if (rep_out) *rep_out = rep;
     return rc;
   }
-  if (rke < rk)
-    ISDF_CUDA(cudaMemsetAsync(rows_out + (size_t)rke * cnt, 0,
-                              sizeof(double) * (size_t)(rk - rke) * cnt, s));
 
   // 5. the reference's column-cyclic layout
   if (layout == ISDF_THETA_CYCLIC) {
@@ -289,15 +384,32 @@ int solve_sharded(Transport* T, const isdf_domain_t* dom, const double* d_psirow
 int kmeans_select_sharded(Transport* T, const isdf_domain_t* dom, const double* d_w, int mu,
                           int max_iter, long long rand_seed, int* piv, int* rk_eff, int* iters,
                           int* npt) {
-  if (!T || !dom || !d_w || !piv) return record_error(ISDF_ERR_ARG, "null pointer");
-  if (dom->num_grid[0] <= 0 || dom->num_grid[1] <= 0 || dom->num_grid[2] <= 0)
-    return record_error(ISDF_ERR_ARG, "empty grid");
-  if (max_iter < 0) return record_error(ISDF_ERR_ARG, "negative K-means iteration cap");
-  const long long ng = (long long)dom->num_grid[0] * dom->num_grid[1] * dom->num_grid[2];
-  if (mu <= 0 || mu > ng) return record_error(ISDF_ERR_ARG, "mu outside [1, Ng]");
-  if (mu > kKmeansMaxMu) return record_error(ISDF_ERR_UNSUPPORTED, "mu above the K-means limit");
+  if (!T) return record_error(ISDF_ERR_ARG, "null comm");
+  // as in solve_sharded: the checks end in the ranks' agreement
+  int rc = T->ensure_stream();
+  long long ng = 0;
+  if (rc == ISDF_OK) {
+    if (!dom || !d_w || !piv) {
+      rc = record_error(ISDF_ERR_ARG, "null pointer");
+    } else if (dom->num_grid[0] <= 0 || dom->num_grid[1] <= 0 || dom->num_grid[2] <= 0) {
+      rc = record_error(ISDF_ERR_ARG, "empty grid");
+    } else {
+      ng = (long long)dom->num_grid[0] * dom->num_grid[1] * dom->num_grid[2];
+      if (max_iter < 0)
+        rc = record_error(ISDF_ERR_ARG, "negative K-means iteration cap");
+      else if (mu <= 0 || mu > ng)
+        rc = record_error(ISDF_ERR_ARG, "mu outside [1, Ng]");
+      else if (mu > kKmeansMaxMu)
+        rc = record_error(ISDF_ERR_UNSUPPORTED, "mu above the K-means limit");
+    }
+  }
+  RankStatus mine;
+  add_domain(&mine, dom);
+  for (long long x : {(long long)mu, (long long)max_iter, rand_seed}) mine.add(x);
   Arena arena;
-  ISDF_TRY(T->acquire(kmeans_shard_workspace_bytes(ng, mu, T->size) + 4096, &arena));
+  if (rc == ISDF_OK)
+    rc = T->acquire(kmeans_shard_workspace_bytes(ng, mu, T->size) + 4096, &arena);
+  ISDF_TRY(agree(T, rc, mine, T->stream, "sharded K-means selection"));
   KmeansArgs ka;
   ka.d_w = d_w;
   ka.ng = ng;

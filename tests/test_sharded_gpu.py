@@ -10,8 +10,15 @@ waits on another rank, so p ranks on one GPU are safe. Checked:
     bit when the pivots agree, FP64 and mixed), the reference's column-cyclic
     layout, and the NCCL transport at one rank;
   * a rank that never reaches a collective: the others fail with
-    ISDF_ERR_COMM after the group's timeout, on the host."""
+    ISDF_ERR_COMM after the group's timeout, on the host;
+  * a rank whose own checks fail, or that was called with other arguments
+    than rank 0: every rank fails at the agreement before the first exchange,
+    without waiting for the timeout;
+  * the callback transport (isdf_comm_create_callbacks, the path for a caller
+    with its own collectives) with Python collectives over host threads: the
+    same theta columns as the one-rank solve."""
 import threading
+import time
 
 import numpy as np
 import pytest
@@ -224,3 +231,167 @@ def test_missing_rank_fails_on_the_host(torch_cuda):
     torch.cuda.synchronize()  # the context is intact
     th1, piv1, _ = _single(torch, psi, dom, a, mu, iters, isdf.Options())
     assert np.isfinite(th1).all()
+
+
+def _small_case():
+    g = load_golden("small_s1s2")
+    psi = g["psi"]
+    a = (int(g["nocc"]), int(g["nv1"]), int(g["nc1"]), int(g["nv2"]), int(g["nc2"]))
+    dom = isdf.Domain(length=tuple(g["length"]), num_grid=tuple(int(x) for x in g["ng"]))
+    return psi, a, dom, int(g["rk_requested"]), int(g["iters"])
+
+
+def _solve_code(torch, c, psi, a, dom, p, r, mu, iters, layout=isdf.THETA_ROWS):
+    start, cnt, d_rows = _split_rows(torch, psi, p, r)
+    shape = (mu, cnt) if layout == isdf.THETA_ROWS else (mu // p + 1, psi.shape[0])
+    d_th = torch.empty(shape, dtype=torch.float64, device="cuda")
+    piv = np.zeros(psi.shape[0], dtype=np.int32)
+    with pytest.raises(isdf.IsdfError) as ei:
+        isdf.solve_sharded(c, d_rows, dom, a[0], psi.shape[1], *a[1:], mu, d_th, piv, iters,
+                           layout=layout)
+    return ei.value.code, str(ei.value)
+
+
+@pytest.mark.parametrize("layout", [isdf.THETA_ROWS, isdf.THETA_CYCLIC])
+def test_failed_rank_fails_every_rank(torch_cuda, layout):
+    """Rank 1 is called with a negative K-means iteration cap: it returns
+    ISDF_ERR_ARG, and ranks 0 and 2 return ISDF_ERR_COMM naming rank 1, at the
+    agreement before the first exchange, well inside the group's 30 s timeout."""
+    torch = torch_cuda
+    psi, a, dom, mu, iters = _small_case()
+    p = 3
+
+    def rank(r, c):
+        return _solve_code(torch, c, psi, a, dom, p, r, mu, -1 if r == 1 else iters, layout)
+
+    t0 = time.monotonic()
+    out = run_ranks(p, rank, timeout_s=30.0)
+    took = time.monotonic() - t0
+    assert [o[0] for o in out] == [isdf.ISDF_ERR_COMM, isdf.ISDF_ERR_ARG, isdf.ISDF_ERR_COMM]
+    assert "negative K-means iteration cap" in out[1][1]
+    assert all("rank 1 failed" in out[q][1] for q in (0, 2))
+    assert took < 20.0, took
+    th1, piv1, _ = _single(torch, psi, dom, a, mu, iters, isdf.Options())
+    assert np.isfinite(th1).all()  # the context is intact
+
+
+def test_ranks_with_other_arguments_fail(torch_cuda):
+    """Rank 2 asks for one interpolation point fewer than ranks 0 and 1: every
+    rank returns ISDF_ERR_ARG before the first exchange. The sharded K-means
+    selection checks its arguments the same way."""
+    torch = torch_cuda
+    psi, a, dom, mu, iters = _small_case()
+    p = 3
+
+    def rank(r, c):
+        return _solve_code(torch, c, psi, a, dom, p, r, mu - 1 if r == 2 else mu, iters)
+
+    out = run_ranks(p, rank, timeout_s=30.0)
+    assert [o[0] for o in out] == [isdf.ISDF_ERR_ARG] * 3
+    assert all("other arguments than rank 0" in o[1] for o in out)
+
+    w = torch.from_numpy(load_golden("small_s1s2")["weight"].copy()).cuda()
+
+    def sel(r, c):
+        with pytest.raises(isdf.IsdfError) as ei:
+            isdf.kmeans_select_sharded(c, dom, w, mu, iters + (r == 0))
+        return ei.value.code
+
+    assert run_ranks(2, sel, timeout_s=30.0) == [isdf.ISDF_ERR_ARG] * 2
+
+
+class _DeviceBytes:
+    """`n` bytes of device memory at a raw address, for torch.as_tensor."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, False),
+                                         "version": 2, "strides": None}
+
+
+class _ThreadCollectives:
+    """A caller's own collectives for ranks on host threads of one process: the
+    sender's stream is synchronised before its buffer is published, every
+    rank copies what it needs on its own stream and synchronises it, and a
+    second barrier keeps send buffers alive until all ranks have read them."""
+
+    def __init__(self, torch, size):
+        self.torch, self.size = torch, size
+        self.barrier = threading.Barrier(size, timeout=30.0)
+        self.slots = [None] * size
+        self.calls = [0] * size
+
+    def _bytes(self, ptr, n):
+        return self.torch.as_tensor(_DeviceBytes(ptr, n), device="cuda")
+
+    def _run(self, rank, stream, slot, copies):
+        torch = self.torch
+        s = torch.cuda.ExternalStream(stream)
+        s.synchronize()
+        self.slots[rank] = slot
+        self.barrier.wait()
+        with torch.cuda.stream(s):
+            for dst, src, n in copies():
+                if n:
+                    self._bytes(dst, n).copy_(self._bytes(src, n))
+        s.synchronize()
+        self.barrier.wait()
+        self.calls[rank] += 1
+
+    def comm(self, rank):
+        def allgatherv(d_send, send_bytes, d_recv, counts, displs, stream):
+            self._run(rank, stream, d_send,
+                      lambda: [(d_recv + displs[q], self.slots[q], counts[q])
+                               for q in range(self.size)])
+
+        def alltoallv(d_send, scounts, sdispls, d_recv, rcounts, rdispls, stream):
+            self._run(rank, stream, (d_send, sdispls),
+                      lambda: [(d_recv + rdispls[q], self.slots[q][0] + self.slots[q][1][rank],
+                                rcounts[q]) for q in range(self.size)])
+
+        return isdf.Comm.callbacks(allgatherv, alltoallv, rank, self.size)
+
+
+def test_callback_transport(torch_cuda):
+    """Two ranks whose collectives are the caller's own (Python callbacks over
+    host threads) give the one-rank solve's theta columns in the reference's
+    cyclic layout, and its piv."""
+    torch = torch_cuda
+    g = load_golden("small_mu0")
+    psi = g["psi"]
+    a = (int(g["nocc"]), int(g["nv1"]), int(g["nc1"]), int(g["nv2"]), int(g["nc2"]))
+    dom = isdf.Domain(length=tuple(g["length"]), num_grid=tuple(int(x) for x in g["ng"]))
+    mu, iters, p = 46, int(g["iters"]), 2
+    th1, piv1, _ = _single(torch, psi, dom, a, mu, iters, isdf.Options())
+    coll = _ThreadCollectives(torch, p)
+    comms = [coll.comm(r) for r in range(p)]
+    out, err = [None] * p, [None] * p
+
+    def body(r):
+        try:
+            start, cnt, d_rows = _split_rows(torch, psi, p, r)
+            w = mu // p + (1 if r < mu % p else 0)
+            d_th = torch.full((w, psi.shape[0]), float("nan"), dtype=torch.float64, device="cuda")
+            piv = np.zeros(psi.shape[0], dtype=np.int32)
+            isdf.solve_sharded(comms[r], d_rows, dom, a[0], psi.shape[1], *a[1:], mu, d_th, piv,
+                               iters, layout=isdf.THETA_CYCLIC)
+            out[r] = (d_th.cpu().numpy().T, piv)
+        except BaseException as e:  # noqa: BLE001 - handed to the main thread
+            err[r] = e
+            coll.barrier.abort()
+
+    th = [threading.Thread(target=body, args=(r,)) for r in range(p)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for c in comms:
+        c.close()
+    for e in err:
+        if e is not None:
+            raise e
+    for r, (cols, piv) in enumerate(out):
+        assert np.array_equal(piv, piv1)
+        assert np.array_equal(cols, th1[:, r::p]), r
+    assert coll.calls[0] == coll.calls[1] > 2
+    record_parity("sharded solve small_mu0, callback transport",
+                  "theta columns vs one rank (p = 2)", "bit-identical")
