@@ -695,28 +695,52 @@ __global__ void __launch_bounds__(256) k_hist(const int* __restrict__ label, int
   for (int l = threadIdx.x; l < rk; l += blockDim.x) row[l] = sh[l];
 }
 
-// Per label: exclusive scan over tiles (in place) and the member count.
-__global__ void __launch_bounds__(256) k_hist_scan(int* __restrict__ hist, int ntiles,
-                                                   const KmState* st, int* __restrict__ members) {
+// Per label: exclusive scan over tiles (in place) and the member count. A
+// block holds 32 labels (one per lane) and kScanWarps warps, each over a
+// contiguous range of tiles: the warps' range sums, their exclusive prefix in
+// shared memory, then each warp rewrites its range from that prefix. One
+// thread per label walking all tiles left the scan bound by the latency of
+// its ~ntiles/16 dependent load batches.
+constexpr int kScanWarps = 16;
+
+__global__ void __launch_bounds__(32 * kScanWarps) k_hist_scan(int* __restrict__ hist, int ntiles,
+                                                               const KmState* st,
+                                                               int* __restrict__ members) {
   if (st->done) return;
   const int rk = st->rk;
-  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int l = blockIdx.x * 32 + lane;
+  const int per = (ntiles + kScanWarps - 1) / kScanWarps;
+  const int t0 = w * per, t1 = min(t0 + per, ntiles);
+  __shared__ int part[kScanWarps][32];
+  constexpr int kB = 8;  // loads batched ahead of the additions and stores
+  int sum = 0;
+  if (l < rk) {
+    for (int t = t0; t < t1; t += kB) {
+      int v[kB];
+#pragma unroll
+      for (int u = 0; u < kB; ++u) v[u] = t + u < t1 ? hist[(size_t)(t + u) * rk + l] : 0;
+#pragma unroll
+      for (int u = 0; u < kB; ++u) sum += v[u];
+    }
+  }
+  part[w][lane] = sum;
+  __syncthreads();
   if (l >= rk) return;
-  // loads batched ahead of the stores (in place: the compiler cannot reorder
-  // a load past an earlier store to the same array on its own)
-  constexpr int kB = 16;
   int run = 0;
-  for (int t0 = 0; t0 < ntiles; t0 += kB) {
+  for (int q = 0; q < w; ++q) run += part[q][lane];
+  for (int t = t0; t < t1; t += kB) {
     int v[kB];
 #pragma unroll
-    for (int u = 0; u < kB; ++u) v[u] = t0 + u < ntiles ? hist[(size_t)(t0 + u) * rk + l] : 0;
+    for (int u = 0; u < kB; ++u) v[u] = t + u < t1 ? hist[(size_t)(t + u) * rk + l] : 0;
 #pragma unroll
     for (int u = 0; u < kB; ++u) {
-      if (t0 + u < ntiles) hist[(size_t)(t0 + u) * rk + l] = run;
+      if (t + u < t1) hist[(size_t)(t + u) * rk + l] = run;
       run += v[u];
     }
   }
-  members[l] = run;
+  // the last warp's prefix covers every tile (its own range may be empty)
+  if (w == kScanWarps - 1) members[l] = run;
 }
 
 // Exclusive scan of the member counts (one block): start[l].
@@ -950,6 +974,9 @@ __global__ void __launch_bounds__(1024) k_centroids(double4* __restrict__ sums, 
     unsigned* tmp = cmax + ncells;
     for (int c = threadIdx.x; c < ncells; c += blockDim.x) cmax[c] = 0u;
     __syncthreads();
+    // the largest move: one atomic per warp (the moves are >= 0, so their bit
+    // patterns order as the values do)
+    unsigned long long mx = 0ull;
     for (int i = threadIdx.x; i < rk; i += blockDim.x) {
       double4 s = sums[i];
       const double4 o = cen[i];
@@ -960,9 +987,12 @@ __global__ void __launch_bounds__(1024) k_centroids(double4* __restrict__ sums, 
       const double d2 = __dadd_ru(__dadd_ru(__dmul_ru(dx, dx), __dmul_ru(dy, dy)), __dmul_ru(dz, dz));
       const double sh = __dmul_ru(__dsqrt_ru(d2), 1.0 + 1e-13);
       shift[i] = sh;
-      atomicMax(&st->maxshift_bits, (unsigned long long)__double_as_longlong(sh));
+      mx = max(mx, (unsigned long long)__double_as_longlong(sh));
       atomicMax(&cmax[cell_of[i]], __float_as_uint(__double2float_ru(sh)));
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(&st->maxshift_bits, mx);
     __syncthreads();
     // 3^3 and 5^3 neighbourhood maxima as separable passes (x, y, z)
     unsigned* t2 = tmp + ncells;
@@ -1527,7 +1557,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
     for (int it = 0; it < kIterChunk; ++it) {
       k_iter_begin<<<1, 1, 0, stream>>>(b.st, max_f, args.max_iter);
       k_hist<<<ntiles, 256, hist_smem, stream>>>(b.label, n, b.st, b.hist);
-      k_hist_scan<<<grid_for(mu, 256), 256, 0, stream>>>(b.hist, ntiles, b.st, b.members);
+      k_hist_scan<<<(mu + 31) / 32, 32 * kScanWarps, 0, stream>>>(b.hist, ntiles, b.st, b.members);
       k_label_start<<<1, 1024, 0, stream>>>(b.members, b.st, b.start);
       k_scatter<<<ntiles, 128, scatter_smem, stream>>>(b.label, n, b.st, b.hist, b.start, b.px,
                                                        b.py, b.pz, b.pw, b.sorted);
@@ -1558,7 +1588,7 @@ int kmeans_select(const KmeansArgs& args, Arena& arena, cudaStream_t stream, Kme
   auto launch_chunk_sharded = [&]() -> int {
     for (int it = 0; it < kIterChunk; ++it) {
       k_hist<<<ntl, 256, hist_smem, stream>>>(b.label + lo, cnt, b.st, b.hist);
-      k_hist_scan<<<grid_for(mu, 256), 256, 0, stream>>>(b.hist, ntl, b.st, b.members);
+      k_hist_scan<<<(mu + 31) / 32, 32 * kScanWarps, 0, stream>>>(b.hist, ntl, b.st, b.members);
       k_label_start<<<1, 1024, 0, stream>>>(b.members, b.st, b.start);
       k_scatter<<<ntl, 128, scatter_smem, stream>>>(b.label + lo, cnt, b.st, b.hist, b.start,
                                                     b.px + lo, b.py + lo, b.pz + lo, b.pw + lo,
