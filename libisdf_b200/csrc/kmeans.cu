@@ -769,10 +769,12 @@ __global__ void __launch_bounds__(1024) k_label_start(const int* __restrict__ me
 }
 
 // One tile per block: 128 threads stage the tile's labels in shared memory,
-// then one warp walks them in order and scatters every point to its stable
-// position (peers with equal labels share one running offset). What lands
-// there is the point's (w x, w y, w z, w), so that the per-cluster fold reads
-// its members contiguously.
+// then one warp walks them in order and gives every point its stable position
+// (peers with equal labels share one running offset), written over its label.
+// All 128 threads then move the points there: what lands is the point's
+// (w x, w y, w z, w), so that the per-cluster fold reads its members
+// contiguously. The walk has no global loads in its dependent chain; the
+// point loads of the move are independent of one another.
 __global__ void __launch_bounds__(128) k_scatter(const int* __restrict__ label, int n,
                                                  const KmState* st, const int* __restrict__ hist,
                                                  const int* __restrict__ start,
@@ -785,45 +787,34 @@ __global__ void __launch_bounds__(128) k_scatter(const int* __restrict__ label, 
   extern __shared__ int sm_scatter[];
   const int rk = st->rk;
   int* run = sm_scatter;
-  int* lab = sm_scatter + rk;
+  int* lab = sm_scatter + rk;  // the tile's labels, then the points' positions
   const int* row = hist + (size_t)blockIdx.x * rk;
   for (int l = threadIdx.x; l < rk; l += 128) run[l] = start[l] + row[l];
   const int base = blockIdx.x * kTile;
   const int cnt = min(kTile, n - base);
   for (int k = threadIdx.x; k < cnt; k += 128) lab[k] = label[base + k];
   __syncthreads();
-  if (threadIdx.x >= 32) return;
-  const int lane = threadIdx.x;
-  // the point values of the next 32 are loaded while this 32 is placed
-  double nw = 0.0, nx = 0.0, ny = 0.0, nz = 0.0;
-  if (lane < cnt) {
-    const int p = base + lane;
-    nw = pw[p];
-    nx = px[p];
-    ny = py[p];
-    nz = pz[p];
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    for (int c = 0; c < cnt; c += 32) {
+      const int k = c + lane;
+      const bool ok = k < cnt;
+      const int l = ok ? lab[k] : -1;
+      const unsigned peers = __match_any_sync(0xffffffffu, l);
+      const int b = ok ? run[l] : 0;
+      __syncwarp();
+      if (ok) {
+        lab[k] = b + __popc(peers & ((1u << lane) - 1u));
+        if (lane == __ffs(peers) - 1) run[l] = b + __popc(peers);
+      }
+      __syncwarp();
+    }
   }
-  for (int c = 0; c < cnt; c += 32) {
-    const int k = c + lane;
-    const bool ok = k < cnt;
-    const double w = nw, x = nx, y = ny, z = nz;
-    if (k + 32 < cnt) {
-      const int p = base + k + 32;
-      nw = pw[p];
-      nx = px[p];
-      ny = py[p];
-      nz = pz[p];
-    }
-    const int l = ok ? lab[k] : -1;
-    const unsigned peers = __match_any_sync(0xffffffffu, l);
-    const int b = ok ? run[l] : 0;
-    __syncwarp();
-    if (ok) {
-      const int r = __popc(peers & ((1u << lane) - 1u));
-      sorted[b + r] = make_double4(rmul(w, x), rmul(w, y), rmul(w, z), w);
-      if (lane == __ffs(peers) - 1) run[l] = b + __popc(peers);
-    }
-    __syncwarp();
+  __syncthreads();
+  for (int k = threadIdx.x; k < cnt; k += 128) {
+    const int p = base + k;
+    const double w = pw[p];
+    sorted[lab[k]] = make_double4(rmul(w, px[p]), rmul(w, py[p]), rmul(w, pz[p]), w);
   }
 }
 

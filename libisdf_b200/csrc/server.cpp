@@ -298,6 +298,20 @@ using namespace isdf_b200;
 namespace isdf_b200 {
 namespace {
 int set_err(int code, const char* msg) { return record_error(code, msg); }
+
+// Runs a C entry point's body and turns what the standard library may throw
+// (host allocation, thread or mutex errors) into a status, so that no
+// exception crosses the C ABI.
+template <class F>
+int guarded(F&& body) {
+  try {
+    return body();
+  } catch (const std::exception& e) {
+    return record_error(ISDF_ERR_NOMEM, e.what());
+  } catch (...) {
+    return record_error(ISDF_ERR_CUDA, "server: unknown exception");
+  }
+}
 }  // namespace
 }  // namespace isdf_b200
 
@@ -315,200 +329,231 @@ void isdf_server_default_config(isdf_server_config_t* cfg) {
 }
 
 int isdf_server_create(const isdf_server_config_t* cfg_in, void** out) {
-  if (!out) return record_error(ISDF_ERR_ARG, "server: null output");
-  isdf_server_config_t cfg;
-  isdf_server_default_config(&cfg);
-  if (cfg_in) cfg = *cfg_in;
-  if (cfg.slots < 1 || cfg.slots > 64) return record_error(ISDF_ERR_ARG, "server: slots in [1, 64]");
-  if (cfg.batch_small < 0 || cfg.batch_small > 1024)
-    return record_error(ISDF_ERR_ARG, "server: batch_small in [0, 1024]");
-  if (cudaSetDevice(cfg.device) != cudaSuccess) return record_error(ISDF_ERR_ARG, "server: device");
-  if (cfg.hbm_budget_bytes == 0) {
-    size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess)
-      return record_error(ISDF_ERR_CUDA, "server: cudaMemGetInfo failed");
-    cfg.hbm_budget_bytes = free_b / 2;
-  }
-  Server* s = new Server();
-  s->cfg = cfg;
-  cudaMemPoolProps props;
-  std::memset(&props, 0, sizeof(props));
-  props.allocType = cudaMemAllocationTypePinned;
-  props.location.type = cudaMemLocationTypeDevice;
-  props.location.id = cfg.device;
-  if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess) {
-    delete s;
-    return record_error(ISDF_ERR_CUDA, "server: cudaMemPoolCreate failed");
-  }
-  unsigned long long keep = cfg.hbm_budget_bytes;
-  cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
-  for (int i = 0; i < cfg.slots; ++i) s->workers.emplace_back(worker, s, i);
-  if (cfg.batch_small > 0) {
-    s->batcher_active = true;
-    s->batcher = std::thread(batcher, s);
-  }
-  *out = s;
-  return ISDF_OK;
+  return guarded([&]() -> int {
+    if (!out) return record_error(ISDF_ERR_ARG, "server: null output");
+    isdf_server_config_t cfg;
+    isdf_server_default_config(&cfg);
+    if (cfg_in) cfg = *cfg_in;
+    if (cfg.slots < 1 || cfg.slots > 64)
+      return record_error(ISDF_ERR_ARG, "server: slots in [1, 64]");
+    if (cfg.batch_small < 0 || cfg.batch_small > 1024)
+      return record_error(ISDF_ERR_ARG, "server: batch_small in [0, 1024]");
+    if (cudaSetDevice(cfg.device) != cudaSuccess)
+      return record_error(ISDF_ERR_ARG, "server: device");
+    if (cfg.hbm_budget_bytes == 0) {
+      size_t free_b = 0, total_b = 0;
+      if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess)
+        return record_error(ISDF_ERR_CUDA, "server: cudaMemGetInfo failed");
+      cfg.hbm_budget_bytes = free_b / 2;
+    }
+    Server* s = new Server();
+    s->cfg = cfg;
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = cfg.device;
+    if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess) {
+      delete s;
+      return record_error(ISDF_ERR_CUDA, "server: cudaMemPoolCreate failed");
+    }
+    unsigned long long keep = cfg.hbm_budget_bytes;
+    cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    try {
+      for (int i = 0; i < cfg.slots; ++i) s->workers.emplace_back(worker, s, i);
+      if (cfg.batch_small > 0) {
+        s->batcher_active = true;
+        s->batcher = std::thread(batcher, s);
+      }
+    } catch (...) {  // a thread did not start: stop the ones that did
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+        s->batcher_active = false;
+      }
+      s->cv_work.notify_all();
+      for (auto& w : s->workers) w.join();
+      cudaMemPoolDestroy(s->pool);
+      delete s;
+      return record_error(ISDF_ERR_NOMEM, "server: a worker thread could not be started");
+    }
+    *out = s;
+    return ISDF_OK;
+  });
 }
 
 int isdf_server_submit(void* server, const isdf_request_t* req, long long* ticket) {
-  Server* s = static_cast<Server*>(server);
-  if (!s || !req || !ticket) return record_error(ISDF_ERR_ARG, "server: null argument");
-  if (!req->d_psi || !req->d_theta || !req->piv)
-    return record_error(ISDF_ERR_ARG, "server: request buffers");
-  const size_t fp = request_footprint(&req->dom, req->nstate, req->nv1, req->nc1, req->nv2,
-                                      req->nc2, req->mu_points, req->selector, req->check,
-                                      &req->opt);
-  if (fp > s->cfg.hbm_budget_bytes)
-    return record_error(ISDF_ERR_UNSUPPORTED, "server: request larger than the whole budget");
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    if (s->stopping) return record_error(ISDF_ERR_CANCELLED, "server: stopping");
-    if ((int)s->queue.size() >= s->cfg.max_queue) return record_error(ISDF_ERR_BUSY, "server: queue full");
-    Job j;
-    j.ticket = s->next_ticket++;
-    j.req = *req;
-    j.req.opt.stream = nullptr;
-    j.footprint = fp;
-    j.submit = Clock::now();
+  return guarded([&]() -> int {
+    Server* s = static_cast<Server*>(server);
+    if (!s || !req || !ticket) return record_error(ISDF_ERR_ARG, "server: null argument");
+    if (!req->d_psi || !req->d_theta || !req->piv)
+      return record_error(ISDF_ERR_ARG, "server: request buffers");
+    const size_t fp = request_footprint(&req->dom, req->nstate, req->nv1, req->nc1, req->nv2,
+                                        req->nc2, req->mu_points, req->selector, req->check,
+                                        &req->opt);
+    if (fp > s->cfg.hbm_budget_bytes)
+      return record_error(ISDF_ERR_UNSUPPORTED, "server: request larger than the whole budget");
     {
-      const isdf_domain_t& d = req->dom;
-      const long long ng = (long long)d.num_grid[0] * d.num_grid[1] * d.num_grid[2];
-      const int rk = req->mu_points == 0 ? default_mu(req->nv1, req->nc1, req->nv2, req->nc2)
-                                         : req->mu_points;
-      j.small = s->cfg.batch_small > 0 && req->selector == ISDF_SELECT_KMEANS &&
-                !req->opt.kmeans_warm_start && ng > 1 && ng <= kKmeansBatchMaxNg && rk > 0 &&
-                rk <= kKmeansBatchMaxMu && rk <= ng && req->kmeans_max_iter >= 0 &&
-                d.num_grid[0] > 0 && d.num_grid[1] > 0 && d.num_grid[2] > 0 &&
-                req->opt.refine_steps == 0 && req->nv1 >= 0 && req->nc1 >= 0 && req->nv2 >= 0 &&
-                req->nc2 >= 0 && req->nv1 + req->nc1 > 0 && req->nv2 + req->nc2 > 0 &&
-                req->nocc - req->nv1 >= 0 && req->nocc + req->nc1 <= req->nstate &&
-                req->nocc - req->nv2 >= 0 && req->nocc + req->nc2 <= req->nstate;
-      if (j.small) j.batch_bytes = kmeans_batch_workspace_bytes(ng, rk) + sizeof(double) * ng + 512;
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (s->stopping) return record_error(ISDF_ERR_CANCELLED, "server: stopping");
+      if ((int)s->queue.size() >= s->cfg.max_queue)
+        return record_error(ISDF_ERR_BUSY, "server: queue full");
+      Job j;
+      j.ticket = s->next_ticket++;
+      j.req = *req;
+      j.req.opt.stream = nullptr;
+      j.footprint = fp;
+      j.submit = Clock::now();
+      {
+        const isdf_domain_t& d = req->dom;
+        const long long ng = (long long)d.num_grid[0] * d.num_grid[1] * d.num_grid[2];
+        const int rk = req->mu_points == 0 ? default_mu(req->nv1, req->nc1, req->nv2, req->nc2)
+                                           : req->mu_points;
+        j.small = s->cfg.batch_small > 0 && req->selector == ISDF_SELECT_KMEANS &&
+                  !req->opt.kmeans_warm_start && ng > 1 && ng <= kKmeansBatchMaxNg && rk > 0 &&
+                  rk <= kKmeansBatchMaxMu && rk <= ng && req->kmeans_max_iter >= 0 &&
+                  d.num_grid[0] > 0 && d.num_grid[1] > 0 && d.num_grid[2] > 0 &&
+                  req->opt.refine_steps == 0 && req->nv1 >= 0 && req->nc1 >= 0 && req->nv2 >= 0 &&
+                  req->nc2 >= 0 && req->nv1 + req->nc1 > 0 && req->nv2 + req->nc2 > 0 &&
+                  req->nocc - req->nv1 >= 0 && req->nocc + req->nc1 <= req->nstate &&
+                  req->nocc - req->nv2 >= 0 && req->nocc + req->nc2 <= req->nstate;
+        if (j.small)
+          j.batch_bytes = kmeans_batch_workspace_bytes(ng, rk) + sizeof(double) * ng + 512;
+      }
+      std::memset(&j.rep, 0, sizeof(j.rep));
+      if (!s->any_submit) {
+        s->first_submit = j.submit;
+        s->any_submit = true;
+      }
+      *ticket = j.ticket;
+      s->jobs[j.ticket] = j;
+      if (j.small) s->small_queue.push_back(j.ticket);
+      else s->queue.push_back(j.ticket);
     }
-    std::memset(&j.rep, 0, sizeof(j.rep));
-    if (!s->any_submit) {
-      s->first_submit = j.submit;
-      s->any_submit = true;
-    }
-    *ticket = j.ticket;
-    s->jobs[j.ticket] = j;
-    if (j.small) s->small_queue.push_back(j.ticket);
-    else s->queue.push_back(j.ticket);
-  }
-  s->cv_work.notify_all();
-  return ISDF_OK;
+    s->cv_work.notify_all();
+    return ISDF_OK;
+  });
 }
 
 int isdf_server_poll(void* server, long long ticket, int* state, int* status, isdf_report_t* rep) {
-  Server* s = static_cast<Server*>(server);
-  if (!s) return record_error(ISDF_ERR_ARG, "server: null");
-  std::lock_guard<std::mutex> lk(s->mu);
-  auto it = s->jobs.find(ticket);
-  if (it == s->jobs.end()) return record_error(ISDF_ERR_ARG, "server: unknown ticket");
-  if (state) *state = it->second.state;
-  if (status) *status = it->second.status;
-  if (rep && it->second.state == 2) *rep = it->second.rep;
-  return ISDF_OK;
+  return guarded([&]() -> int {
+    Server* s = static_cast<Server*>(server);
+    if (!s) return record_error(ISDF_ERR_ARG, "server: null");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(ticket);
+    if (it == s->jobs.end()) return record_error(ISDF_ERR_ARG, "server: unknown ticket");
+    if (state) *state = it->second.state;
+    if (status) *status = it->second.status;
+    if (rep && it->second.state == 2) *rep = it->second.rep;
+    return ISDF_OK;
+  });
 }
 
 int isdf_server_wait(void* server, long long ticket, double timeout_ms, int* status,
                      isdf_report_t* rep) {
-  Server* s = static_cast<Server*>(server);
-  if (!s) return record_error(ISDF_ERR_ARG, "server: null");
-  std::unique_lock<std::mutex> lk(s->mu);
-  auto it = s->jobs.find(ticket);
-  if (it == s->jobs.end()) return record_error(ISDF_ERR_ARG, "server: unknown ticket");
-  auto done = [&] { return s->jobs[ticket].state == 2; };
-  if (timeout_ms < 0) s->cv_done.wait(lk, done);
-  else if (!s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), done))
-    return record_error(ISDF_ERR_TIMEOUT, "server: wait timed out");
-  Job& j = s->jobs[ticket];
-  if (status) *status = j.status;
-  if (rep) *rep = j.rep;
-  return ISDF_OK;
+  return guarded([&]() -> int {
+    Server* s = static_cast<Server*>(server);
+    if (!s) return record_error(ISDF_ERR_ARG, "server: null");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(ticket);
+    if (it == s->jobs.end()) return record_error(ISDF_ERR_ARG, "server: unknown ticket");
+    auto done = [&] { return s->jobs[ticket].state == 2; };
+    if (timeout_ms < 0) s->cv_done.wait(lk, done);
+    else if (!s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), done))
+      return record_error(ISDF_ERR_TIMEOUT, "server: wait timed out");
+    Job& j = s->jobs[ticket];
+    if (status) *status = j.status;
+    if (rep) *rep = j.rep;
+    return ISDF_OK;
+  });
 }
 
 int isdf_server_cancel(void* server, long long ticket) {
-  Server* s = static_cast<Server*>(server);
-  if (!s) return record_error(ISDF_ERR_ARG, "server: null");
-  std::lock_guard<std::mutex> lk(s->mu);
-  auto it = std::find(s->small_queue.begin(), s->small_queue.end(), ticket);
-  if (it != s->small_queue.end()) {
-    s->small_queue.erase(it);
-  } else {
-    auto qt = std::find(s->queue.begin(), s->queue.end(), ticket);
-    if (qt == s->queue.end() || s->jobs[ticket].selected)
-      return record_error(ISDF_ERR_ARG, "server: not queued (running or done)");
-    s->queue.erase(qt);
-  }
-  Job& j = s->jobs[ticket];
-  j.state = 2;
-  j.status = ISDF_ERR_CANCELLED;
-  j.finish = Clock::now();
-  s->cancelled++;
-  s->cv_done.notify_all();
-  return ISDF_OK;
+  return guarded([&]() -> int {
+    Server* s = static_cast<Server*>(server);
+    if (!s) return record_error(ISDF_ERR_ARG, "server: null");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = std::find(s->small_queue.begin(), s->small_queue.end(), ticket);
+    if (it != s->small_queue.end()) {
+      s->small_queue.erase(it);
+    } else {
+      auto qt = std::find(s->queue.begin(), s->queue.end(), ticket);
+      if (qt == s->queue.end() || s->jobs[ticket].selected)
+        return record_error(ISDF_ERR_ARG, "server: not queued (running or done)");
+      s->queue.erase(qt);
+    }
+    Job& j = s->jobs[ticket];
+    j.state = 2;
+    j.status = ISDF_ERR_CANCELLED;
+    j.finish = Clock::now();
+    s->cancelled++;
+    s->cv_done.notify_all();
+    return ISDF_OK;
+  });
 }
 
 int isdf_server_stats(void* server, isdf_server_stats_t* st) {
-  Server* s = static_cast<Server*>(server);
-  if (!s || !st) return record_error(ISDF_ERR_ARG, "server: null");
-  std::lock_guard<std::mutex> lk(s->mu);
-  std::memset(st, 0, sizeof(*st));
-  st->submitted = s->next_ticket - 1;
-  st->completed = s->completed;
-  st->failed = s->failed;
-  st->cancelled = s->cancelled;
-  st->p50_ms = percentile(s->latencies_ms, 0.50);
-  st->p99_ms = percentile(s->latencies_ms, 0.99);
-  double sum = 0;
-  for (double v : s->latencies_ms) sum += v;
-  st->mean_ms = s->latencies_ms.empty() ? 0.0 : sum / (double)s->latencies_ms.size();
-  const double span = s->any_submit && s->completed
-                          ? std::chrono::duration<double>(s->last_finish - s->first_submit).count()
-                          : 0.0;
-  st->solves_per_s = span > 0 ? (double)s->completed / span : 0.0;
-  st->peak_concurrency = s->peak_running;
-  st->peak_bytes = s->peak_bytes;
-  st->queued = (int)(s->queue.size() + s->small_queue.size());
-  st->running = s->running;
-  return ISDF_OK;
+  return guarded([&]() -> int {
+    Server* s = static_cast<Server*>(server);
+    if (!s || !st) return record_error(ISDF_ERR_ARG, "server: null");
+    std::lock_guard<std::mutex> lk(s->mu);
+    std::memset(st, 0, sizeof(*st));
+    st->submitted = s->next_ticket - 1;
+    st->completed = s->completed;
+    st->failed = s->failed;
+    st->cancelled = s->cancelled;
+    st->p50_ms = percentile(s->latencies_ms, 0.50);
+    st->p99_ms = percentile(s->latencies_ms, 0.99);
+    double sum = 0;
+    for (double v : s->latencies_ms) sum += v;
+    st->mean_ms = s->latencies_ms.empty() ? 0.0 : sum / (double)s->latencies_ms.size();
+    const auto busy = s->last_finish - s->first_submit;
+    const double span =
+        s->any_submit && s->completed ? std::chrono::duration<double>(busy).count() : 0.0;
+    st->solves_per_s = span > 0 ? (double)s->completed / span : 0.0;
+    st->peak_concurrency = s->peak_running;
+    st->peak_bytes = s->peak_bytes;
+    st->queued = (int)(s->queue.size() + s->small_queue.size());
+    st->running = s->running;
+    return ISDF_OK;
+  });
 }
 
 int isdf_server_destroy(void* server) {
-  Server* s = static_cast<Server*>(server);
-  if (!s) return ISDF_OK;
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    std::deque<long long> keep;  // selected small requests finish their fits
-    for (long long t : s->queue) {
-      Job& j = s->jobs[t];
-      if (j.selected) {
-        keep.push_back(t);
-        continue;
+  return guarded([&]() -> int {
+    Server* s = static_cast<Server*>(server);
+    if (!s) return ISDF_OK;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      std::deque<long long> keep;  // selected small requests finish their fits
+      for (long long t : s->queue) {
+        Job& j = s->jobs[t];
+        if (j.selected) {
+          keep.push_back(t);
+          continue;
+        }
+        j.state = 2;
+        j.status = ISDF_ERR_CANCELLED;
+        s->cancelled++;
       }
-      j.state = 2;
-      j.status = ISDF_ERR_CANCELLED;
-      s->cancelled++;
+      for (long long t : s->small_queue) {
+        Job& j = s->jobs[t];
+        j.state = 2;
+        j.status = ISDF_ERR_CANCELLED;
+        s->cancelled++;
+      }
+      s->small_queue.clear();
+      s->queue = keep;
+      s->stopping = true;
     }
-    for (long long t : s->small_queue) {
-      Job& j = s->jobs[t];
-      j.state = 2;
-      j.status = ISDF_ERR_CANCELLED;
-      s->cancelled++;
-    }
-    s->small_queue.clear();
-    s->queue = keep;
-    s->stopping = true;
-  }
-  s->cv_work.notify_all();
-  s->cv_done.notify_all();
-  if (s->batcher.joinable()) s->batcher.join();
-  for (auto& w : s->workers) w.join();
-  if (s->pool) cudaMemPoolDestroy(s->pool);
-  delete s;
-  return ISDF_OK;
+    s->cv_work.notify_all();
+    s->cv_done.notify_all();
+    if (s->batcher.joinable()) s->batcher.join();
+    for (auto& w : s->workers) w.join();
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    delete s;
+    return ISDF_OK;
+  });
 }
 
 }  // extern "C"
