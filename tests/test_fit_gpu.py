@@ -2,8 +2,8 @@
 reference build itself where it is present) and the numpy restatement
 (oracle/fit.py).
 
-Tolerances. The north star asks theta and the fitted pair densities theta C
-within 1e-10 relative. theta = (Z C^T)(C C^T + eps I)^{-1} with eps =
+Tolerances. The target is theta and the fitted pair densities theta C within
+1e-10 relative. theta = (Z C^T)(C C^T + eps I)^{-1} with eps =
 1e-10 tr/mu is determined only to about cond(C C^T) * 1e-16, and the fitted
 densities carry a share of that: at mu ~ 10 x nstate, C C^T has cond ~ 1e9-1e10
 on the synthetic inputs and ~1e18 on the reference's own Si8 example (rank
@@ -11,7 +11,7 @@ deficient). Two correct FP64 CPU orderings of the reference's own algorithm
 (Cholesky and triangular solves vs LU; OpenBLAS dtrsm vs a LAPACK triangular
 solve) already differ by far more than 1e-10 there. Each bound is therefore
 max(1e-10, 20 x that CPU-vs-CPU spread), the spread measured per case in the
-test; on the well-conditioned cases the bound is the north star's 1e-10.
+test; on the well-conditioned cases the bound is the target's 1e-10.
 Every achieved difference and spread is printed in the run's parity summary.
 """
 import numpy as np

@@ -16,7 +16,7 @@
 theta is compared on 2048 sampled grid rows (oracle.fit.getbasis_rows computes
 exactly those rows of the full-size fit) and the fitted pair densities theta C
 on 1024 sampled state pairs. Bounds: the mixed form's fitted densities within
-1e-6 of the oracle (the north star's figure); the FP64 form's within
+1e-6 of the oracle (the mixed form's accuracy target); the FP64 form's within
 max(1e-10, 20 x the distance between two correct FP64 CPU solutions of the
 same rows, Cholesky + triangular solves vs LU): at cond(C C^T) ~ 1e10 FP64
 rounding alone moves the fitted densities far more than 1e-10, and the test
